@@ -1,0 +1,401 @@
+"""Python mirror of the GCtfFind CTF-estimation interface over the B200 C ABI.
+
+The classes keep the reference's names and call shape so tests and tools
+read like the reference: ``CCTFTheory.Setup`` (FindCTF/CCTFTheory.cpp:69-86),
+``CFindCtf2D.Setup1/Setup2/GenHalfSpectrum/SetPhase/Do2D/Refine/
+GenFullSpectrum/GetSpectSize`` (FindCTF/CFindCTFInc.h:541-623) with the
+public result members ``m_fDfMin, m_fDfMax, m_fAstAng, m_fExtPhase,
+m_fScore``.  All compute runs in lib/libgctf_b200.so (sm_100a); this module
+only marshals arguments.  There is no CPU path: without the library (or a
+GPU) every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgctf_b200.so")
+CLI_PATH = os.path.join(HERE, "bin", "GCtfFind")
+
+GCF_SPECT_FUSED = 0
+GCF_SPECT_CUFFT = 1
+
+# Every symbol include/gctf_b200.h declares.
+EXPORTS = [
+    "gcf_create", "gcf_destroy", "gcf_strerror", "gcf_last_error", "gcf_set_spectrum_impl",
+    "gcf_setup", "gcf_gen_half_spectrum", "gcf_set_phase", "gcf_do2d", "gcf_refine",
+    "gcf_get_spect_size", "gcf_get_half_spectrum", "gcf_gen_full_spectrum",
+    "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
+    "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
+    "gcf_get_stage_times", "gcf_get_launch_count",
+]
+
+
+class GcfError(RuntimeError):
+    pass
+
+
+class Optics(C.Structure):
+    _fields_ = [("kv", C.c_float), ("cs_mm", C.c_float), ("amp_contrast", C.c_float),
+                ("pixel_size", C.c_float), ("ext_phase_deg", C.c_float),
+                ("ext_phase_range", C.c_float)]
+
+
+class Result(C.Structure):
+    _fields_ = [("df_min", C.c_float), ("df_max", C.c_float), ("azimuth", C.c_float),
+                ("ext_phase", C.c_float), ("score", C.c_float), ("ctf_res", C.c_float),
+                ("df_1d", C.c_float), ("phase_1d", C.c_float), ("score_1d", C.c_float),
+                ("lowpassed", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+    def __repr__(self):
+        return "Result(%s)" % ", ".join("%s=%.4f" % (k, v) if isinstance(v, float) else
+                                        "%s=%s" % (k, v) for k, v in self.as_dict().items())
+
+
+class Item(C.Structure):
+    _fields_ = [("image", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
+                ("pixel_size", C.c_float)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libgctf_b200.so not built: run `make -C gctffind_b200` "
+                          "(or __graft_entry__.build())")
+    L = C.CDLL(path)
+    vp, i, f = C.c_void_p, C.c_int, C.c_float
+    L.gcf_create.argtypes = [i, i, i, C.POINTER(vp)]
+    L.gcf_destroy.argtypes = [vp]
+    L.gcf_destroy.restype = None
+    L.gcf_strerror.argtypes = [i]
+    L.gcf_strerror.restype = C.c_char_p
+    L.gcf_last_error.argtypes = [vp]
+    L.gcf_last_error.restype = C.c_char_p
+    L.gcf_set_spectrum_impl.argtypes = [vp, i]
+    L.gcf_setup.argtypes = [vp, C.POINTER(Optics), i, i]
+    L.gcf_gen_half_spectrum.argtypes = [vp, vp, i, i]
+    L.gcf_set_phase.argtypes = [vp, f, f]
+    L.gcf_do2d.argtypes = [vp, C.POINTER(Result)]
+    L.gcf_refine.argtypes = [vp, C.POINTER(f), C.POINTER(f), C.POINTER(f), C.POINTER(f),
+                             C.POINTER(Result)]
+    L.gcf_get_spect_size.argtypes = [vp, C.POINTER(i), i]
+    L.gcf_get_half_spectrum.argtypes = [vp, i, vp]
+    L.gcf_gen_full_spectrum.argtypes = [vp, C.POINTER(Result), vp]
+    L.gcf_get_radial_average.argtypes = [vp, vp]
+    L.gcf_rescale_dims.argtypes = [i, i, f, C.POINTER(i), C.POINTER(i), C.POINTER(f)]
+    L.gcf_rescale_dims.restype = None
+    L.gcf_rescale.argtypes = [vp, vp, i, i, f, i, vp]
+    L.gcf_run_series.argtypes = [vp, C.POINTER(vp), i, i, i, i, C.POINTER(Optics),
+                                 C.POINTER(i), i, C.POINTER(Result), vp]
+    L.gcf_run_batch.argtypes = [vp, C.POINTER(Item), i, i, C.POINTER(Optics), C.POINTER(Result)]
+    L.gcf_mrc_info.argtypes = [C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(f), C.POINTER(i)]
+    L.gcf_mrc_read.argtypes = [C.c_char_p, i, vp]
+    L.gcf_mrc_read_tilts.argtypes = [C.c_char_p, vp, i]
+    L.gcf_mrc_write.argtypes = [C.c_char_p, vp, i, i, i, f]
+    L.gcf_get_stage_times.argtypes = [vp, C.POINTER(f)]
+    L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    for name in EXPORTS:   # every declared entry point must resolve
+        getattr(L, name)
+    _lib = L
+    return L
+
+
+def _check(status: int, ctx=None):
+    if status != 0:
+        L = load_library()
+        msg = L.gcf_strerror(status).decode()
+        if ctx is not None:
+            detail = L.gcf_last_error(ctx).decode()
+            if detail:
+                msg += ": " + detail
+        raise GcfError(msg)
+
+
+def _ptr(a):
+    """(pointer, is_device) of a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data, 0
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr(), 1 if a.is_cuda else 0
+    raise TypeError("expected a numpy array or torch tensor")
+
+
+def _as_f32(a):
+    if isinstance(a, np.ndarray):
+        return np.ascontiguousarray(a, dtype=np.float32)
+    import torch
+    if a.dtype != torch.float32 or not a.is_contiguous():
+        a = a.to(torch.float32).contiguous()
+    return a
+
+
+def rescale_dims(w: int, h: int, px: float):
+    L = load_library()
+    nw, nh, npx = C.c_int(), C.c_int(), C.c_float()
+    L.gcf_rescale_dims(w, h, px, C.byref(nw), C.byref(nh), C.byref(npx))
+    return nw.value, nh.value, npx.value
+
+
+def make_optics(kv=300.0, cs_mm=2.7, amp_contrast=0.07, pixel_size=1.0, ext_phase_deg=0.0,
+                ext_phase_range=0.0) -> Optics:
+    return Optics(kv, cs_mm, amp_contrast, pixel_size, ext_phase_deg, ext_phase_range)
+
+
+class Context:
+    """One CUDA stream + all device state (gcf_ctx)."""
+
+    def __init__(self, gpu: int = 0, tile_size: int = 512, log_spect: int = 0,
+                 spectrum_impl: int | None = None):
+        L = load_library()
+        h = C.c_void_p()
+        _check(L.gcf_create(gpu, tile_size, log_spect, C.byref(h)))
+        self._h = h
+        self.tile_size = tile_size
+        self.L = L
+        if spectrum_impl is not None:
+            _check(L.gcf_set_spectrum_impl(h, spectrum_impl), h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.gcf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_spectrum_impl(self, impl: int):
+        _check(self.L.gcf_set_spectrum_impl(self._h, impl), self._h)
+
+    # -- CFindCtf2D shape ------------------------------------------------------
+    def setup(self, optics: Optics, width: int, height: int):
+        _check(self.L.gcf_setup(self._h, C.byref(optics), width, height), self._h)
+
+    def gen_half_spectrum(self, img, pitch: int | None = None):
+        img = _as_f32(img)
+        p, dev = _ptr(img)
+        if pitch is None:
+            pitch = img.shape[-1]
+        _check(self.L.gcf_gen_half_spectrum(self._h, p, pitch, dev), self._h)
+
+    def set_phase(self, phase_deg: float, range_deg: float):
+        _check(self.L.gcf_set_phase(self._h, phase_deg, range_deg), self._h)
+
+    def do2d(self) -> Result:
+        r = Result()
+        _check(self.L.gcf_do2d(self._h, C.byref(r)), self._h)
+        return r
+
+    def refine(self, df_mean, ast_ratio, ast_angle, ext_phase) -> Result:
+        arr = lambda v: (C.c_float * 2)(*v)
+        r = Result()
+        _check(self.L.gcf_refine(self._h, arr(df_mean), arr(ast_ratio), arr(ast_angle),
+                                 arr(ext_phase), C.byref(r)), self._h)
+        return r
+
+    def half_spectrum(self, raw: bool) -> np.ndarray:
+        out = np.zeros((self.tile_size, self.tile_size // 2 + 1), np.float32)
+        _check(self.L.gcf_get_half_spectrum(self._h, 1 if raw else 0, out.ctypes.data), self._h)
+        return out
+
+    def radial_average(self) -> np.ndarray:
+        out = np.zeros(self.tile_size // 2 + 1, np.float32)
+        _check(self.L.gcf_get_radial_average(self._h, out.ctypes.data), self._h)
+        return out
+
+    def full_spectrum(self, res: Result) -> np.ndarray:
+        out = np.zeros((self.tile_size, self.tile_size), np.float32)
+        _check(self.L.gcf_gen_full_spectrum(self._h, C.byref(res), out.ctypes.data), self._h)
+        return out
+
+    def rescale(self, img, px: float) -> np.ndarray:
+        img = _as_f32(img)
+        h, w = img.shape
+        nw, nh, _ = rescale_dims(w, h, px)
+        out = np.zeros((nh, nw), np.float32)
+        p, dev = _ptr(img)
+        _check(self.L.gcf_rescale(self._h, p, w, h, px, dev, out.ctypes.data), self._h)
+        return out
+
+    # -- batched paths -----------------------------------------------------------
+    def run_series(self, images, optics: Optics, order=None, is_tomo: bool = True,
+                   want_full: bool = False):
+        imgs = [_as_f32(a) for a in images]
+        n = len(imgs)
+        h, w = imgs[0].shape
+        ptrs = [_ptr(a) for a in imgs]
+        dev = ptrs[0][1]
+        if any(d != dev for _, d in ptrs):
+            raise ValueError("images must all be on the host or all on the GPU")
+        if order is None:
+            order = list(range(n))
+        parr = (C.c_void_p * n)(*[p for p, _ in ptrs])
+        oarr = (C.c_int * n)(*order)
+        res = (Result * n)()
+        full = np.zeros((n, self.tile_size, self.tile_size), np.float32) if want_full else None
+        _check(self.L.gcf_run_series(self._h, parr, n, w, h, dev, C.byref(optics), oarr,
+                                     1 if is_tomo else 0, res,
+                                     full.ctypes.data if want_full else None), self._h)
+        out = [res[i] for i in range(n)]
+        return (out, full) if want_full else out
+
+    def run_batch(self, images, pixel_sizes, optics: Optics):
+        imgs = [_as_f32(a) for a in images]
+        n = len(imgs)
+        items = (Item * n)()
+        dev = None
+        for k, a in enumerate(imgs):
+            p, d = _ptr(a)
+            dev = d if dev is None else dev
+            if d != dev:
+                raise ValueError("images must all be on the host or all on the GPU")
+            items[k] = Item(p, a.shape[1], a.shape[0], float(pixel_sizes[k]))
+        res = (Result * n)()
+        _check(self.L.gcf_run_batch(self._h, items, n, dev, C.byref(optics), res), self._h)
+        return [res[i] for i in range(n)]
+
+    def stage_times(self):
+        t = (C.c_float * 7)()
+        _check(self.L.gcf_get_stage_times(self._h, t), self._h)
+        keys = ["upload", "rescale", "spectrum", "post", "search1d", "search2d", "total"]
+        return dict(zip(keys, list(t)))
+
+    def launch_count(self) -> int:
+        v = C.c_longlong()
+        _check(self.L.gcf_get_launch_count(self._h, C.byref(v)), self._h)
+        return v.value
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped classes
+# ---------------------------------------------------------------------------
+class CCTFTheory:
+    """Optics holder with CCTFTheory::Setup's signature (FindCTF/CCTFTheory.cpp:69-86)."""
+
+    def __init__(self):
+        self.optics = make_optics()
+
+    def Setup(self, fKv, fCs, fAmpContrast, fPixelSize, fAstTol=100.0, fExtPhase=0.0):
+        # fExtPhase in radian as in the reference; stored in degrees for the ABI.
+        self.optics = make_optics(fKv, fCs, fAmpContrast, fPixelSize,
+                                  float(np.degrees(fExtPhase)), 0.0)
+
+
+class CFindCtf2D:
+    """CFindCtf2D call shape (FindCTF/CFindCTFInc.h:605-623) on a Context."""
+
+    def __init__(self, tile_size: int = 512, log_spect: int = 0, gpu: int = 0, ctx=None):
+        self.ctx = ctx or Context(gpu, tile_size, log_spect)
+        self.m_fDfMin = self.m_fDfMax = self.m_fAstAng = 0.0
+        self.m_fExtPhase = self.m_fScore = 0.0
+        self._theory = None
+        self._result = None
+
+    def Setup1(self, theory: CCTFTheory):
+        self._theory = theory
+
+    def Setup2(self, img_size):
+        self.ctx.setup(self._theory.optics, int(img_size[0]), int(img_size[1]))
+
+    def SetPhase(self, fInitPhase, fPhaseRange):
+        self.ctx.set_phase(fInitPhase, fPhaseRange)
+
+    def GenHalfSpectrum(self, img):
+        self.ctx.gen_half_spectrum(img)
+
+    def _take(self, r: Result):
+        self._result = r
+        self.m_fDfMin, self.m_fDfMax = r.df_min, r.df_max
+        self.m_fAstAng, self.m_fExtPhase, self.m_fScore = r.azimuth, r.ext_phase, r.score
+
+    def Do2D(self):
+        self._take(self.ctx.do2d())
+
+    def Refine(self, afDfMean, afAstRatio, afAstAngle, afExtPhase):
+        self._take(self.ctx.refine(afDfMean, afAstRatio, afAstAngle, afExtPhase))
+
+    def GenFullSpectrum(self):
+        return self.ctx.full_spectrum(self._result)
+
+    def GetSpectSize(self, bHalf: bool):
+        t = self.ctx.tile_size
+        return (t // 2 + 1, t) if bHalf else (t, t)
+
+    def GetHalfSpect(self, bRaw: bool):
+        return self.ctx.half_spectrum(bRaw)
+
+
+# ---------------------------------------------------------------------------
+# MRC helpers
+# ---------------------------------------------------------------------------
+def mrc_info(path: str):
+    L = load_library()
+    dims = (C.c_int * 3)()
+    mode, px, nf = C.c_int(), C.c_float(), C.c_int()
+    _check(L.gcf_mrc_info(path.encode(), dims, C.byref(mode), C.byref(px), C.byref(nf)))
+    return {"dims": tuple(dims), "mode": mode.value, "pixel_size": px.value, "ext_floats": nf.value}
+
+
+def mrc_read(path: str, z: int = 0) -> np.ndarray:
+    L = load_library()
+    info = mrc_info(path)
+    nx, ny, _ = info["dims"]
+    out = np.zeros((ny, nx), np.float32)
+    _check(L.gcf_mrc_read(path.encode(), z, out.ctypes.data))
+    return out
+
+
+def mrc_read_tilts(path: str, n: int) -> np.ndarray:
+    L = load_library()
+    out = np.zeros(n, np.float32)
+    _check(L.gcf_mrc_read_tilts(path.encode(), out.ctypes.data, n))
+    return out
+
+
+def mrc_write(path: str, data: np.ndarray, pixel_size: float = 1.0):
+    L = load_library()
+    data = np.ascontiguousarray(data, np.float32)
+    if data.ndim == 2:
+        data = data[None]
+    nz, ny, nx = data.shape
+    _check(L.gcf_mrc_write(path.encode(), data.ctypes.data, nx, ny, nz, pixel_size))
+
+
+@dataclass
+class SeriesOrder:
+    """Processing order of a tilt series: the zero tilt first, then the
+    others in file order (CLoadImages::mReadTomo, MrcUtil/CLoadImages.cpp:71-91,
+    CInputFolder::FindZeroTilt, CInputFolder.cpp:50-69)."""
+    zero_tilt: int
+    order: list
+
+
+def series_order(tilts) -> SeriesOrder:
+    n = len(tilts)
+    if n > 1 and abs(float(tilts[0]) - float(tilts[1])) < 0.0001:
+        z = n // 2
+    else:
+        z, fmin = -1, 10000.0
+        for i, t in enumerate(tilts):
+            a = abs(float(np.float32(t)))
+            if a >= fmin:
+                continue
+            fmin, z = a, i
+        if z < 0:
+            z = n // 2
+    return SeriesOrder(z, [z] + [i for i in range(n) if i != z])

@@ -1,0 +1,1218 @@
+// gcf_capi.cpp -- host side of the B200 CTF-estimation library: context,
+// host-built tables, device buffers, the C ABI of include/gctf_b200.h and
+// the batched series driver.
+//
+// Compiled with -ffp-contract=off: the float expressions that the
+// reference evaluates on the host (search windows, steps, tables) are
+// rounded operation by operation here too.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "gcf_internal.h"
+
+using namespace gcf;
+
+namespace gcf {
+// Optional: fused spectrum path (gcf_fused.cu).
+int fused_tile_supported(int tile);
+}
+
+namespace {
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t cnt)
+    {
+        if (cnt <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(cnt, 1) * sizeof(T));
+        if (e == cudaSuccess) n = cnt;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct BandHost {
+    int tile;
+    float px, kv, cs, ac;
+    int n;
+    DBuf<int> idx;
+    DBuf<float> a, d, env, c2t, s2t;
+    BandDev dev;
+};
+
+struct FftPlan {
+    cufftHandle h = 0;
+};
+
+}  // namespace
+
+struct gcf_ctx {
+    int dev = 0;
+    int tile = 512;
+    int log_spect = 0;
+    int impl = GCF_SPECT_CUFFT;
+    cudaStream_t st = nullptr;
+    std::string err;
+    long long launches = 0;
+    float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t ev[8] = {};
+
+    // per-tile tables
+    DBuf<float> taper;
+    DBuf<int> rad_off, rad_pix;
+    DBuf<double> lp_h;
+    int lp_radius = 0;
+
+    // bands
+    std::vector<BandHost*> bands;
+    DBuf<BandDev> d_bands;
+    bool bands_dirty = true;
+
+    // buffers
+    DBuf<float> images, rescaled, tiles;
+    DBuf<float2> cmp, rs_cmp, rs_crop;
+    DBuf<double> acc, hsum, lptmp, moments, moments2;
+    DBuf<float> raw, ctf0, ctf, radial, band_spec, cc_res, full;
+    DBuf<int> lowpassed, spec_off, mic_of;
+    DBuf<SearchJob> jobs;
+    DBuf<double> sum_ss;
+    DBuf<float4> cand;
+    DBuf<float2> cval;
+    DBuf<double2> part;
+    DBuf<gcf_result> d_res;
+    DBuf<PixOptics> d_optics;
+
+    std::map<std::tuple<int, int, int>, FftPlan> plans;   // (kind, a, b)
+
+    // CFindCtf2D call-shape state
+    gcf_optics optics{};
+    bool have_setup = false;
+    bool have_spectrum = false;
+    int img_w = 0, img_h = 0;
+    float phase_deg = 0.0f, phase_range = 0.0f;
+    int cur_lowpassed = 0;
+};
+
+namespace {
+
+gcf_status fail(gcf_ctx* c, gcf_status s, const char* what)
+{
+    if (c) c->err = what ? what : "";
+    return s;
+}
+
+gcf_status cuda_fail(gcf_ctx* c, cudaError_t e, const char* where)
+{
+    if (c) c->err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? GCF_ERR_NO_MEMORY : GCF_ERR_CUDA;
+}
+
+#define CK(call)                                                     \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);     \
+    } while (0)
+
+#define CKS(call)                                                    \
+    do {                                                             \
+        gcf_status s_ = (call);                                      \
+        if (s_ != GCF_OK) return s_;                                 \
+    } while (0)
+
+#define CKL()                                                        \
+    do {                                                             \
+        cudaError_t e_ = cudaGetLastError();                         \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, "kernel launch"); \
+    } while (0)
+
+// CCTFTheory::Setup + GCalcCTF2D::SetParam in pixel units.
+PixOptics make_optics(const gcf_optics& op, float px_n)
+{
+    PixOptics o;
+    double wl = 12.26 / std::sqrt((double)op.kv * 1000.0 + 0.9784 * (double)op.kv * op.kv);
+    o.wl = (float)wl / px_n;
+    o.cs = (float)((double)op.cs_mm * 1e7 / px_n);
+    float ac = op.amp_contrast;
+    o.amp_phase = (float)atanf(ac / sqrtf(1.0f - ac * ac));
+    o.px = px_n;
+    return o;
+}
+
+void res_range_of(float px, float r[2])
+{
+    r[0] = 25.0f * px;
+    r[1] = (2.0f * px) / 0.8f;
+    if (r[1] < 3.5f) r[1] = 3.5f;
+}
+
+struct Layout {
+    int ntx, nty, offx, offy, ov, stride;
+};
+
+Layout tile_layout(int w, int h, int tile)
+{
+    Layout L;
+    int ov = (int)(tile * 0.50f);
+    ov = ov / 2 * 2;
+    L.ov = ov;
+    L.stride = tile - ov;
+    L.ntx = (w - ov) / L.stride;
+    L.nty = (h - ov) / L.stride;
+    L.offx = (w - L.ntx * tile + (L.ntx - 1) * ov) / 2;
+    L.offy = (h - L.nty * tile + (L.nty - 1) * ov) / 2;
+    return L;
+}
+
+gcf_status build_tile_tables(gcf_ctx* ctx)
+{
+    int T = ctx->tile, cx = T / 2 + 1, cy = T;
+    // GRoundEdge taper (FindCTF/GRoundEdge.cu:7-25)
+    std::vector<float> tp((size_t)T * T);
+    double c = T * 0.5, s = T;
+    for (int y = 0; y < T; ++y)
+        for (int x = 0; x < T; ++x) {
+            double fx = 2.0 * std::fabs(x - c) / s, fy = 2.0 * std::fabs(y - c) / s;
+            double r = std::sqrt(fx * fx + fy * fy), v = 0.0;
+            if (r < 1.0) {
+                double q = 0.5 * (1.0 - std::cos(M_PI * r));
+                v = 1.0 - q * q * q;
+            }
+            tp[(size_t)y * T + x] = (float)v;
+        }
+    CK(ctx->taper.ensure(tp.size()));
+    CK(cudaMemcpy(ctx->taper.p, tp.data(), tp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    // GRadialAvg nearest-pixel samples (FindCTF/GRadialAvg.cu:11-33)
+    std::vector<int> off(cx + 1), pix;
+    for (int r = 0; r < cx; ++r) {
+        off[r] = (int)pix.size();
+        int np = (int)(3.1415926f * r + 0.5f);
+        if (np < 1) np = 1;
+        else if (np > 180) np = 180;
+        float step = 180.0f / np;
+        for (int i = 0; i < np; ++i) {
+            float rad = (-90.0f + i * step) * 0.017453f;
+            int x = (int)(r * cosf(rad) + 0.5f);
+            int y = (int)(r * sinf(rad) + cy / 2 + 0.5f);
+            if (y > cy - 1) y = cy - 1;   // the reference reads one row past for r = cx-1
+            if (x > cx - 1) x = cx - 1;
+            pix.push_back(y * cx + x);
+        }
+    }
+    off[cx] = (int)pix.size();
+    CK(ctx->rad_off.ensure(off.size()));
+    CK(ctx->rad_pix.ensure(pix.size()));
+    CK(cudaMemcpy(ctx->rad_off.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->rad_pix.p, pix.data(), pix.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // Periodic kernel of the B-factor lowpass, B = 10
+    // (FindCTF/CFindCtfBase.cpp:203-206, FindCTF/GLowpass2D.cu:57-70).
+    double a = 10.0 / ((double)T * T + (double)T * T);
+    auto hval = [&](int t) {
+        double sacc = 0.0;
+        for (int k = -T / 2 + 1; k <= T / 2; ++k)
+            sacc += std::exp(-a * (double)k * k) * std::cos(2.0 * M_PI * (double)k * t / T);
+        return sacc / T;
+    };
+    double h0 = hval(0);
+    int R = 1;
+    while (R < T / 2 - 1 && std::fabs(hval(R + 1)) > 1e-17 * h0) ++R;
+    std::vector<double> h(2 * R + 1);
+    for (int t = -R; t <= R; ++t) h[t + R] = hval(t);
+    ctx->lp_radius = R;
+    CK(ctx->lp_h.ensure(h.size()));
+    CK(cudaMemcpy(ctx->lp_h.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return GCF_OK;
+}
+
+// In-band pixels of the 2D correlation (CFindDefocus2D::Setup2,
+// FindCTF/CFindDefocus2D.cpp:86-92; GCC2D band, FindCTF/GCC2D.cu:148-160).
+gcf_status get_band(gcf_ctx* ctx, const gcf_optics& op, float px_n, int* slot)
+{
+    int T = ctx->tile;
+    for (size_t i = 0; i < ctx->bands.size(); ++i) {
+        BandHost* b = ctx->bands[i];
+        if (b->tile == T && b->px == px_n && b->kv == op.kv && b->cs == op.cs_mm &&
+            b->ac == op.amp_contrast) {
+            *slot = (int)i;
+            return GCF_OK;
+        }
+    }
+    int cx = T / 2 + 1, cy = T;
+    PixOptics o = make_optics(op, px_n);
+    float rr[2];
+    res_range_of(px_n, rr);
+    float res1 = cy * px_n;
+    float lo = res1 / rr[0], hi = res1 / rr[1];
+    float l = lo / cy, hh = hi / cy;
+    if (hh > 0.75f) hh = 0.75f;
+    float lo2 = l * l, hi2 = hh * hh;
+    std::vector<int> idx;
+    std::vector<float> va, vd, ve, vc, vs;
+    for (int y = 0; y < cy; ++y) {
+        float fyf = (y - cy * 0.5f) / cy;
+        double fy = (double)(y - cy / 2) / cy;
+        for (int x = 0; x < cx; ++x) {
+            float fxf = (0.5f * x) / (cx - 1);
+            float s2f = fxf * fxf + fyf * fyf;
+            if (s2f < lo2 || s2f > hi2) continue;
+            double fx = x * 0.5 / (cx - 1);
+            double s2 = fx * fx + fy * fy;
+            double th = std::atan(fy / (fx + 1e-30));
+            idx.push_back(y * cx + x);
+            va.push_back((float)((double)o.wl * s2));
+            vd.push_back((float)(-0.5 * (double)o.wl * o.wl * o.wl * s2 * s2 * o.cs));
+            ve.push_back((float)std::exp(-16.0 * s2));
+            vc.push_back((float)std::cos(2.0 * th));
+            vs.push_back((float)std::sin(2.0 * th));
+        }
+    }
+    BandHost* b = new BandHost();
+    b->tile = T;
+    b->px = px_n;
+    b->kv = op.kv;
+    b->cs = op.cs_mm;
+    b->ac = op.amp_contrast;
+    b->n = (int)idx.size();
+    size_t n = idx.size();
+    cudaError_t e = cudaSuccess;
+    if ((e = b->idx.ensure(n)) != cudaSuccess || (e = b->a.ensure(n)) != cudaSuccess ||
+        (e = b->d.ensure(n)) != cudaSuccess || (e = b->env.ensure(n)) != cudaSuccess ||
+        (e = b->c2t.ensure(n)) != cudaSuccess || (e = b->s2t.ensure(n)) != cudaSuccess) {
+        delete b;
+        return cuda_fail(ctx, e, "band alloc");
+    }
+    CK(cudaMemcpy(b->idx.p, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->a.p, va.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d.p, vd.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->env.p, ve.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->c2t.p, vc.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->s2t.p, vs.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    b->dev.n = b->n;
+    b->dev.cx = cx;
+    b->dev.cy = cy;
+    b->dev.pad = 0;
+    b->dev.idx = b->idx.p;
+    b->dev.a = b->a.p;
+    b->dev.d = b->d.p;
+    b->dev.env = b->env.p;
+    b->dev.c2t = b->c2t.p;
+    b->dev.s2t = b->s2t.p;
+    ctx->bands.push_back(b);
+    ctx->bands_dirty = true;
+    *slot = (int)ctx->bands.size() - 1;
+    return GCF_OK;
+}
+
+gcf_status upload_bands(gcf_ctx* ctx)
+{
+    if (!ctx->bands_dirty) return GCF_OK;
+    std::vector<BandDev> v;
+    for (auto* b : ctx->bands) v.push_back(b->dev);
+    CK(ctx->d_bands.ensure(v.size()));
+    CK(cudaMemcpy(ctx->d_bands.p, v.data(), v.size() * sizeof(BandDev), cudaMemcpyHostToDevice));
+    ctx->bands_dirty = false;
+    return GCF_OK;
+}
+
+gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
+{
+    auto key = std::make_tuple(kind, a, b);
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end()) {
+        *out = it->second.h;
+        return GCF_OK;
+    }
+    cufftHandle h;
+    cufftResult r;
+    if (kind == 0) {   // batched tile R2C: a = tile, b = batch
+        int n[2] = {a, a};
+        r = cufftPlanMany(&h, 2, n, nullptr, 1, a * a, nullptr, 1, (a / 2 + 1) * a, CUFFT_R2C, b);
+    } else if (kind == 1) {   // image R2C: a = height, b = width
+        r = cufftPlan2d(&h, a, b, CUFFT_R2C);
+    } else {   // image C2R: a = height, b = width
+        r = cufftPlan2d(&h, a, b, CUFFT_C2R);
+    }
+    if (r != CUFFT_SUCCESS) {
+        ctx->err = "cufft plan creation failed (" + std::to_string((int)r) + ")";
+        return r == CUFFT_ALLOC_FAILED ? GCF_ERR_NO_MEMORY : GCF_ERR_CUFFT;
+    }
+    if (cufftSetStream(h, ctx->st) != CUFFT_SUCCESS) {
+        cufftDestroy(h);
+        return fail(ctx, GCF_ERR_CUFFT, "cufftSetStream failed");
+    }
+    ctx->plans[key].h = h;
+    *out = h;
+    return GCF_OK;
+}
+
+// Image description for the spectrum stage.
+struct MicImage {
+    const float* img;   // device
+    int w, h, pitch;
+    float px_n;
+};
+
+// CGenAvgSpectrum::DoIt for one micrograph, batched-cuFFT variant.
+gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
+{
+    int T = ctx->tile, cx = T / 2 + 1;
+    Layout L = tile_layout(m.w, m.h, T);
+    int nt = L.ntx * L.nty;
+    if (L.ntx <= 0 || L.nty <= 0) return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no tile");
+    const int kBatch = 256;
+    int batch = std::min(nt, kBatch);
+    CK(ctx->tiles.ensure((size_t)batch * T * T));
+    CK(ctx->cmp.ensure((size_t)batch * cx * T));
+    CK(ctx->acc.ensure((size_t)cx * T));
+    CK(cudaMemsetAsync(ctx->acc.p, 0, (size_t)cx * T * sizeof(double), ctx->st));
+    for (int t0 = 0; t0 < nt; t0 += batch) {
+        int nb = std::min(batch, nt - t0);
+        launch_extract_tiles(m.img, m.w, m.h, m.pitch, T, L.ntx, L.offx, L.offy, L.stride, t0, nb,
+                             ctx->taper.p, ctx->tiles.p, ctx->st);
+        CKL();
+        ctx->launches += 1;
+        cufftHandle plan;
+        CKS(get_plan(ctx, 0, T, nb, &plan));
+        if (cufftExecR2C(plan, ctx->tiles.p, (cufftComplex*)ctx->cmp.p) != CUFFT_SUCCESS)
+            return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (tiles) failed");
+        launch_amp_accumulate(ctx->cmp.p, T, nb, ctx->acc.p, ctx->st);
+        CKL();
+        ctx->launches += 1;
+    }
+    launch_finalize_raw(ctx->acc.p, cx * T, 1.0 / nt, raw_out, ctx->st);
+    CKL();
+    ctx->launches += 1;
+    return GCF_OK;
+}
+
+// CFindCtfBase::GenHalfSpectrum for n micrographs (slots 0..n-1):
+// spectrum, background removal, moments, lowpass, radial average.
+gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
+{
+    int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
+    size_t cmp_n = (size_t)cx * T;
+    CK(ctx->raw.ensure(cmp_n * nm));
+    CK(ctx->ctf0.ensure(cmp_n * nm));
+    CK(ctx->ctf.ensure(cmp_n * nm));
+    CK(ctx->hsum.ensure(cmp_n * nm));
+    CK(ctx->lptmp.ensure(cmp_n * nm));
+    CK(ctx->moments.ensure(2 * (size_t)nm));
+    CK(ctx->lowpassed.ensure(nm));
+    CK(ctx->radial.ensure((size_t)cx * nm));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    for (int i = 0; i < nm; ++i) CKS(spectrum_cufft(ctx, mics[i], ctx->raw.p + cmp_n * i));
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    launch_bg_horizontal(ctx->raw.p, T, nm, ctx->log_spect, ctx->hsum.p, ctx->st);
+    CKL();
+    launch_bg_vertical(ctx->raw.p, ctx->hsum.p, T, nm, ctx->log_spect, ctx->ctf0.p, ctx->st);
+    CKL();
+    launch_moments(ctx->ctf0.p, (int)cmp_n, nm, ctx->moments.p, ctx->st);
+    CKL();
+    launch_lowpass(ctx->ctf0.p, T, nm, ctx->moments.p, ctx->lp_h.p, ctx->lp_radius, ctx->lptmp.p,
+                   ctx->ctf.p, ctx->lowpassed.p, ctx->st);
+    CKL();
+    launch_radial(ctx->ctf.p, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p, ctx->st);
+    CKL();
+    ctx->launches += 6;
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    return GCF_OK;
+}
+
+// Host description of one search job.
+struct JobSpec {
+    int mic;
+    int mode;   // 0 Do2D, 1 Refine
+    gcf_optics optics;
+    float px_n;
+    float phase_deg, phase_range;     // Do2D: CFindCtfBase::m_fExtPhase / m_fPhaseRange
+    float rin[8];                     // Refine: {df, df_range, ast, ast_range, ang, ang_range, ph, ph_range}
+};
+
+// CFindDefocus2D::Setup3 + Refine (FindCTF/CFindDefocus2D.cpp:98-151) on the host.
+void refine_init(SearchJob& J, const float* rin)
+{
+    J.df_mean = rin[0];
+    J.ast_ratio = rin[2];
+    J.ast_angle = rin[4];
+    J.phase_range[0] = rin[6];
+    J.ext_phase = rin[6];
+    float h = 0.5f * rin[1];
+    J.df_range[0] = fmaxf(J.df_mean - h, 3000.0f);
+    J.df_range[1] = J.df_mean + h;
+    h = 0.5f * rin[3];
+    J.ast_range[0] = fmaxf(J.ast_ratio - h, 0.0f);
+    J.ast_range[1] = fminf(J.ast_ratio + h, 0.02f);
+    h = 0.5f * rin[5];
+    J.ang_range[0] = fmaxf(J.ast_angle - h, -90.0f);
+    J.ang_range[1] = fminf(J.ast_angle + h, 90.0f);
+    J.phase_range[1] = rin[7];
+}
+
+// Runs the 1D + 2D searches of `specs` on the spectra already in their
+// slots; results in job order.
+gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vector<gcf_result>& out)
+{
+    int nj = (int)specs.size();
+    out.assign(nj, gcf_result{});
+    if (nj == 0) return GCF_OK;
+    int T = ctx->tile, cx = T / 2 + 1;
+    size_t cmp_n = (size_t)cx * T;
+    std::vector<SearchJob> jh(nj);
+    std::vector<int> soff(nj);
+    int tot = 0, max_band = 0;
+    bool any_full = false, any_grid = false, any_phase = false;
+    for (int j = 0; j < nj; ++j) {
+        const JobSpec& s = specs[j];
+        SearchJob& J = jh[j];
+        std::memset(&J, 0, sizeof(J));
+        int slot = -1;
+        CKS(get_band(ctx, s.optics, s.px_n, &slot));
+        J.mic = s.mic;
+        J.band = slot;
+        J.mode = s.mode;
+        J.o = make_optics(s.optics, s.px_n);
+        J.phase_range_in = fmaxf(s.phase_range, 0.0f);
+        J.ext_phase_in = s.phase_deg;
+        J.step = STEP_CC0;
+        if (s.mode == 1) {
+            refine_init(J, s.rin);
+            if (J.ast_range[1] - J.ast_range[0] >= (float)1e-20 ||
+                J.ang_range[1] - J.ang_range[0] >= (float)1e-20)
+                any_grid = true;
+            if (J.phase_range[1] > 0) any_phase = true;
+        } else {
+            any_full = true;
+            any_grid = true;
+            if (J.phase_range_in > 0) any_phase = true;
+        }
+        soff[j] = tot;
+        int bn = ctx->bands[slot]->n;
+        tot += bn;
+        max_band = std::max(max_band, bn);
+    }
+    CKS(upload_bands(ctx));
+    int max_chunks = std::max(1, (max_band + kEvalChunk - 1) / kEvalChunk);
+    CK(ctx->jobs.ensure(nj));
+    CK(ctx->spec_off.ensure(nj));
+    CK(ctx->band_spec.ensure(std::max(tot, 1)));
+    CK(ctx->sum_ss.ensure(nj));
+    CK(ctx->cand.ensure((size_t)nj * kMaxCand));
+    CK(ctx->cval.ensure((size_t)nj * kMaxCand));
+    CK(ctx->part.ensure((size_t)nj * kMaxCand * max_chunks));
+    CK(ctx->cc_res.ensure((size_t)nj * cx));
+    CK(ctx->d_res.ensure(nj));
+    CK(cudaMemcpyAsync(ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->spec_off.p, soff.data(), nj * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->st));
+    launch_band_gather(ctx->ctf.p, (int)cmp_n, ctx->jobs.p, ctx->d_bands.p, ctx->spec_off.p, nj,
+                       ctx->band_spec.p, ctx->sum_ss.p, ctx->st);
+    CKL();
+    ctx->launches += 1;
+    EvalArgs a;
+    a.jobs = ctx->jobs.p;
+    a.bands = ctx->d_bands.p;
+    a.band_spec = ctx->band_spec.p;
+    a.sum_ss = ctx->sum_ss.p;
+    a.spec_off = ctx->spec_off.p;
+    a.cand = ctx->cand.p;
+    a.cval = ctx->cval.p;
+    a.part = ctx->part.p;
+    a.max_chunks = max_chunks;
+    a.njobs = nj;
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    if (any_full) {
+        launch_search1d(ctx->jobs.p, nj, ctx->radial.p, cx, ctx->cand.p, ctx->cval.p, ctx->st);
+        CKL();
+        ctx->launches += 1;
+    }
+    launch_init_jobs(a, ctx->st);   // Refine jobs: pending step CC0
+    CKL();
+    ctx->launches += 1;
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    // Upper bound of non-empty steps: CC0 + astigmatism grid + 19 x 4 refinements.
+    int pairs = 2 + 19 * ((any_grid ? 2 : 0) + 1 + (any_phase ? 1 : 0));
+    for (int k = 0; k < pairs; ++k) {
+        int cb = (k == 0) ? 1 : (k == 1 && any_grid) ? (kMaxCand / kEvalCB + 3) / 4 : 4;
+        launch_eval2d(a, cb, max_band, ctx->st);
+        CKL();
+        launch_update2d(a, ctx->st);
+        CKL();
+        ctx->launches += 2;
+    }
+    // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)
+    launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->cc_res.p, ctx->st);
+    CKL();
+    launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
+    CKL();
+    launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->st);
+    CKL();
+    ctx->launches += 3;
+    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    float t1 = 0, t2 = 0;
+    cudaEventElapsedTime(&t1, ctx->ev[5], ctx->ev[6]);
+    cudaEventElapsedTime(&t2, ctx->ev[6], ctx->ev[7]);
+    ctx->stage_ms[4] += t1;
+    ctx->stage_ms[5] += t2;
+    return GCF_OK;
+}
+
+gcf_status set_device(gcf_ctx* ctx)
+{
+    CK(cudaSetDevice(ctx->dev));
+    return GCF_OK;
+}
+
+// CRescaleImage::DoIt on the device: returns a dense new_w x new_h image
+// (FindCTF/CRescaleImage.cpp:68-99).
+gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px, float* out,
+                          int* nw_out, int* nh_out, float* px_out, bool* copied)
+{
+    int nw, nh;
+    float pxn;
+    gcf_rescale_dims(w, h, px, &nw, &nh, &pxn);
+    *nw_out = nw;
+    *nh_out = nh;
+    *px_out = pxn;
+    float bin = 1.2f / px;
+    if (bin <= 1) bin = 1.0f;
+    if (bin == 1.0f) {
+        *copied = false;
+        return GCF_OK;
+    }
+    *copied = true;
+    int cxi = w / 2 + 1, cxo = nw / 2 + 1;
+    CK(ctx->rs_cmp.ensure((size_t)cxi * h));
+    CK(ctx->rs_crop.ensure((size_t)cxo * nh));
+    cufftHandle p1, p2;
+    CKS(get_plan(ctx, 1, h, w, &p1));
+    CKS(get_plan(ctx, 2, nh, nw, &p2));
+    if (cufftExecR2C(p1, (cufftReal*)img, (cufftComplex*)ctx->rs_cmp.p) != CUFFT_SUCCESS)
+        return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (rescale) failed");
+    launch_fourier_crop(ctx->rs_cmp.p, cxi, h, ctx->rs_crop.p, cxo, nh, ctx->st);
+    CKL();
+    ctx->launches += 1;
+    if (cufftExecC2R(p2, (cufftComplex*)ctx->rs_crop.p, (cufftReal*)out) != CUFFT_SUCCESS)
+        return fail(ctx, GCF_ERR_CUFFT, "cufftExecC2R (rescale) failed");
+    return GCF_OK;
+}
+
+bool valid_optics(const gcf_optics* o)
+{
+    return o && o->kv > 0 && o->cs_mm >= 0 && o->amp_contrast >= 0 && o->amp_contrast < 1 &&
+           o->pixel_size > 0;
+}
+
+// Uploads (if needed), rescales and produces the spectra of n images.
+gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* ws, const int* hs,
+                          const float* pxs, int n, int on_device, std::vector<MicImage>& mics)
+{
+    mics.clear();
+    size_t tot_raw = 0, tot_new = 0;
+    std::vector<int> nws(n), nhs(n);
+    std::vector<float> pxn(n);
+    for (int i = 0; i < n; ++i) {
+        gcf_rescale_dims(ws[i], hs[i], pxs[i], &nws[i], &nhs[i], &pxn[i]);
+        tot_raw += (size_t)ws[i] * hs[i];
+        float bin = 1.2f / pxs[i];
+        if (bin > 1) tot_new += (size_t)nws[i] * nhs[i];
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    std::vector<const float*> dimg(n);
+    if (!on_device) {
+        CK(ctx->images.ensure(tot_raw));
+        size_t off = 0;
+        for (int i = 0; i < n; ++i) {
+            size_t cnt = (size_t)ws[i] * hs[i];
+            CK(cudaMemcpyAsync(ctx->images.p + off, images[i], cnt * sizeof(float),
+                               cudaMemcpyHostToDevice, ctx->st));
+            dimg[i] = ctx->images.p + off;
+            off += cnt;
+        }
+    } else {
+        for (int i = 0; i < n; ++i) dimg[i] = images[i];
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    if (tot_new) CK(ctx->rescaled.ensure(tot_new));
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        MicImage m;
+        bool copied = false;
+        int nw, nh;
+        float pn;
+        float* dst = tot_new ? ctx->rescaled.p + off : nullptr;
+        CKS(rescale_device(ctx, dimg[i], ws[i], hs[i], pxs[i], dst, &nw, &nh, &pn, &copied));
+        if (copied) {
+            m.img = dst;
+            m.pitch = nw;
+            off += (size_t)nw * nh;
+        } else {
+            m.img = dimg[i];
+            m.pitch = ws[i];
+        }
+        m.w = nw;
+        m.h = nh;
+        m.px_n = pn;
+        Layout L = tile_layout(m.w, m.h, ctx->tile);
+        if (L.ntx <= 0 || L.nty <= 0 || m.w < ctx->tile || m.h < ctx->tile)
+            return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no full tile");
+        mics.push_back(m);
+    }
+    return spectra(ctx, mics);
+}
+
+void accumulate_stage_times(gcf_ctx* ctx)
+{
+    float t;
+    if (cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]) == cudaSuccess) ctx->stage_ms[0] += t;
+    if (cudaEventElapsedTime(&t, ctx->ev[1], ctx->ev[2]) == cudaSuccess) ctx->stage_ms[1] += t;
+    if (cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev[3]) == cudaSuccess) ctx->stage_ms[2] += t;
+    if (cudaEventElapsedTime(&t, ctx->ev[3], ctx->ev[4]) == cudaSuccess) ctx->stage_ms[3] += t;
+}
+
+gcf_status full_spectra(gcf_ctx* ctx, const std::vector<int>& mics,
+                        const std::vector<gcf_result>& res, const std::vector<float>& pxn,
+                        const gcf_optics& op, float* host_out)
+{
+    int T = ctx->tile, cx = T / 2 + 1, k = (int)mics.size();
+    if (k == 0) return GCF_OK;
+    int nm = 0;
+    for (int m : mics) nm = std::max(nm, m + 1);
+    CK(ctx->moments2.ensure(2 * (size_t)nm));
+    launch_moments(ctx->ctf.p, cx * T, nm, ctx->moments2.p, ctx->st);
+    CKL();
+    std::vector<PixOptics> o(k);
+    for (int i = 0; i < k; ++i) o[i] = make_optics(op, pxn[i]);
+    CK(ctx->d_optics.ensure(k));
+    CK(ctx->mic_of.ensure(k));
+    CK(ctx->d_res.ensure(std::max<size_t>(k, ctx->d_res.n)));
+    CK(ctx->full.ensure((size_t)k * T * T));
+    CK(cudaMemcpyAsync(ctx->d_optics.p, o.data(), k * sizeof(PixOptics), cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->mic_of.p, mics.data(), k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_res.p, res.data(), k * sizeof(gcf_result), cudaMemcpyHostToDevice,
+                       ctx->st));
+    launch_full_spectrum(ctx->ctf.p, T, k, ctx->mic_of.p, ctx->d_res.p, ctx->d_optics.p,
+                         ctx->moments2.p, 0.0f, ctx->full.p, ctx->st);
+    CKL();
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(host_out, ctx->full.p, (size_t)k * T * T * sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* gcf_strerror(gcf_status s)
+{
+    switch (s) {
+    case GCF_OK: return "ok";
+    case GCF_ERR_INVALID_ARG: return "invalid argument";
+    case GCF_ERR_CUDA: return "CUDA error";
+    case GCF_ERR_CUFFT: return "cuFFT error";
+    case GCF_ERR_NO_MEMORY: return "out of memory";
+    case GCF_ERR_IMAGE_TOO_SMALL: return "image smaller than one tile";
+    case GCF_ERR_STATE: return "call out of order";
+    case GCF_ERR_IO: return "file I/O error";
+    case GCF_ERR_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+const char* gcf_last_error(gcf_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : "";
+}
+
+gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
+{
+    if (!out) return GCF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (tile_size < 16 || tile_size > 2048 || (tile_size & 1)) return GCF_ERR_INVALID_ARG;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return GCF_ERR_CUDA;
+    if (gpu < 0 || gpu >= ndev) return GCF_ERR_INVALID_ARG;
+    gcf_ctx* ctx = new gcf_ctx();
+    ctx->dev = gpu;
+    ctx->tile = tile_size;
+    ctx->log_spect = log_spect ? 1 : 0;
+    ctx->impl = GCF_SPECT_CUFFT;
+    if (cudaSetDevice(gpu) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return GCF_ERR_CUDA;
+    }
+    for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+    gcf_status s = build_tile_tables(ctx);
+    if (s != GCF_OK) {
+        gcf_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return GCF_OK;
+}
+
+void gcf_destroy(gcf_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->dev);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
+    for (auto* b : ctx->bands) {
+        b->idx.release();
+        b->a.release();
+        b->d.release();
+        b->env.release();
+        b->c2t.release();
+        b->s2t.release();
+        delete b;
+    }
+    ctx->taper.release();
+    ctx->rad_off.release();
+    ctx->rad_pix.release();
+    ctx->lp_h.release();
+    ctx->d_bands.release();
+    ctx->images.release();
+    ctx->rescaled.release();
+    ctx->tiles.release();
+    ctx->cmp.release();
+    ctx->rs_cmp.release();
+    ctx->rs_crop.release();
+    ctx->acc.release();
+    ctx->hsum.release();
+    ctx->lptmp.release();
+    ctx->moments.release();
+    ctx->moments2.release();
+    ctx->raw.release();
+    ctx->ctf0.release();
+    ctx->ctf.release();
+    ctx->radial.release();
+    ctx->band_spec.release();
+    ctx->cc_res.release();
+    ctx->full.release();
+    ctx->lowpassed.release();
+    ctx->spec_off.release();
+    ctx->mic_of.release();
+    ctx->jobs.release();
+    ctx->sum_ss.release();
+    ctx->cand.release();
+    ctx->cval.release();
+    ctx->part.release();
+    ctx->d_res.release();
+    ctx->d_optics.release();
+    for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl)
+{
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    if (impl == GCF_SPECT_CUFFT) {
+        ctx->impl = impl;
+        return GCF_OK;
+    }
+    if (impl == GCF_SPECT_FUSED && fused_tile_supported(ctx->tile)) {
+        ctx->impl = impl;
+        return GCF_OK;
+    }
+    return fail(ctx, GCF_ERR_INVALID_ARG, "spectrum implementation not available for this tile size");
+}
+
+void gcf_rescale_dims(int w, int h, float px, int* nw, int* nh, float* npx)
+{
+    // CRescaleImage::Setup (FindCTF/CRescaleImage.cpp:47-66)
+    float bin = 1.2f / px;
+    if (bin <= 1) bin = 1.0f;
+    float pxn = px * bin;
+    int a = (int)(w / bin + 0.5f), b = (int)(h / bin + 0.5f);
+    a = a / 2 * 2;
+    b = b / 2 * 2;
+    if (nw) *nw = a;
+    if (nh) *nh = b;
+    if (npx) *npx = pxn;
+}
+
+gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int w, int h, float px, int on_device,
+                       float* host_out)
+{
+    if (!ctx || !img || !host_out || w <= 0 || h <= 0 || !(px > 0)) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    const float* d = img;
+    if (!on_device) {
+        CK(ctx->images.ensure((size_t)w * h));
+        CK(cudaMemcpyAsync(ctx->images.p, img, (size_t)w * h * sizeof(float),
+                           cudaMemcpyHostToDevice, ctx->st));
+        d = ctx->images.p;
+    }
+    int nw, nh;
+    float pxn;
+    bool copied;
+    gcf_rescale_dims(w, h, px, &nw, &nh, &pxn);
+    CK(ctx->rescaled.ensure((size_t)nw * nh));
+    CKS(rescale_device(ctx, d, w, h, px, ctx->rescaled.p, &nw, &nh, &pxn, &copied));
+    if (copied) {
+        CK(cudaMemcpyAsync(host_out, ctx->rescaled.p, (size_t)nw * nh * sizeof(float),
+                           cudaMemcpyDeviceToHost, ctx->st));
+    } else {
+        CK(cudaMemcpy2DAsync(host_out, nw * sizeof(float), d, w * sizeof(float),
+                             nw * sizeof(float), nh, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_setup(gcf_ctx* ctx, const gcf_optics* optics, int width, int height)
+{
+    if (!ctx || !valid_optics(optics) || width <= 0 || height <= 0) return GCF_ERR_INVALID_ARG;
+    ctx->optics = *optics;
+    ctx->img_w = width;
+    ctx->img_h = height;
+    ctx->have_setup = true;
+    ctx->have_spectrum = false;
+    ctx->phase_deg = 0.0f;
+    ctx->phase_range = 0.0f;
+    return GCF_OK;
+}
+
+gcf_status gcf_gen_half_spectrum(gcf_ctx* ctx, const float* img, int pitch, int on_device)
+{
+    if (!ctx || !img || pitch < ctx->img_w) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_setup) return fail(ctx, GCF_ERR_STATE, "gcf_setup first");
+    CKS(set_device(ctx));
+    const float* d = img;
+    if (!on_device) {
+        CK(ctx->images.ensure((size_t)pitch * ctx->img_h));
+        CK(cudaMemcpyAsync(ctx->images.p, img, (size_t)pitch * ctx->img_h * sizeof(float),
+                           cudaMemcpyHostToDevice, ctx->st));
+        d = ctx->images.p;
+    }
+    Layout L = tile_layout(ctx->img_w, ctx->img_h, ctx->tile);
+    if (L.ntx <= 0 || L.nty <= 0 || ctx->img_w < ctx->tile || ctx->img_h < ctx->tile)
+        return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no full tile");
+    std::vector<MicImage> mics(1);
+    mics[0] = MicImage{d, ctx->img_w, ctx->img_h, pitch, ctx->optics.pixel_size};
+    CKS(spectra(ctx, mics));
+    int lp = 0;
+    CK(cudaMemcpyAsync(&lp, ctx->lowpassed.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->cur_lowpassed = lp;
+    ctx->have_spectrum = true;
+    return GCF_OK;
+}
+
+gcf_status gcf_set_phase(gcf_ctx* ctx, float phase_deg, float range_deg)
+{
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    ctx->phase_deg = phase_deg;
+    ctx->phase_range = range_deg;
+    return GCF_OK;
+}
+
+gcf_status gcf_do2d(gcf_ctx* ctx, gcf_result* out)
+{
+    if (!ctx || !out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum: call gcf_gen_half_spectrum");
+    CKS(set_device(ctx));
+    JobSpec s;
+    std::memset(&s, 0, sizeof(s));
+    s.mic = 0;
+    s.mode = 0;
+    s.optics = ctx->optics;
+    s.px_n = ctx->optics.pixel_size;
+    s.phase_deg = ctx->phase_deg;
+    s.phase_range = ctx->phase_range;
+    std::vector<gcf_result> r;
+    CKS(run_search(ctx, {s}, r));
+    *out = r[0];
+    return GCF_OK;
+}
+
+gcf_status gcf_refine(gcf_ctx* ctx, const float df[2], const float ast[2], const float ang[2],
+                      const float ph[2], gcf_result* out)
+{
+    if (!ctx || !df || !ast || !ang || !ph || !out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum: call gcf_gen_half_spectrum");
+    CKS(set_device(ctx));
+    JobSpec s;
+    std::memset(&s, 0, sizeof(s));
+    s.mic = 0;
+    s.mode = 1;
+    s.optics = ctx->optics;
+    s.px_n = ctx->optics.pixel_size;
+    float rin[8] = {df[0], df[1], ast[0], ast[1], ang[0], ang[1], ph[0], ph[1]};
+    std::memcpy(s.rin, rin, sizeof(rin));
+    std::vector<gcf_result> r;
+    CKS(run_search(ctx, {s}, r));
+    *out = r[0];
+    return GCF_OK;
+}
+
+gcf_status gcf_get_spect_size(gcf_ctx* ctx, int size[2], int half)
+{
+    if (!ctx || !size) return GCF_ERR_INVALID_ARG;
+    size[0] = ctx->tile / 2 + 1;
+    size[1] = ctx->tile;
+    if (!half) size[0] = (size[0] - 1) * 2;
+    return GCF_OK;
+}
+
+gcf_status gcf_get_half_spectrum(gcf_ctx* ctx, int raw, float* host_out)
+{
+    if (!ctx || !host_out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum");
+    CKS(set_device(ctx));
+    size_t n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
+    CK(cudaMemcpyAsync(host_out, raw ? ctx->raw.p : ctx->ctf.p, n * sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_get_radial_average(gcf_ctx* ctx, float* host_out)
+{
+    if (!ctx || !host_out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum");
+    CKS(set_device(ctx));
+    CK(cudaMemcpyAsync(host_out, ctx->radial.p, (ctx->tile / 2 + 1) * sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_gen_full_spectrum(gcf_ctx* ctx, const gcf_result* res, float* host_out)
+{
+    if (!ctx || !res || !host_out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum");
+    CKS(set_device(ctx));
+    return full_spectra(ctx, {0}, {*res}, {ctx->optics.pixel_size}, ctx->optics, host_out);
+}
+
+gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w, int h,
+                          int on_device, const gcf_optics* optics, const int* order, int is_tomo,
+                          gcf_result* results, float* full_out)
+{
+    if (!ctx || !images || n <= 0 || w <= 0 || h <= 0 || !valid_optics(optics) || !order ||
+        !results)
+        return GCF_ERR_INVALID_ARG;
+    std::vector<int> seen(n, 0);
+    for (int k = 0; k < n; ++k) {
+        if (order[k] < 0 || order[k] >= n || seen[order[k]]) return GCF_ERR_INVALID_ARG;
+        seen[order[k]] = 1;
+    }
+    for (int i = 0; i < n; ++i)
+        if (!images[i]) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    for (float& t : ctx->stage_ms) t = 0.0f;
+    ctx->launches = 0;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, ctx->st));
+    std::vector<int> ws(n, w), hs(n, h);
+    std::vector<float> pxs(n, optics->pixel_size);
+    std::vector<MicImage> mics;
+    gcf_status st = prepare_images(ctx, images, ws.data(), hs.data(), pxs.data(), n, on_device, mics);
+    if (st != GCF_OK) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        return st;
+    }
+    accumulate_stage_times(ctx);
+    float pxn = mics[0].px_n;
+    const gcf_optics op = *optics;
+    auto full_job = [&](int idx) {
+        JobSpec s;
+        std::memset(&s, 0, sizeof(s));
+        s.mic = idx;
+        s.mode = 0;
+        s.optics = op;
+        s.px_n = pxn;
+        // mProcessFull: SetPhase(extPhase[0], max(extPhase[1], 0)) (CFindSeriesCtfs.cpp:154-157)
+        s.phase_deg = op.ext_phase_deg;
+        s.phase_range = fmaxf(op.ext_phase_range, 0.0f);
+        return s;
+    };
+    auto refine_job = [&](int idx, const gcf_result& rp) {
+        // CFindSeriesCtfs::mProcessRefine (CFindSeriesCtfs.cpp:168-199)
+        JobSpec s;
+        std::memset(&s, 0, sizeof(s));
+        s.mic = idx;
+        s.mode = 1;
+        s.optics = op;
+        s.px_n = pxn;
+        float dmin = rp.df_min, dmax = rp.df_max;
+        float dfr = 5000.0f * op.pixel_size * op.pixel_size;
+        s.rin[0] = 0.5f * (dmin + dmax);
+        s.rin[1] = fmaxf(s.rin[0] * 0.5f, dfr);
+        float diff = (dmax - dmin) * 0.5f, mean = (dmax + dmin) * 0.5f;
+        s.rin[2] = mean <= 0.0f ? 0.0f : (diff / mean);
+        s.rin[4] = rp.azimuth;
+        s.rin[6] = rp.ext_phase;
+        if (!is_tomo) {
+            s.rin[3] = 0.04f;
+            s.rin[5] = 30.0f;
+            if (op.ext_phase_range > 0) s.rin[7] = 40.0f;
+        }
+        return s;
+    };
+    std::vector<gcf_result> res(n);
+    std::vector<int> ref_used(n, -1);   // ref image whose result seeded this refine
+    std::vector<gcf_result> r;
+    // package 0 of the processing order: full search
+    st = run_search(ctx, {full_job(order[0])}, r);
+    if (st != GCF_OK) goto done;
+    res[order[0]] = r[0];
+    {
+        int cur_ref = order[0];
+        int k = 1;
+        bool batch_valid = false;
+        while (k < n) {
+            if (!batch_valid) {
+                // speculative batch: refine every remaining package around cur_ref
+                std::vector<JobSpec> js;
+                for (int q = k; q < n; ++q) js.push_back(refine_job(order[q], res[cur_ref]));
+                st = run_search(ctx, js, r);
+                if (st != GCF_OK) goto done;
+                for (int q = k; q < n; ++q) {
+                    res[order[q]] = r[q - k];
+                    ref_used[order[q]] = cur_ref;
+                }
+                batch_valid = true;
+            }
+            int idx = order[k];
+            if (ref_used[idx] != cur_ref) {
+                batch_valid = false;
+                continue;
+            }
+            // mProcessPackage / mProcessRefine ref update (CFindSeriesCtfs.cpp:133-146, :200-203)
+            int new_ref = cur_ref;
+            if (res[cur_ref].score < res[idx].score) new_ref = idx;
+            if (res[idx].score <= 0) {
+                st = run_search(ctx, {full_job(idx)}, r);
+                if (st != GCF_OK) goto done;
+                res[idx] = r[0];
+                new_ref = idx;
+            }
+            if (new_ref != cur_ref) {
+                cur_ref = new_ref;
+                batch_valid = false;
+            }
+            ++k;
+        }
+    }
+    if (full_out) {
+        std::vector<int> mi(n);
+        std::vector<float> pv(n, pxn);
+        for (int i = 0; i < n; ++i) mi[i] = i;
+        st = full_spectra(ctx, mi, res, pv, op, full_out);
+        if (st != GCF_OK) goto done;
+    }
+    for (int i = 0; i < n; ++i) results[i] = res[i];
+done:
+    cudaEventRecord(t1, ctx->st);
+    cudaEventSynchronize(t1);
+    float tt = 0;
+    cudaEventElapsedTime(&tt, t0, t1);
+    ctx->stage_ms[6] = tt;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return st;
+}
+
+gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
+                         const gcf_optics* optics, gcf_result* results)
+{
+    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
+    std::vector<const float*> imgs(n);
+    std::vector<int> ws(n), hs(n);
+    std::vector<float> pxs(n);
+    for (int i = 0; i < n; ++i) {
+        if (!items[i].image || items[i].width <= 0 || items[i].height <= 0 ||
+            !(items[i].pixel_size > 0))
+            return GCF_ERR_INVALID_ARG;
+        imgs[i] = items[i].image;
+        ws[i] = items[i].width;
+        hs[i] = items[i].height;
+        pxs[i] = items[i].pixel_size;
+    }
+    CKS(set_device(ctx));
+    for (float& t : ctx->stage_ms) t = 0.0f;
+    ctx->launches = 0;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, ctx->st));
+    std::vector<MicImage> mics;
+    gcf_status st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics);
+    if (st == GCF_OK) {
+        accumulate_stage_times(ctx);
+        std::vector<JobSpec> js(n);
+        for (int i = 0; i < n; ++i) {
+            std::memset(&js[i], 0, sizeof(JobSpec));
+            js[i].mic = i;
+            js[i].mode = 0;
+            js[i].optics = *optics;
+            js[i].optics.pixel_size = pxs[i];
+            js[i].px_n = mics[i].px_n;
+            js[i].phase_deg = optics->ext_phase_deg;
+            js[i].phase_range = fmaxf(optics->ext_phase_range, 0.0f);
+        }
+        std::vector<gcf_result> r;
+        st = run_search(ctx, js, r);
+        if (st == GCF_OK)
+            for (int i = 0; i < n; ++i) results[i] = r[i];
+    }
+    cudaEventRecord(t1, ctx->st);
+    cudaEventSynchronize(t1);
+    float tt = 0;
+    cudaEventElapsedTime(&tt, t0, t1);
+    ctx->stage_ms[6] = tt;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return st;
+}
+
+gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7])
+{
+    if (!ctx || !times_ms) return GCF_ERR_INVALID_ARG;
+    for (int i = 0; i < 7; ++i) times_ms[i] = ctx->stage_ms[i];
+    return GCF_OK;
+}
+
+gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count)
+{
+    if (!ctx || !count) return GCF_ERR_INVALID_ARG;
+    *count = ctx->launches;
+    return GCF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,624 @@
+// gcf_control.cu -- device-resident control of the CTF search.
+//
+// The reference drives every candidate from the host with a synchronous
+// readback (FindCTF/CFindDefocus1D.cpp:76-137, FindCTF/CFindDefocus2D.cpp:153-380).
+// Here the whole control flow lives on the GPU:
+//   k_search1d : radial average -> 1D brute force -> 1D refine -> 2D init,
+//                one CTA per Do2D job (CFindCtf1D::Do1D, FindCTF/CFindCtf1D.cpp:49-111);
+//   k_update2d : reduce the candidate partial sums of the pending line
+//                search, take the first strict maximum, advance the
+//                CFindDefocus2D::mIterate state machine and write the next
+//                candidate set, one CTA per job.
+// The host only enqueues (eval, update) pairs; no value comes back until
+// the search is over.
+//
+// Compiled with -fmad=false: every float step/range expression is rounded
+// operation by operation like the reference's host code, so candidate grids
+// coincide with the reference and with the oracle.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "gcf_internal.h"
+
+namespace gcf {
+
+namespace {
+
+constexpr float kD2R2D = 0.01745329f;   // FindCTF/CFindDefocus2D.cpp:11
+constexpr float kD2R1D = 0.0174533f;    // FindCTF/CFindDefocus1D.cpp:11
+constexpr double kPi = 3.14159265358979323846;
+
+struct Cand {
+    float ast, ang, phase, dfmean;
+};
+
+// Candidate -> (mean px, sigma*cos 2a, sigma*sin 2a, add/pi); mCorrelate +
+// GCalcCTF2D::DoIt (FindCTF/CFindDefocus2D.cpp:363-380, FindCTF/GCalcCTF2D.cu:117-132).
+__device__ float4 cand_params(const Cand& c, const PixOptics& o)
+{
+    float ph = c.phase * kD2R2D;
+    float az = c.ang * kD2R2D;
+    float dmin = c.dfmean * (1.0f - c.ast) / o.px;
+    float dmax = c.dfmean * (1.0f + c.ast) / o.px;
+    float mean = 0.5f * (dmin + dmax);
+    float sig = 0.5f * (dmax - dmin);
+    float add = o.amp_phase + ph;
+    double a2 = 2.0 * (double)az;
+    float4 q;
+    q.x = mean;
+    q.y = (float)((double)sig * cos(a2));
+    q.z = (float)((double)sig * sin(a2));
+    q.w = (float)((double)add / kPi);
+    return q;
+}
+
+// Candidate i of the pending step of job J.
+__device__ Cand cand_of(const SearchJob& J, int i, const float2* cval)
+{
+    Cand c{J.ast_ratio, J.ast_angle, J.ext_phase, J.df_mean};
+    switch (J.step) {
+    case STEP_CC0:
+        break;
+    case STEP_ASTIG: {
+        int jj = i / J.gen_n1, ii = i - jj * J.gen_n1;
+        c.ast = J.gen_lo + ii * J.gen_step;
+        c.ang = J.gen_lo2 + jj * J.gen_step2;
+        break;
+    }
+    case STEP_ASTMAG:
+        c.ast = J.gen_lo + i * J.gen_step;
+        break;
+    case STEP_ASTANG:
+        c.ang = J.gen_lo + i * J.gen_step;
+        break;
+    case STEP_DFMEAN:
+        c.dfmean = J.gen_lo + i * J.gen_step;
+        break;
+    case STEP_PHASE:
+        c.phase = cval[i].x;
+        break;
+    default:
+        break;
+    }
+    return c;
+}
+
+__device__ __forceinline__ float iter_scale(int i)
+{
+    const int iters = 20;
+    return 1.0f - i * 0.5f / iters;   // FindCTF/CFindDefocus2D.cpp:167
+}
+
+// Sets the generator of J.step and returns its candidate count (0 where the
+// reference returns early).  Phase candidates are compacted into cval.
+__device__ int prepare_step(SearchJob& J, float2* cval)
+{
+    switch (J.step) {
+    case STEP_CC0:
+        return 1;
+    case STEP_ASTIG: {   // mFindAstig, :185-199
+        float tiny = (float)1e-20;
+        float ar = J.ast_range[1] - J.ast_range[0];
+        float gr = J.ang_range[1] - J.ang_range[0];
+        if (ar < tiny && gr < tiny) return 0;
+        int ns = 51, ng = 51;
+        float as = ar / ns, gs = gr / ng;
+        if ((double)as < 1e-5) ns = 1;
+        if ((double)gs < 1e-5) ng = 1;
+        if (ns == 1 && ng == 1) return 0;
+        J.gen_lo = J.ast_range[0];
+        J.gen_step = as;
+        J.gen_n1 = ns;
+        J.gen_lo2 = J.ang_range[0];
+        J.gen_step2 = gs;
+        J.gen_n2 = ng;
+        return ns * ng;
+    }
+    case STEP_ASTMAG: {   // mRefineAstMag, :224-236
+        float range = iter_scale(J.iter) * J.range_ast;
+        if (range < (float)1e-20) return 0;
+        float lo = fmaxf(J.ast_ratio - range * 0.5f, J.ast_range[0]);
+        float hi = fminf(J.ast_ratio + range * 0.5f, J.ast_range[1]);
+        int n = 21;
+        float step = (hi - lo) / (n - 1);
+        if (step < 0.001f) step = 0.001f;
+        n = (int)((hi - lo) / step) / 2 * 2 + 1;
+        if (n == 1) return 0;
+        J.gen_lo = lo;
+        J.gen_step = step;
+        return n;
+    }
+    case STEP_ASTANG: {   // mRefineAstAng, :256-268
+        float range = iter_scale(J.iter) * J.range_ang;
+        if (range < (float)1e-20) return 0;
+        float lo = fmaxf(J.ast_angle - range * 0.5f, J.ang_range[0]);
+        float hi = fminf(J.ast_angle + range * 0.5f, J.ang_range[1]);
+        int n = 51;
+        float step = (hi - lo) / (n - 1);
+        if (step < 1.0f) step = 1.0f;
+        n = (int)((hi - lo) / step) / 2 * 2 + 1;
+        if (n == 1) return 0;
+        J.gen_lo = lo;
+        J.gen_step = step;
+        return n;
+    }
+    case STEP_DFMEAN: {   // mRefineDfMean, :288-301
+        float range = iter_scale(J.iter) * J.range_df;
+        if (range < (float)1e-30) return 0;
+        int n = 31;
+        float lo = fmaxf(J.df_mean - range * 0.5f, J.df_range[0]);
+        float hi = fminf(J.df_mean + range * 0.5f, J.df_range[1]);
+        float step = (hi - lo) / n;
+        if (step < 20) step = 20.0f;
+        n = (int)((hi - lo) / step) / 2 * 2 + 1;
+        if (n == 1) return 0;
+        J.gen_lo = lo;
+        J.gen_step = step;
+        return n;
+    }
+    case STEP_PHASE: {   // mRefinePhase, :324-347
+        float range = iter_scale(J.iter) * J.phase_range[1];
+        if (range < (float)1e-30) return 0;
+        int n = 61;
+        float step = range / n;
+        if (step < 0.03f) return 0;
+        if (step > 1.0f) {
+            step = 1.0f;
+            n = (int)(range / step);
+            n = n / 2 * 2 + 1;
+        }
+        float pmin = J.phase_range[0] - J.phase_range[1] * 0.5f;
+        float pmax = J.phase_range[0] + J.phase_range[1] * 0.5f;
+        if (pmin < 0) pmin = 0.0f;
+        if (pmax > 150) pmax = 150.0f;
+        int k = 0;
+        for (int i = 0; i < n && k < kMaxCand; ++i) {
+            float ph = J.ext_phase + (i - n / 2) * step;
+            if (ph < pmin || ph > pmax) continue;
+            cval[k++] = make_float2(ph, 0.0f);
+        }
+        return k;
+    }
+    default:
+        return 0;
+    }
+}
+
+// Applies the outcome of the pending step (best CC `best` at candidate
+// `bi`, best = -1e20 when the step had no candidates) and moves J.step on.
+__device__ void finish_step(SearchJob& J, float best, int bi, float cc0, const float2* cval)
+{
+    switch (J.step) {
+    case STEP_CC0:   // mIterate, :155-156
+        J.cc_max = cc0;
+        J.old_cc = cc0;
+        J.step = STEP_ASTIG;
+        return;
+    case STEP_ASTIG: {   // :214-221, then mIterate :159-165
+        if (bi >= 0 && best > J.cc_max) {
+            Cand c = cand_of(J, bi, cval);
+            J.ast_ratio = c.ast;
+            J.ast_angle = c.ang;
+            J.cc_max = best;
+        }
+        if (J.old_cc > J.cc_max) {
+            J.step = STEP_DONE;
+            return;
+        }
+        J.ext_phase = J.phase_range[0];
+        J.range_df = J.df_range[1] - J.df_range[0];
+        J.range_ast = J.ast_range[1] - J.ast_range[0];
+        J.range_ang = J.ang_range[1] - J.ang_range[0];
+        J.iter = 1;
+        J.step = STEP_ASTMAG;
+        return;
+    }
+    case STEP_ASTMAG:   // :248-253, then mIterate :171-173
+        if (bi >= 0 && best > J.cc_max) {
+            J.ast_ratio = cand_of(J, bi, cval).ast;
+            J.cc_max = best;
+        }
+        if (J.old_cc > J.cc_max) {
+            J.step = STEP_DONE;
+            return;
+        }
+        J.cc_max = J.old_cc;
+        J.step = STEP_ASTANG;
+        return;
+    case STEP_ASTANG:   // :280-285
+        if (bi >= 0 && best > J.cc_max) {
+            J.ast_angle = cand_of(J, bi, cval).ang;
+            J.cc_max = best;
+        }
+        J.step = STEP_DFMEAN;
+        return;
+    case STEP_DFMEAN:   // :313-321
+        if (bi >= 0 && best > J.cc_max) {
+            J.df_mean = cand_of(J, bi, cval).dfmean;
+            J.cc_max = best;
+        }
+        J.step = STEP_PHASE;
+        return;
+    case STEP_PHASE:   // :355-360
+        if (bi >= 0 && best > J.cc_max) {
+            J.ext_phase = cand_of(J, bi, cval).phase;
+            J.cc_max = best;
+        }
+        J.iter += 1;
+        J.step = (J.iter < 20) ? STEP_ASTMAG : STEP_DONE;
+        return;
+    default:
+        J.step = STEP_DONE;
+        return;
+    }
+}
+
+// Advance past steps without candidates; returns the pending count.
+__device__ int advance(SearchJob& J, float2* cval)
+{
+    while (J.step != STEP_DONE) {
+        int n = prepare_step(J, cval);
+        if (n > 0) return n;
+        finish_step(J, (float)-1e20, -1, 0.0f, cval);
+    }
+    return 0;
+}
+
+// Argmax with the reference's tie rule (first strict maximum in index
+// order, starting from -1e20; NaN never wins).
+struct ArgMax {
+    float v;
+    int i;
+};
+
+__device__ __forceinline__ ArgMax better(ArgMax a, ArgMax b)
+{
+    if (b.i < 0) return a;
+    if (a.i < 0) return b;
+    if (b.v > a.v) return b;
+    if (a.v > b.v) return a;
+    return (b.i < a.i) ? b : a;
+}
+
+__device__ ArgMax block_argmax(ArgMax m, ArgMax* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        ArgMax t;
+        t.v = __shfl_xor_sync(0xffffffffu, m.v, o);
+        t.i = __shfl_xor_sync(0xffffffffu, m.i, o);
+        m = better(m, t);
+    }
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) sh[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        ArgMax t = lane < nw ? sh[lane] : ArgMax{0.0f, -1};
+        for (int o = 16; o > 0; o >>= 1) {
+            ArgMax u;
+            u.v = __shfl_xor_sync(0xffffffffu, t.v, o);
+            u.i = __shfl_xor_sync(0xffffffffu, t.i, o);
+            t = better(t, u);
+        }
+        if (lane == 0) sh[0] = t;
+    }
+    __syncthreads();
+    ArgMax r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ void write_candidates(const SearchJob& J, int n, float4* cand, float2* cval)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        Cand c = cand_of(J, i, cval);
+        cand[i] = cand_params(c, J.o);
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_update2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands,
+                           const double* __restrict__ sum_ss, float4* __restrict__ cand,
+                           float2* __restrict__ cval, const double2* __restrict__ part,
+                           int max_chunks, int init)
+{
+    __shared__ SearchJob sJ;
+    __shared__ ArgMax shm[32];
+    __shared__ float s_cc0;
+    __shared__ int s_n;
+    const int j = blockIdx.x;
+    if (threadIdx.x == 0) sJ = jobs[j];
+    __syncthreads();
+    float4* cj = cand + (size_t)j * kMaxCand;
+    float2* vj = cval + (size_t)j * kMaxCand;
+    if (init) {
+        // fresh job: pending step is CC0 with one candidate
+        if (threadIdx.x == 0) {
+            sJ.step = STEP_CC0;
+            s_n = advance(sJ, vj);
+            sJ.ncand = s_n;
+            jobs[j] = sJ;
+        }
+        __syncthreads();
+        write_candidates(sJ, s_n, cj, vj);
+        return;
+    }
+    if (sJ.step == STEP_DONE) return;
+    const int n = sJ.ncand;
+    const BandDev b = bands[sJ.band];
+    const int nch = (b.n + kEvalChunk - 1) / kEvalChunk;
+    const double ss = sum_ss[j];
+    ArgMax m{(float)-1e20, -1};
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        const double2* p = part + ((size_t)j * kMaxCand + c) * max_chunks;
+        double cs = 0.0, cc = 0.0;
+        for (int k = 0; k < nch; ++k) {
+            double2 v = p[k];
+            cs += v.x;
+            cc += v.y;
+        }
+        double d = sqrt(cc * ss);
+        float ccv = (d == 0.0) ? 0.0f : (float)(cs / d);   // GCC2D mGCalc1D, FindCTF/GCC2D.cu:81-87
+        if (c == 0) s_cc0 = ccv;
+        if (ccv > m.v) m = ArgMax{ccv, c};   // strict, in index order per thread
+    }
+    __syncthreads();
+    m = block_argmax(m, shm);
+    if (threadIdx.x == 0) {
+        finish_step(sJ, m.i >= 0 ? m.v : (float)-1e20, m.i, s_cc0, vj);
+        s_n = advance(sJ, vj);
+        sJ.ncand = s_n;
+        jobs[j] = sJ;
+    }
+    __syncthreads();
+    write_candidates(sJ, s_n, cj, vj);
+}
+
+// ---------------------------------------------------------------------------
+// 1D search.  Bin data of GCalcCTF1D/GCC1D (FindCTF/GCalcCTF1D.cu:17-33,
+// FindCTF/GCC1D.cu:15-65) in the same turns formulation as the 2D kernel.
+struct Bins1D {
+    float a[kMax1DBins], d[kMax1DBins], env[kMax1DBins], s[kMax1DBins];
+};
+
+struct Brute {
+    float df, ph, cc;
+};
+
+__device__ Brute brute_1d(const Bins1D& B, int lo_bin, int hi_bin, double ss, const PixOptics& o,
+                          const float dfr[2], const float phr[2], ArgMax* shm)
+{
+    // CFindDefocus1D::mBrutalForceSearch (FindCTF/CFindDefocus1D.cpp:76-119)
+    int ndf = 501;
+    float dfrange = dfr[1] - dfr[0];
+    float dfs = dfrange / (ndf - 1);
+    if (dfs < 10) dfs = 10.0f;
+    ndf = (int)(dfrange / dfs) / 2 * 2 + 1;
+    int nps = 37;
+    float psr = phr[1] - phr[0];
+    float pss = psr / (nps - 1);
+    if (pss == 0) nps = 1;
+    else nps = (int)(psr / pss) / 2 * 2 + 1;
+    int npts = ndf * nps;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    ArgMax m{(float)-1e20, -1};
+    for (int i = warp; i < npts; i += nw) {
+        int f = i % ndf, p = i / ndf;
+        float df = dfr[0] + f * dfs;
+        float ph = phr[0] + p * pss;
+        if (ph < 0) ph = 0.0f;
+        else if (ph > 150.0f) ph = 150.0f;
+        float pdf = df / o.px;
+        float add = o.amp_phase + ph * kD2R1D;
+        float tw = (float)((double)add / kPi);
+        float cs = 0.f, cc = 0.f;
+        for (int x = lo_bin + lane; x < hi_bin; x += 32) {
+            float t = B.a[x] * pdf + B.d[x] + tw;
+            float r = t - rintf(t);
+            float sv = __sinf(r * 3.14159265358979f);
+            float C = (fabsf(sv) - 0.5f) * B.env[x];
+            cs += C * B.s[x];
+            cc += C * C;
+        }
+        double dcs = cs, dcc = cc;
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+            dcs += __shfl_xor_sync(0xffffffffu, dcs, o2);
+            dcc += __shfl_xor_sync(0xffffffffu, dcc, o2);
+        }
+        float v = (dcc > 0 && ss > 0) ? (float)(dcs / sqrt(dcc * ss)) : 0.0f;
+        if (v > m.v) m = ArgMax{v, i};
+    }
+    __syncthreads();
+    m = block_argmax(m, shm);
+    Brute r{0.0f, 0.0f, (float)-1e20};
+    if (m.i >= 0) {
+        int f = m.i % ndf, p = m.i / ndf;
+        float ph = phr[0] + p * pss;
+        if (ph < 0) ph = 0.0f;
+        else if (ph > 150.0f) ph = 150.0f;
+        r.df = dfr[0] + f * dfs;
+        r.ph = ph;
+        r.cc = m.v;
+    }
+    return r;
+}
+
+__global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict__ radial, int cx,
+                           float4* __restrict__ cand, float2* __restrict__ cval)
+{
+    extern __shared__ unsigned char smem_raw[];
+    Bins1D& B = *reinterpret_cast<Bins1D*>(smem_raw);
+    __shared__ ArgMax shm[32];
+    __shared__ double s_ss;
+    __shared__ SearchJob sJ;
+    const int j = blockIdx.x;
+    if (threadIdx.x == 0) sJ = jobs[j];
+    __syncthreads();
+    if (sJ.mode != 0) return;
+    const PixOptics o = sJ.o;
+    const float* rad = radial + (size_t)sJ.mic * cx;
+    // CFindDefocus1D::mCorrelate band (FindCTF/CFindDefocus1D.cpp:128-137)
+    float r0 = 25.0f * o.px, r1 = (2.0f * o.px) / 0.8f;
+    if (r1 < 3.5f) r1 = 3.5f;
+    float res1 = ((cx - 1) * 2) * o.px;
+    float flo = res1 / r0, fhi = res1 / r1;
+    int lo_bin = cx, hi_bin = 0;
+    for (int x = 0; x < cx; ++x) {
+        if ((float)x >= flo && (float)x < fhi) {
+            if (x < lo_bin) lo_bin = x;
+            hi_bin = x + 1;
+        }
+    }
+    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
+        double s = (x * 0.5) / (cx - 1.0);
+        double s2 = s * s;
+        double f = x / (cx - 1.0);
+        B.a[x] = (float)((double)o.wl * s2);
+        B.d[x] = (float)(-0.5 * (double)o.wl * o.wl * o.wl * s2 * s2 * o.cs);
+        B.env[x] = (float)exp(-f * f);
+        B.s[x] = rad[x];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double ss = 0.0;
+        for (int x = lo_bin + (int)threadIdx.x; x < hi_bin; x += 32) ss += (double)B.s[x] * B.s[x];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o2);
+        if (threadIdx.x == 0) s_ss = ss;
+    }
+    __syncthreads();
+    const double ss = s_ss;
+    // CFindCtf1D::mFindDefocus (FindCTF/CFindCtf1D.cpp:73-90)
+    float ext = sJ.ext_phase_in, prange = sJ.phase_range_in;
+    float px2 = o.px * o.px;
+    float dfr[2] = {3000.0f * px2, 30000.0f * px2};
+    float phr[2];
+    phr[0] = fmaxf(ext - prange / 2, 0.0f);
+    phr[1] = fminf(phr[0] + prange, 150.0f);
+    Brute b1 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr, phr, shm);
+    // CFindCtf1D::mRefineDefocus (FindCTF/CFindCtf1D.cpp:92-111)
+    float range = fmaxf(0.3f * b1.df, 3000.0f);
+    float mindf = 3000.0f * o.px * o.px;
+    float dfr2[2];
+    dfr2[0] = fmaxf(b1.df - range / 2, mindf);
+    dfr2[1] = dfr2[0] + range;
+    float pr = 0.2f * prange;
+    float phr2[2];
+    phr2[0] = fmaxf(b1.ph - pr / 2, 0.0f);
+    phr2[1] = fminf(0.0f + pr, 150.0f);   // the reference reads the zero-initialised bound
+    Brute b2 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr2, phr2, shm);
+    float2* vj = cval + (size_t)j * kMaxCand;
+    __shared__ int s_n;
+    if (threadIdx.x == 0) {
+        sJ.df_1d = b2.df;
+        sJ.phase_1d = b2.ph;
+        sJ.score_1d = b2.cc;
+        // CFindCtf2D::Do2D + CFindDefocus2D::Setup3/DoIt (FindCTF/CFindCtf2D.cpp:44-53,
+        // FindCTF/CFindDefocus2D.cpp:98-124)
+        float mu = (b2.df + b2.df) * 0.5f;
+        sJ.df_mean = mu;
+        sJ.ast_ratio = 0.0f;
+        sJ.ast_angle = 0.0f;
+        sJ.phase_range[0] = b2.ph;
+        sJ.phase_range[1] = prange;
+        sJ.ext_phase = b2.ph;
+        sJ.df_range[0] = mu * 0.9f;
+        sJ.df_range[1] = mu * 1.1f;
+        sJ.ast_range[0] = 0.0f;
+        sJ.ast_range[1] = 0.06f;
+        sJ.ang_range[0] = -90.0f;
+        sJ.ang_range[1] = 90.0f;
+        sJ.step = STEP_CC0;
+        s_n = advance(sJ, vj);
+        sJ.ncand = s_n;
+        jobs[j] = sJ;
+    }
+    __syncthreads();
+    write_candidates(sJ, s_n, cand + (size_t)j * kMaxCand, vj);
+}
+
+// Shell choice of GSpectralCC2D::DoIt (FindCTF/GSpectralCC2D.cu:144-172) and
+// CFindDefocus2D::mCalcCtfRes (FindCTF/CFindDefocus2D.cpp:382-400).
+__global__ void k_shell_select(SearchJob* __restrict__ jobs, int njobs, const float* __restrict__ cc,
+                               int cx, int cy)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const float* c = cc + (size_t)j * cx;
+    int imax = 1;
+    float fmx = (float)-1e30;
+    for (int i = 1; i < cx; ++i) {
+        if (c[i] <= fmx) continue;
+        fmx = c[i];
+        imax = i;
+    }
+    int shell = imax;
+    if (!(fmx < 0.143f)) {
+        for (int i = imax; i < cx; ++i) {
+            if (c[i] < 0.143f) break;
+            shell = i;
+        }
+    }
+    jobs[j].ctf_res = cy * jobs[j].o.px / shell;
+}
+
+// CFindCtf2D::mGetResults (FindCTF/CFindCtf2D.cpp:68-76) and the getters
+// of CFindDefocus2D (FindCTF/CFindDefocus2D.cpp:38-68).
+__global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const int* __restrict__ lowpassed,
+                          gcf_result* __restrict__ out)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const SearchJob& J = jobs[j];
+    gcf_result r;
+    r.df_min = J.df_mean * (1.0f - J.ast_ratio);
+    r.df_max = J.df_mean * (1.0f + J.ast_ratio);
+    r.azimuth = J.ast_angle;
+    r.ext_phase = J.ext_phase;
+    r.score = J.cc_max;
+    r.ctf_res = J.ctf_res;
+    r.df_1d = J.mode == 0 ? J.df_1d : 0.0f;
+    r.phase_1d = J.mode == 0 ? J.phase_1d : 0.0f;
+    r.score_1d = J.mode == 0 ? J.score_1d : 0.0f;
+    r.lowpassed = lowpassed ? lowpassed[J.mic] : 0;
+    out[j] = r;
+}
+
+}  // namespace
+
+void launch_update2d(const EvalArgs& a, cudaStream_t st)
+{
+    if (a.njobs <= 0) return;
+    k_update2d<<<a.njobs, 256, 0, st>>>(a.jobs, a.bands, a.sum_ss, a.cand, a.cval, a.part,
+                                        a.max_chunks, 0);
+}
+
+void launch_init_jobs(const EvalArgs& a, cudaStream_t st)
+{
+    if (a.njobs <= 0) return;
+    k_update2d<<<a.njobs, 256, 0, st>>>(a.jobs, a.bands, a.sum_ss, a.cand, a.cval, a.part,
+                                        a.max_chunks, 1);
+}
+
+void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, float4* cand,
+                     float2* cval, cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    size_t sm = sizeof(Bins1D);   // 16.4 KB, below the default dynamic limit
+    k_search1d<<<njobs, 256, sm, st>>>(jobs, radial, cx, cand, cval);
+}
+
+void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, int cy,
+                         cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    k_shell_select<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, cc, cx, cy);
+}
+
+void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out,
+                    cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    k_results<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, lowpassed, out);
+}
+
+}  // namespace gcf

@@ -1,0 +1,162 @@
+// gcf_internal.h -- shared definitions of the B200 CTF-estimation library.
+//
+// Data layout in HBM (per context):
+//   images     : dense float, width x height per micrograph (row pitch = width)
+//   raw / ctf  : per micrograph a (tile/2+1) x tile float half spectrum,
+//                row-major with cmpX = tile/2+1 floats per row and the DC at
+//                (x = 0, y = tile/2), the layout of GCalcSpectrum
+//                (FindCTF/GCalcSpectrum.cu:8-31)
+//   band       : per (tile, pixel size, optics) the in-band pixels of the 2D
+//                correlation as structure-of-arrays (index, a, d, envelope,
+//                cos 2theta, sin 2theta) so the candidate kernel streams them
+//   jobs       : one SearchJob per micrograph being searched
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/gctf_b200.h"
+
+namespace gcf {
+
+constexpr int kMaxCand = 2624;        // >= 51 * 51 astigmatism grid
+constexpr int kEvalThreads = 256;     // threads of the candidate kernel
+constexpr int kEvalPPT = 8;           // band pixels per thread per chunk
+constexpr int kEvalChunk = kEvalThreads * kEvalPPT;
+constexpr int kEvalCB = 16;           // candidates per CTA
+constexpr int kMax1DBins = 1025;      // tile <= 2048
+
+// Search step kinds (CFindDefocus2D::mIterate, FindCTF/CFindDefocus2D.cpp:153-183)
+enum StepKind : int {
+    STEP_CC0 = 0,
+    STEP_ASTIG = 1,
+    STEP_ASTMAG = 2,
+    STEP_ASTANG = 3,
+    STEP_DFMEAN = 4,
+    STEP_PHASE = 5,
+    STEP_DONE = 6
+};
+
+// Optics in pixel units (CCTFTheory::Setup, FindCTF/CCTFTheory.cpp:69-86).
+struct PixOptics {
+    float wl;         // wavelength, pixels
+    float cs;         // Cs, pixels
+    float amp_phase;  // radian (GCalcCTF2D::SetParam, FindCTF/GCalcCTF2D.cu:99-104)
+    float px;         // Angstrom / pixel
+};
+
+// Per-job search state: the members of CFindDefocus2D plus the position in
+// the mIterate sequence.  Lives in device memory; the update kernel owns it.
+struct SearchJob {
+    // inputs
+    int mic;            // spectrum slot
+    int band;           // band-table slot
+    int mode;           // 0 = Do2D (after the 1D search), 1 = Refine
+    int pad0;
+    PixOptics o;
+    float phase_range_in;   // CFindCtfBase::m_fPhaseRange (Do2D)
+    float ext_phase_in;     // CFindCtfBase::m_fExtPhase   (Do2D)
+    float res_lo, res_hi;   // 1D band, Fourier pixels [lo, hi)
+    // CFindDefocus2D state
+    float df_mean, ast_ratio, ast_angle, ext_phase, cc_max, old_cc;
+    float phase_range[2], df_range[2], ast_range[2], ang_range[2];
+    float range_df, range_ast, range_ang;  // full ranges captured by mIterate
+    int iter;
+    int step;           // StepKind of the pending candidate set
+    int ncand;          // candidates of the pending step
+    // generator of the pending step
+    float gen_lo, gen_step;
+    int gen_n1, gen_n2;
+    float gen_lo2, gen_step2;
+    // results
+    float df_1d, phase_1d, score_1d;
+    float ctf_res;
+    int lowpassed;
+    int pad1[3];
+};
+
+// Per-band device pointers (structure of arrays).
+struct BandDev {
+    int n;
+    int cx, cy;
+    int pad;
+    const int* idx;
+    const float* a;     // wl * s^2                     (turns / pixel defocus)
+    const float* d;     // -0.5 * wl^3 * s^4 * Cs       (turns)
+    const float* env;   // exp(-16 s^2)
+    const float* c2t;   // cos(2 theta)
+    const float* s2t;   // sin(2 theta)
+};
+
+// Arguments of the 2D candidate kernels.
+struct EvalArgs {
+    SearchJob* jobs;
+    const BandDev* bands;
+    const float* band_spec;     // [job][band pixels] spectrum gathered in band order
+    const double* sum_ss;       // [job] sum of S^2 over the band
+    const int* spec_off;        // [job] offset of the job's band spectrum
+    float4* cand;               // [job][kMaxCand] (mean_px, sig*cos2a, sig*sin2a, phase/pi)
+    float2* cval;               // [job][kMaxCand] searched parameter values
+    double2* part;              // [job][kMaxCand][max_chunks] (sum CS, sum CC)
+    int max_chunks;
+    int njobs;
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (defined in the .cu units).  All enqueue on `st`.
+// ---------------------------------------------------------------------------
+
+// gcf_spectrum.cu
+void launch_extract_tiles(const float* img, int w, int h, int pitch, int tile, int ntx,
+                          int offx, int offy, int stride, int first_tile, int ntiles,
+                          const float* taper, float* out, cudaStream_t st);
+void launch_amp_accumulate(const float2* cmp, int tile, int ntiles, double* acc, cudaStream_t st);
+void launch_finalize_raw(const double* acc, int n, double inv, float* raw, cudaStream_t st);
+void launch_fourier_crop(const float2* in, int cx_in, int cy_in, float2* out, int cx_out,
+                         int cy_out, cudaStream_t st);
+int  fused_tile_supported(int tile);
+// Fused spectrum: one pass over all tiles of `nimg` images described by
+// `descs` (device), accumulating the averaged amplitude spectrum into raw.
+struct TileImage {
+    const float* img;
+    int pitch;
+    int ntx, nty;
+    int offx, offy, stride;
+    int tile_base;      // first global tile index of this image
+    float inv_ntiles;
+};
+void launch_fused_spectrum(const TileImage* descs, int nimg, int total_tiles, int tile,
+                           const float* taper, const float2* taper_hat, float* raw_out,
+                           float* scratch, int grid, cudaStream_t st);
+
+// gcf_post.cu
+void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,
+                          cudaStream_t st);
+void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic, int log_spect,
+                        float* ctf, cudaStream_t st);
+void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st);
+void launch_lowpass(const float* in, int tile, int nmic, const double* moments, const double* h,
+                    int radius, double* tmp, float* out, int* lowpassed, cudaStream_t st);
+void launch_radial(const float* spect, int tile, int nmic, const int* off, const int* pix,
+                   float* radial, cudaStream_t st);
+void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, const BandDev* bands,
+                        const int* spec_off, int njobs, float* band_spec, double* sum_ss,
+                        cudaStream_t st);
+void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_of,
+                          const gcf_result* res, const PixOptics* o, const double* moments,
+                          float res_lo_freq_dummy, float* full, cudaStream_t st);
+void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, float* cc,
+                    cudaStream_t st);
+
+// gcf_search.cu (candidate kernel) and gcf_control.cu (state machine)
+void launch_eval2d(const EvalArgs& a, int cand_blocks, int max_band_n, cudaStream_t st);
+void launch_update2d(const EvalArgs& a, cudaStream_t st);
+void launch_init_jobs(const EvalArgs& a, cudaStream_t st);
+void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, float4* cand,
+                     float2* cval, cudaStream_t st);
+void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, int cy,
+                         cudaStream_t st);
+void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out,
+                    cudaStream_t st);
+
+}  // namespace gcf

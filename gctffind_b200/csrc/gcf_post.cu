@@ -1,0 +1,423 @@
+// gcf_post.cu -- spectrum post-processing on the averaged half spectrum:
+// background removal (GRmBackground2D), moments and B-factor lowpass
+// (CFindCtfBase::mRemoveBackground/mLowpass), radial average (GRadialAvg),
+// gathering of the in-band pixels for the candidate kernels, the diagnostic
+// full spectrum (CSpectrumImage, GCalcCTF2D::EmbedCtf) and the spectral-CC
+// resolution (GSpectralCC2D).
+//
+// Compiled with -fmad=false: the float expressions that decide masks and
+// bands are rounded operation by operation, like the oracle.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "gcf_internal.h"
+
+namespace gcf {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /* 32*NV */)
+{
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        v[k] = warp_sum(v[k]);
+        if (lane == 0) sh[k * 32 + warp] = v[k];
+    }
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = lane < nw ? sh[k * 32 + lane] : 0.0;
+            t = warp_sum(t);
+            if (lane == 0) sh[k * 32] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = sh[k * 32];
+    __syncthreads();
+}
+
+// Value of the background plane at relative position (u, R): the Hermitian
+// fold of GRmBackground2D::mGRemove (FindCTF/GRmBackground2D.cu:42-64).
+__device__ __forceinline__ float bg_val(const float* row, const float* mrow, int u, int half_x,
+                                        int tile)
+{
+    if (u >= half_x) u -= 2 * half_x;
+    (void)tile;
+    return (u >= 0) ? row[u] : mrow[-u];
+}
+
+// Horizontal box sums of sqrt(raw) (or raw if log_spect) for every row and
+// every output column x in [0, cx).
+__global__ void k_bg_horizontal(const float* __restrict__ raw, int tile, int log_spect, int box,
+                                double* __restrict__ hsum)
+{
+    extern __shared__ float sh[];
+    int cx = tile / 2 + 1, half_x = cx - 1;
+    int R = blockIdx.x, m = blockIdx.y;
+    int mr = (tile - R) % tile;   // half_y - (R - half_y) modulo tile
+    const float* src = raw + (size_t)m * cx * tile;
+    float* row = sh;
+    float* mrow = sh + cx;
+    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
+        float a = src[(size_t)R * cx + x], b = src[(size_t)mr * cx + x];
+        row[x] = log_spect ? a : sqrtf(a);
+        mrow[x] = log_spect ? b : sqrtf(b);
+    }
+    __syncthreads();
+    int hb = box / 2;
+    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
+        double s = 0.0;
+        for (int j = -hb; j <= hb; ++j) s += (double)bg_val(row, mrow, x + j, half_x, tile);
+        hsum[((size_t)m * tile + R) * cx + x] = s;
+    }
+}
+
+// Vertical box sums, DC mask (fR < 0.04) and subtraction
+// (FindCTF/GRmBackground2D.cu:18-31, :67-69).
+__global__ void k_bg_vertical(const float* __restrict__ raw, const double* __restrict__ hsum,
+                              int tile, int log_spect, int box, float* __restrict__ ctf)
+{
+    int cx = tile / 2 + 1, cy = tile;
+    int m = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cx * cy) return;
+    int y = i / cx, x = i - y * cx;
+    int yr = y - cy / 2;
+    size_t base = (size_t)m * cx * cy;
+    float fr = x * 0.5f / (cx - 1);
+    fr = sqrtf(fr * fr + yr * yr / (float)(cy * cy));
+    if ((double)fr < 0.04) {
+        ctf[base + i] = 0.0f;
+        return;
+    }
+    int hb = box / 2;
+    double s = 0.0;
+    for (int k = -hb; k <= hb; ++k) {
+        int yy = y + k;
+        if (yy < 0) yy += cy;
+        else if (yy >= cy) yy -= cy;
+        s += hsum[base + (size_t)yy * cx + x];
+    }
+    s /= (double)box * (double)box;
+    if (!log_spect) s *= s;
+    ctf[base + i] = (float)((double)raw[base + i] - s);
+}
+
+// Mean and second moment of each half spectrum (Util/GCalcMoment2D.cu:10-58).
+__global__ void k_moments(const float* __restrict__ spect, int n, double* __restrict__ out2)
+{
+    __shared__ double sh[64];
+    int m = blockIdx.x;
+    const float* p = spect + (size_t)m * n;
+    double v[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = p[i];
+        v[0] += a;
+        v[1] += a * a;
+    }
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        out2[2 * m] = v[0] / n;
+        out2[2 * m + 1] = v[1] / n;
+    }
+}
+
+// Full spectrum value (DC at column tile/2) from the half spectrum
+// (FindCTF/GCalcSpectrum.cu:47-69; mirror row modulo tile).
+__device__ __forceinline__ float full_val(const float* half, int tile, int y, int X)
+{
+    int cx = tile / 2 + 1, hx = cx - 1;
+    int xd = X - hx;
+    if (xd >= 0) return half[(size_t)y * cx + xd];
+    int ys = tile - y;
+    if (ys >= tile) ys -= tile;
+    return half[(size_t)ys * cx - xd];
+}
+
+// Horizontal pass of the separable, periodic B-factor filter on the full
+// spectrum; output at the columns copied back by mLowpass
+// (FindCTF/CFindCtfBase.cpp:211-218).
+__global__ void k_lowpass_h(const float* __restrict__ in, int tile, const double* __restrict__ mom,
+                            const double* __restrict__ h, int radius, double* __restrict__ tmp,
+                            int* __restrict__ lowpassed)
+{
+    int cx = tile / 2 + 1, hx = cx - 1;
+    int m = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mean = mom[2 * m], var = mom[2 * m + 1] - mean * mean;
+    bool run = !(var < 1.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) lowpassed[m] = run ? 1 : 0;
+    if (!run || i >= cx * tile) return;
+    int y = i / cx, x = i - y * cx;
+    int X = x + hx;
+    if (X >= tile) X -= tile;
+    const float* half = in + (size_t)m * cx * tile;
+    double s = 0.0;
+    for (int t = -radius; t <= radius; ++t) {
+        int xx = X - t;
+        if (xx < 0) xx += tile;
+        else if (xx >= tile) xx -= tile;
+        s += h[t + radius] * (double)full_val(half, tile, y, xx);
+    }
+    tmp[(size_t)m * cx * tile + i] = s;
+}
+
+__global__ void k_lowpass_v(const float* __restrict__ in, int tile, const double* __restrict__ h,
+                            int radius, const double* __restrict__ tmp,
+                            const int* __restrict__ lowpassed, float* __restrict__ out)
+{
+    int cx = tile / 2 + 1;
+    int m = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cx * tile) return;
+    size_t base = (size_t)m * cx * tile;
+    if (!lowpassed[m]) {
+        out[base + i] = in[base + i];
+        return;
+    }
+    int y = i / cx, x = i - y * cx;
+    double s = 0.0;
+    for (int t = -radius; t <= radius; ++t) {
+        int yy = y - t;
+        if (yy < 0) yy += tile;
+        else if (yy >= tile) yy -= tile;
+        s += h[t + radius] * tmp[base + (size_t)yy * cx + x];
+    }
+    out[base + i] = (float)s;
+}
+
+// GRadialAvg (FindCTF/GRadialAvg.cu:11-33) with the nearest-pixel sample
+// table precomputed on the host.
+__global__ void k_radial(const float* __restrict__ spect, int cmp_n, int cx,
+                         const int* __restrict__ off, const int* __restrict__ pix,
+                         float* __restrict__ radial)
+{
+    int m = blockIdx.x;
+    const float* p = spect + (size_t)m * cmp_n;
+    for (int r = threadIdx.x; r < cx; r += blockDim.x) {
+        double s = 0.0;
+        int a = off[r], b = off[r + 1];
+        for (int k = a; k < b; ++k) s += p[pix[k]];
+        radial[(size_t)m * cx + r] = (float)(s / (b - a));
+    }
+}
+
+// Spectrum of each job gathered in band order, and its sum of squares.
+__global__ void k_band_gather(const float* __restrict__ ctf, int cmp_n,
+                              const SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands,
+                              const int* __restrict__ spec_off, float* __restrict__ band_spec,
+                              double* __restrict__ sum_ss)
+{
+    __shared__ double sh[32];
+    int j = blockIdx.x;
+    const SearchJob& jb = jobs[j];
+    const BandDev& b = bands[jb.band];
+    const float* src = ctf + (size_t)jb.mic * cmp_n;
+    float* dst = band_spec + spec_off[j];
+    double v[1] = {0.0};
+    for (int k = threadIdx.x; k < b.n; k += blockDim.x) {
+        float s = src[b.idx[k]];
+        dst[k] = s;
+        v[0] += (double)s * (double)s;
+    }
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0) sum_ss[j] = v[0];
+}
+
+// Signed CTF of GCalcCTF2D (FindCTF/GCalcCTF2D.cu:15-38) at one pixel, double.
+__device__ double ctf_at(int x, int y, int cx, int cy, const PixOptics& o, double add,
+                         double mean, double sigma, double az)
+{
+    double fx = x * 0.5 / (cx - 1);
+    double fy = (double)(y - cy / 2) / cy;
+    double s2 = fx * fx + fy * fy;
+    double th = atan(fy / (fx + 1e-30));
+    double df = mean + sigma * cos(2.0 * (th - az));
+    double chi = add + M_PI * (double)o.wl * s2 * (df - 0.5 * s2 * (double)o.wl * o.wl * o.cs);
+    return -sin(chi);
+}
+
+// CSpectrumImage::mGenFullSpectrum + mEmbedCTF (FindCTF/CSpectrumImage.cpp:36-71,
+// FindCTF/GCalcCTF2D.cu:49-78).
+__global__ void k_full_spectrum(const float* __restrict__ ctf, int tile, const int* __restrict__ mic_of,
+                                const gcf_result* __restrict__ res, const PixOptics* __restrict__ op,
+                                const double* __restrict__ mom, float* __restrict__ full)
+{
+    int k = blockIdx.y;
+    int m = mic_of[k];
+    int cx = tile / 2 + 1, cy = tile, hx = cx - 1;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tile * tile) return;
+    int y = i / tile, X = i - y * tile;
+    const float* half = ctf + (size_t)m * cx * cy;
+    float v = full_val(half, tile, y, X);
+    const PixOptics o = op[k];
+    const gcf_result r = res[k];
+    // CFindCtfBase::Setup1 resolution range (FindCTF/CFindCtfBase.cpp:64-68)
+    float r0 = 25.0f * o.px, r1 = (2.0f * o.px) / 0.8f;
+    if (r1 < 3.5f) r1 = 3.5f;
+    float fmn = o.px / r0, fmx = o.px / r1;
+    if (X < hx) {
+        float fy = (y - cy * 0.5f) / cy;
+        float fx = (X - (float)hx) * 0.5f / hx;
+        float rr = sqrtf(fx * fx + fy * fy);
+        if (!(rr < fmn || rr > fmx)) {
+            double mean = mom[2 * m], var = mom[2 * m + 1] - mean * mean;
+            double sd = var < 0 ? 0.0 : sqrt(var);
+            // CFindCtfBase::GenFullSpectrum (FindCTF/CFindCtfBase.cpp:118-126)
+            float az = r.azimuth * 0.017453f;
+            float dmin = r.df_min / o.px, dmax = r.df_max / o.px;
+            float ph = fmodf(r.ext_phase * 0.01745329f, 3.14159265358979f);
+            float mn = 0.5f * (dmin + dmax), sg = 0.5f * (dmax - dmin);
+            int ix = hx - X, iy = (cy - y) % cy;
+            double c = fabs(ctf_at(ix, iy, cx, cy, o, (double)(o.amp_phase + ph), mn, sg, az));
+            v = (float)((c - 0.5) * (sd * 1.5) + mean);
+        }
+    }
+    full[(size_t)k * tile * tile + i] = v;
+}
+
+// GSpectralCC2D::mGCalc2D (FindCTF/GSpectralCC2D.cu:12-110): per shell b,
+// Pearson CC of the signed CTF and the spectrum in [lo, hi).
+__global__ void k_ctf_res(const float* __restrict__ ctf, int tile, const SearchJob* __restrict__ jobs,
+                          float* __restrict__ cc_out)
+{
+    __shared__ double sh[6 * 32];
+    int b = blockIdx.x, j = blockIdx.y;
+    const SearchJob jb = jobs[j];
+    int cx = tile / 2 + 1, cy = tile;
+    const int width = 10;
+    int lo = b - width / 2, hi = lo + width;
+    if (lo < 0) {
+        lo = 0;
+        hi = width;
+    } else if (hi > cx) {
+        lo = cx - width;
+        hi = cx;
+    }
+    const PixOptics o = jb.o;
+    float dmin = jb.df_mean * (1.0f - jb.ast_ratio) / o.px;
+    float dmax = jb.df_mean * (1.0f + jb.ast_ratio) / o.px;
+    float mn = 0.5f * (dmin + dmax), sg = 0.5f * (dmax - dmin);
+    double add = (double)(o.amp_phase + jb.ext_phase * 0.01745329f);
+    double az = (double)(jb.ast_angle * 0.01745329f);
+    const float* sp = ctf + (size_t)jb.mic * cx * cy;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int y = threadIdx.x; y < cy; y += blockDim.x) {
+        float fy = fabsf(y - cy * 0.5f);
+        if (fy >= hi) continue;
+        for (int x = 0; x < cx && x < hi; ++x) {
+            float r = sqrtf((float)(x * x) + fy * fy);
+            if (r < lo || r >= hi) continue;
+            double c = ctf_at(x, y, cx, cy, o, add, mn, sg, az);
+            double s = sp[(size_t)y * cx + x];
+            v[0] += c * s;
+            v[1] += c;
+            v[2] += s;
+            v[3] += c * c;
+            v[4] += s * s;
+            v[5] += 1.0;
+        }
+    }
+    block_sum<6>(v, sh);
+    if (threadIdx.x != 0) return;
+    float out = 0.0f;
+    if (v[5] > 0) {
+        double n = v[5];
+        double mc = v[1] / n, ms = v[2] / n, cs = v[0] / n, sc = v[3] / n, ss = v[4] / n;
+        sc -= mc * mc;
+        ss -= ms * ms;
+        if (sc > 0 && ss > 0) out = (float)((cs - mc * ms) / sqrt(sc * ss));
+    }
+    cc_out[(size_t)j * cx + b] = out;
+}
+
+}  // namespace
+
+void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,
+                          cudaStream_t st)
+{
+    // box of GRmBackground2D::mGRemove (FindCTF/GRmBackground2D.cu:33-36), fMinFreq = 1/15
+    float fmin = 1.0f / 15.0f;
+    int box = (int)(fmin * tile);
+    if (box > (0.3f * tile)) box = (int)(0.3f * tile);
+    box = box / 2 * 2 + 1;
+    if (box < 7) box = 7;
+    int cx = tile / 2 + 1;
+    int th = cx < 256 ? ((cx + 31) / 32) * 32 : 256;
+    dim3 grid(tile, nmic);
+    k_bg_horizontal<<<grid, th, 2 * cx * sizeof(float), st>>>(raw, tile, log_spect, box, hsum);
+}
+
+void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic, int log_spect,
+                        float* ctf, cudaStream_t st)
+{
+    float fmin = 1.0f / 15.0f;
+    int box = (int)(fmin * tile);
+    if (box > (0.3f * tile)) box = (int)(0.3f * tile);
+    box = box / 2 * 2 + 1;
+    if (box < 7) box = 7;
+    int n = (tile / 2 + 1) * tile;
+    dim3 grid((n + 255) / 256, nmic);
+    k_bg_vertical<<<grid, 256, 0, st>>>(raw, hsum, tile, log_spect, box, ctf);
+}
+
+void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st)
+{
+    k_moments<<<nmic, 512, 0, st>>>(spect, n, out2);
+}
+
+void launch_lowpass(const float* in, int tile, int nmic, const double* moments, const double* h,
+                    int radius, double* tmp, float* out, int* lowpassed, cudaStream_t st)
+{
+    int n = (tile / 2 + 1) * tile;
+    dim3 grid((n + 255) / 256, nmic);
+    k_lowpass_h<<<grid, 256, 0, st>>>(in, tile, moments, h, radius, tmp, lowpassed);
+    k_lowpass_v<<<grid, 256, 0, st>>>(in, tile, h, radius, tmp, lowpassed, out);
+}
+
+void launch_radial(const float* spect, int tile, int nmic, const int* off, const int* pix,
+                   float* radial, cudaStream_t st)
+{
+    int cx = tile / 2 + 1;
+    k_radial<<<nmic, 256, 0, st>>>(spect, cx * tile, cx, off, pix, radial);
+}
+
+void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, const BandDev* bands,
+                        const int* spec_off, int njobs, float* band_spec, double* sum_ss,
+                        cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    k_band_gather<<<njobs, 512, 0, st>>>(ctf, cmp_n, jobs, bands, spec_off, band_spec, sum_ss);
+}
+
+void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_of,
+                          const gcf_result* res, const PixOptics* o, const double* moments,
+                          float res_lo_freq_dummy, float* full, cudaStream_t st)
+{
+    (void)res_lo_freq_dummy;
+    if (nmic <= 0) return;
+    dim3 grid((tile * tile + 255) / 256, nmic);
+    k_full_spectrum<<<grid, 256, 0, st>>>(ctf, tile, mic_of, res, o, moments, full);
+}
+
+void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, float* cc,
+                    cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    dim3 grid(tile / 2 + 1, njobs);
+    k_ctf_res<<<grid, 256, 0, st>>>(ctf, tile, jobs, cc);
+}
+
+}  // namespace gcf

@@ -1,0 +1,189 @@
+/*
+ * gctf_b200.h -- C ABI of the B200-native GCtfFind CTF-estimation path.
+ *
+ * Plain C types only (no CUDA or torch types in any signature).  Every entry
+ * point returns a gcf_status; none asserts, exits or resets the device.
+ * A context owns all device memory and one CUDA stream; the caller owns
+ * every host buffer.  Use one context per host thread.
+ *
+ * The reference surface each entry point replaces is cited beside it
+ * (paths are relative to the GCtfFind source tree).
+ */
+#ifndef GCTF_B200_H
+#define GCTF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GCF_OK = 0,
+    GCF_ERR_INVALID_ARG = 1,     /* bad pointer, size or flag           */
+    GCF_ERR_CUDA = 2,            /* CUDA runtime error                  */
+    GCF_ERR_CUFFT = 3,           /* cuFFT error (rescale, cuFFT variant) */
+    GCF_ERR_NO_MEMORY = 4,       /* device or host allocation failed    */
+    GCF_ERR_IMAGE_TOO_SMALL = 5, /* image holds no full tile            */
+    GCF_ERR_STATE = 6,           /* call out of order (e.g. Do2D before
+                                    a spectrum was generated)           */
+    GCF_ERR_IO = 7,              /* file could not be read or written   */
+    GCF_ERR_TIMEOUT = 8          /* bounded device wait gave up         */
+} gcf_status;
+
+typedef struct gcf_ctx gcf_ctx;
+
+/* Optics of CCTFTheory::Setup (FindCTF/CCTFTheory.cpp:69-86) and the
+ * -ExtPhase pair of CInput (CInput.cpp:43-58, :152-155). */
+typedef struct {
+    float kv;               /* keV                                    */
+    float cs_mm;            /* spherical aberration, mm               */
+    float amp_contrast;     /* amplitude contrast fraction            */
+    float pixel_size;       /* raw pixel size, Angstrom               */
+    float ext_phase_deg;    /* initial extra phase, degree            */
+    float ext_phase_range;  /* extra-phase search range, degree (<=0: off) */
+} gcf_optics;
+
+/* Result row (CFindSeriesCtfs::mGetResults, CFindSeriesCtfs.cpp:378-386)
+ * plus the 1D estimate and the spectral-CC resolution that the reference
+ * computes but does not report (FindCTF/CFindDefocus2D.cpp:382-400). */
+typedef struct {
+    float df_min;      /* Angstrom */
+    float df_max;      /* Angstrom */
+    float azimuth;     /* degree   */
+    float ext_phase;   /* degree   */
+    float score;       /* CC       */
+    float ctf_res;     /* Angstrom */
+    float df_1d;       /* 1D estimate, Angstrom (0 after Refine) */
+    float phase_1d;    /* 1D estimate, degree   */
+    float score_1d;    /* 1D CC                 */
+    int   lowpassed;   /* 1 if the B-factor lowpass ran           */
+} gcf_result;
+
+/* Spectrum-stage implementation. */
+typedef enum {
+    GCF_SPECT_FUSED = 0,   /* hand-written fused tile-FFT kernel (default) */
+    GCF_SPECT_CUFFT = 1    /* batched cuFFT comparison variant            */
+} gcf_spectrum_impl;
+
+/* ---------------------------------------------------------------------- */
+/* Context                                                                  */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces the CInput tile/log-spectrum globals read by CFindCtfBase
+ * (FindCTF/CFindCtfBase.cpp:52-54, :111-112) and the device choice of
+ * CProcessMain::DoIt (CProcessMain.cpp:26). */
+gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out);
+void       gcf_destroy(gcf_ctx* ctx);
+const char* gcf_strerror(gcf_status s);
+/* Last error detail of this context (CUDA/cuFFT message), never NULL. */
+const char* gcf_last_error(gcf_ctx* ctx);
+gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
+
+/* ---------------------------------------------------------------------- */
+/* CFindCtf2D call shape (FindCTF/CFindCTFInc.h:541-623)                    */
+/* ---------------------------------------------------------------------- */
+
+/* CFindCtf2D::Setup1 + Setup2 (FindCTF/CFindCtf2D.cpp:33-42,
+ * FindCTF/CFindCtfBase.cpp:48-76): optics with the pixel size of the image
+ * that will be passed to gcf_gen_half_spectrum (i.e. after rescaling). */
+gcf_status gcf_setup(gcf_ctx* ctx, const gcf_optics* optics, int width, int height);
+
+/* CFindCtfBase::GenHalfSpectrum (FindCTF/CFindCtfBase.cpp:109-116): average
+ * amplitude spectrum of the tiles of `img` (width x height floats, row
+ * pitch `pitch` floats), background removal and lowpass.  `img_is_device`
+ * = 1 when img is a device pointer on the context's GPU. */
+gcf_status gcf_gen_half_spectrum(gcf_ctx* ctx, const float* img, int pitch, int img_is_device);
+
+/* CFindCtfBase::SetPhase (FindCTF/CFindCtfBase.cpp:78-82). */
+gcf_status gcf_set_phase(gcf_ctx* ctx, float phase_deg, float range_deg);
+
+/* CFindCtf2D::Do2D (FindCTF/CFindCtf2D.cpp:44-53). */
+gcf_status gcf_do2d(gcf_ctx* ctx, gcf_result* out);
+
+/* CFindCtf2D::Refine (FindCTF/CFindCtf2D.cpp:55-66): {centre, range} pairs. */
+gcf_status gcf_refine(gcf_ctx* ctx, const float df_mean[2], const float ast_ratio[2],
+                      const float ast_angle[2], const float ext_phase[2], gcf_result* out);
+
+/* CFindCtfBase::GetSpectSize (FindCTF/CFindCtfBase.cpp:102-107). */
+gcf_status gcf_get_spect_size(gcf_ctx* ctx, int size[2], int half);
+
+/* CFindCtfBase::GetHalfSpect (FindCTF/CFindCtfBase.cpp:90-100): raw (1) or
+ * background-removed (0) half spectrum, (tile/2+1) x tile floats, DC at
+ * (0, tile/2), copied to host. */
+gcf_status gcf_get_half_spectrum(gcf_ctx* ctx, int raw, float* host_out);
+
+/* CFindCtfBase::GenFullSpectrum (FindCTF/CFindCtfBase.cpp:118-133): the
+ * tile x tile diagnostic spectrum with the fitted |CTF| in the left half,
+ * for the result `res` (normally the last Do2D/Refine result). */
+gcf_status gcf_gen_full_spectrum(gcf_ctx* ctx, const gcf_result* res, float* host_out);
+
+/* GRadialAvg of the current spectrum (FindCTF/GRadialAvg.cu:43-53):
+ * tile/2+1 floats to host. */
+gcf_status gcf_get_radial_average(gcf_ctx* ctx, float* host_out);
+
+/* ---------------------------------------------------------------------- */
+/* Rescale (CRescaleImage, FindCTF/CRescaleImage.cpp:47-99)                  */
+/* ---------------------------------------------------------------------- */
+void       gcf_rescale_dims(int width, int height, float pixel_size, int* new_width,
+                            int* new_height, float* new_pixel_size);
+/* Fourier-crop `img` (host or device) to >= 1.2 A/px; output dense
+ * new_width x new_height floats to host. */
+gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int width, int height, float pixel_size,
+                       int img_is_device, float* host_out);
+
+/* ---------------------------------------------------------------------- */
+/* Batched paths                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* CFindSeriesCtfs::DoIt policy (CFindSeriesCtfs.cpp:50-213) over n
+ * equally-sized raw images: images[i] is image i (host or device, dense
+ * width x height floats); `order` is the processing order (order[0] gets the
+ * full search; every later image is refined around the best-scoring earlier
+ * one; a refine with score <= 0 falls back to the full search).  is_tomo
+ * selects the tilt-series refine windows (CFindSeriesCtfs.cpp:168-193).
+ * results[i] receives image i.  full_spectra (nullable) receives n
+ * tile x tile diagnostic spectra in image order. */
+gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int width,
+                          int height, int images_are_device, const gcf_optics* optics,
+                          const int* order, int is_tomo, gcf_result* results,
+                          float* full_spectra);
+
+/* Independent full searches (CFindCtf2D::Do2D per image, the single-file
+ * mode of CInputFolder::mReadSingle, CInputFolder.cpp:159-192) of n images
+ * of possibly different sizes and pixel sizes, batched on the GPU. */
+typedef struct {
+    const float* image;      /* host or device, dense width x height */
+    int width, height;
+    float pixel_size;        /* raw pixel size, Angstrom */
+} gcf_item;
+gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int images_are_device,
+                         const gcf_optics* optics, gcf_result* results);
+
+/* ---------------------------------------------------------------------- */
+/* MRC input/output (Mrc::CLoadMrc / Mrc::CSaveMrc subset,                  */
+/* Include/Mrcfile/CMrcFileInc.h:52-120, MrcUtil/CLoadImages.cpp:108-181)   */
+/* ---------------------------------------------------------------------- */
+/* dims = {nx, ny, nz}; mode; pixel size from the cell (0 if absent);
+ * ext_floats = floats per section in the extended header. */
+gcf_status gcf_mrc_info(const char* path, int dims[3], int* mode, float* pixel_size,
+                        int* ext_floats);
+/* Section z as float (modes 0, 1, 2, 5, 6). */
+gcf_status gcf_mrc_read(const char* path, int z, float* out);
+/* Tilt angle of each of the first n sections from the extended header. */
+gcf_status gcf_mrc_read_tilts(const char* path, float* tilts, int n);
+/* float32 (mode 2) stack of nz sections. */
+gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, int nz,
+                         float pixel_size);
+
+/* Device time (ms, CUDA events on the context stream) of the stages of the
+ * last batched call: [0] upload, [1] rescale, [2] spectrum, [3] background
+ * + lowpass + radial, [4] 1D search, [5] 2D search, [6] total. */
+gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7]);
+/* Number of kernels this library launched in the last batched call. */
+gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GCTF_B200_H */

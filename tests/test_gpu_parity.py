@@ -1,0 +1,166 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances (north star: averaged spectra within 1e-4 relative, defocus within
+one reference search step, astigmatism angle within 1 degree, CC within 1e-3):
+  raw averaged spectrum : |gpu - orc| <= 1e-4 * |orc| + 1e-5 * mean(orc) per pixel
+  ctf spectrum          : |gpu - orc| <= 1e-4 * rms(orc) per pixel
+  radial average        : |gpu - orc| <= 1e-4 * rms(orc) per bin
+  search results        : |d df| <= one search step (the last DfMean step,
+                          max(20 A, range/31) <= 60 A here), |d azimuth| <= 1 deg
+                          (modulo 180), |d CC| <= 1e-3
+"""
+import numpy as np
+import pytest
+
+from gctffind_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+TILE = 256
+PX = 1.35
+
+
+def _img(seed=3, w=1024, h=1024, px=PX, df=(14800.0, 15200.0), az=20.0, dose=3.0, tilt=0.0):
+    spec = synth.MicrographSpec(width=w, height=h, pixel_size=px, df_min=df[0], df_max=df[1],
+                                azimuth_deg=az, dose=dose, seed=seed, tilt_deg=tilt)
+    return synth.make_micrograph(spec).numpy()
+
+
+def _ang_diff(a, b):
+    d = (a - b) % 180.0
+    return min(d, 180.0 - d)
+
+
+def _assert_result_close(g, o, df_tol=60.0, ang_tol=1.0, cc_tol=1e-3):
+    assert abs(g.df_min - o.df_min) <= df_tol, (g, o.as_dict())
+    assert abs(g.df_max - o.df_max) <= df_tol, (g, o.as_dict())
+    if abs(o.df_max - o.df_min) > 50.0:   # azimuth is meaningless without astigmatism
+        assert _ang_diff(g.azimuth, o.azimuth) <= ang_tol, (g, o.as_dict())
+    assert abs(g.score - o.score) <= cc_tol, (g, o.as_dict())
+
+
+@pytest.fixture(scope="module")
+def case(gpu_lib, oracle):
+    G = gpu_lib
+    img = _img()
+    ctx = G.Context(0, TILE, 0)
+    op = G.make_optics(pixel_size=PX)
+    ctx.setup(op, img.shape[1], img.shape[0])
+    ctx.gen_half_spectrum(img)
+    p = oracle.params(pixel_size=PX, tile_size=TILE)
+    ores, oraw, octf, ofull = oracle.find_ctf_image(img, PX, p, want_spectra=True)
+    return dict(G=G, ctx=ctx, img=img, op=op, p=p, ores=ores, oraw=oraw, octf=octf, ofull=ofull)
+
+
+def test_raw_spectrum_matches_oracle(case):
+    g = case["ctx"].half_spectrum(raw=True).astype(np.float64)
+    o = case["oraw"]
+    tol = 1e-4 * np.abs(o) + 1e-5 * o.mean()
+    err = np.abs(g - o)
+    assert np.all(err <= tol), float((err / (np.abs(o) + 1e-30)).max())
+
+
+def test_ctf_spectrum_matches_oracle_given_gpu_raw(case, oracle):
+    # isolate background + lowpass: oracle fed with the GPU raw spectrum
+    graw = case["ctx"].half_spectrum(raw=True).astype(np.float64)
+    octf, lp = oracle.ctf_spectrum(graw, 0)
+    g = case["ctx"].half_spectrum(raw=False).astype(np.float64)
+    rms = np.sqrt(np.mean(octf ** 2))
+    assert lp == 1
+    assert np.max(np.abs(g - octf)) <= 1e-4 * rms
+
+
+def test_radial_average_matches_oracle(case, oracle):
+    g_ctf = case["ctx"].half_spectrum(raw=False).astype(np.float64)
+    orad = oracle.radial_average(g_ctf)
+    grad = case["ctx"].radial_average().astype(np.float64)
+    rms = np.sqrt(np.mean(orad ** 2))
+    assert np.max(np.abs(grad - orad)) <= 1e-4 * rms
+
+
+def test_do2d_matches_oracle(case):
+    r = case["ctx"].do2d()
+    o = case["ores"]
+    assert abs(r.df_1d - o.df_1d) <= 20.0, (r, o.as_dict())
+    _assert_result_close(r, o)
+    # and the synthetic truth (14800 / 15200 at 20 degrees) within 150 A / 3 degrees
+    assert abs(r.df_min - 14800.0) < 150.0 and abs(r.df_max - 15200.0) < 150.0
+    assert _ang_diff(r.azimuth, 20.0) < 3.0
+
+
+def test_do2d_search_on_oracle_spectrum(case, oracle):
+    # search alone: both sides on (nearly) the same spectrum
+    r = case["ctx"].do2d()
+    s = oracle.search(case["ctx"].half_spectrum(raw=False).astype(np.float64), PX, case["p"])
+    _assert_result_close(r, s, df_tol=25.0, ang_tol=1.0, cc_tol=2e-4)
+
+
+def test_refine_matches_oracle(case, oracle):
+    ctx = case["ctx"]
+    rin = [15100.0, 7550.0, 0.01, 0.04, 10.0, 30.0, 0.0, 0.0]
+    r = ctx.refine(rin[0:2], rin[2:4], rin[4:6], rin[6:8])
+    o = oracle.search(ctx.half_spectrum(raw=False).astype(np.float64), PX, case["p"], mode=1,
+                      refine_in=rin)
+    _assert_result_close(r, o, df_tol=25.0, cc_tol=2e-4)
+
+
+def test_full_spectrum_matches_oracle(case, oracle):
+    ctx = case["ctx"]
+    r = ctx.do2d()
+    g = ctx.full_spectrum(r).astype(np.float64)
+    octf = ctx.half_spectrum(raw=False).astype(np.float64)
+    ores = oracle.OrcResult(r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score, 0, 0, 0, 0, 1)
+    o = oracle.full_spectrum(octf, PX, case["p"], ores).astype(np.float64)
+    rms = np.sqrt(np.mean(o ** 2))
+    assert np.max(np.abs(g - o)) <= 1e-4 * rms
+
+
+def test_series_matches_oracle(gpu_lib, oracle):
+    G = gpu_lib
+    tilts = [-6.0, -3.0, 0.0, 3.0, 6.0]
+    imgs = [_img(seed=10 + i, w=768, h=768, df=(19850.0, 20150.0), az=-35.0, tilt=t)
+            for i, t in enumerate(tilts)]
+    so = G.series_order(tilts)
+    ctx = G.Context(0, TILE, 0)
+    op = G.make_optics(pixel_size=PX)
+    gres = ctx.run_series(imgs, op, so.order, is_tomo=True)
+    p = oracle.params(pixel_size=PX, tile_size=TILE)
+    ores = oracle.series(imgs, p, so.order, True)
+    for g, o in zip(gres, ores):
+        _assert_result_close(g, o)
+
+
+def test_batch_mixed_sizes(gpu_lib, oracle):
+    G = gpu_lib
+    specs = [(768, 640, 1.35, (9900.0, 10100.0)), (1024, 768, 1.5, (24800.0, 25200.0))]
+    imgs = [_img(seed=40 + i, w=w, h=h, px=px, df=df) for i, (w, h, px, df) in enumerate(specs)]
+    ctx = G.Context(0, TILE, 0)
+    op = G.make_optics()
+    gres = ctx.run_batch(imgs, [s[2] for s in specs], op)
+    for img, s, g in zip(imgs, specs, gres):
+        p = oracle.params(pixel_size=s[2], tile_size=TILE)
+        o = oracle.find_ctf_image(img, s[2], p)
+        _assert_result_close(g, o)
+
+
+def test_rescale_matches_oracle(gpu_lib, oracle):
+    G = gpu_lib
+    img = _img(seed=7, w=1024, h=1024, px=0.8, df=(9900.0, 10100.0))
+    ctx = G.Context(0, TILE, 0)
+    g = ctx.rescale(img, 0.8).astype(np.float64)
+    o = oracle.rescale(img, 0.8).astype(np.float64)
+    assert g.shape == o.shape == (682, 682)
+    rel = np.linalg.norm(g - o) / np.linalg.norm(o)
+    assert rel < 5e-3, rel   # differs only on the cropped Nyquist row/column treatment
+
+
+def test_errors_are_status_codes(gpu_lib):
+    G = gpu_lib
+    ctx = G.Context(0, TILE, 0)
+    with pytest.raises(G.GcfError):
+        ctx.do2d()   # no spectrum yet
+    op = G.make_optics(pixel_size=PX)
+    small = np.zeros((100, 100), np.float32)
+    ctx.setup(op, 100, 100)
+    with pytest.raises(G.GcfError):
+        ctx.gen_half_spectrum(small)
