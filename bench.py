@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the CTF-estimation hot path on B200.
+
+Workload (one "step"): a synthetic tilt series of 41 micrographs, 4096 x 4096
+float32 at 1.35 A/px (-60..+60 degrees in 3-degree steps, 3 e/A^2 per tilt,
+defocus 30000 A at 0 degrees with a per-column gradient set by the tilt,
+astigmatism uniform in 0-800 A at a random angle), processed with the
+reference's series policy (CFindSeriesCtfs: zero tilt full search, every
+other tilt refined around the best-scoring earlier one) through the C ABI
+call gcf_run_series.
+
+  value : micrographs/s with the series already resident in HBM
+          (device pointers), device time from CUDA events on the library stream
+  e2e   : the same call with pinned HOST buffers; the host->device copy of
+          the 41 images and the device->host read of the results are inside
+          the timed region
+
+Rank r of N processes its own series (seeded by r): weak scaling, replicas
+only, no data-path collective.  `--impl reference` times the reference
+implementation of the path instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_TILTS = 41
+SIZE = 4096
+PX = 1.35
+METRIC = "4096^2 micrographs/s (tilt series, plain FP32 search)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--spectrum", default="auto", choices=["auto", "fused", "cufft"])
+    ap.add_argument("--n-tilts", type=int, default=N_TILTS)
+    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        import torch
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        busy = [r for r in rows if r[0] > 0.5 * r[1]] or rows
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, v in zip(names, r[2:]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": rows[0][1],
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def make_series(rank, n_tilts, size, device):
+    import torch
+    from gctffind_b200 import synth
+    specs = synth.tilt_series_specs(n_tilts=n_tilts, step_deg=3.0, size=size, pixel_size=PX,
+                                    dose=3.0, df0=30000.0, seed=1 + rank)
+    imgs = [synth.make_micrograph(s, device=device) for s in specs]
+    torch.cuda.synchronize()
+    return specs, imgs
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "_fallback": True}
+
+
+def cpu_baseline(imgs_host, order, budget_s=25.0):
+    """FP64 OpenMP oracle on the host cores: the zero-tilt full search plus
+    refinements of the next tilts in processing order, as many as fit the
+    time budget (at least one)."""
+    from oracle import oracle as O
+    O.build()
+    cores = O.num_threads(os.cpu_count() or 1)
+    p = O.params(pixel_size=PX, tile_size=512)
+    t0 = time.perf_counter()
+    z = order[0]
+    r0 = O.find_ctf_image(imgs_host[z], PX, p, mode=0)
+    done = 1
+    for idx in order[1:]:
+        if time.perf_counter() - t0 > budget_s:
+            break
+        dmin, dmax = r0.df_min, r0.df_max
+        mean = 0.5 * (dmin + dmax)
+        rin = [mean, max(mean * 0.5, 5000.0 * PX * PX), (dmax - dmin) * 0.5 / mean, 0.0,
+               r0.azimuth, 0.0, r0.ext_phase, 0.0]
+        O.find_ctf_image(imgs_host[idx], PX, p, mode=1, refine_in=rin)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "micrographs/s", "cores": cores, "kind": "port",
+            "sample": f"{done} of the series' 4096^2 micrographs (zero-tilt full search + "
+                      f"{done - 1} refinements), FP64 oracle, {cores} OpenMP threads, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference implementation of the path on this box."""
+    if rank != 0:
+        return 0
+    import torch
+    specs, imgs = make_series(0, args.n_tilts, args.size, "cuda" if torch.cuda.is_available() else "cpu")
+    host = [im.cpu().numpy() for im in imgs]
+    from gctffind_b200.api import series_order
+    from gctffind_b200 import synth
+    order = series_order(synth.tilt_angles(args.n_tilts, 3.0)).order
+    vals = []
+    cb = None
+    for k in range(max(1, args.warmup) + max(1, args.steps)):
+        cb = cpu_baseline(host, order, budget_s=8.0)
+        if k >= max(1, args.warmup):
+            vals.append(cb["value"])
+        if len(vals) >= args.steps:
+            break
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "micrographs/s", "n_gpus": world,
+            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1000.0 * args.n_tilts / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"tilt series {args.n_tilts} x {args.size}^2 float32 @ {PX} A/px, "
+                                   "zero-tilt full search + refinements (sampled)",
+                       "l2": "inputs larger than L2"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "micrographs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import numpy as np
+    import torch
+    import gctffind_b200 as G
+    from gctffind_b200 import synth
+    torch.cuda.set_device(local)
+    specs, imgs = make_series(rank, args.n_tilts, args.size, f"cuda:{local}")
+    order = G.series_order(synth.tilt_angles(args.n_tilts, 3.0)).order
+    ctx = G.Context(local, 512, 0)
+    if args.spectrum == "cufft":
+        ctx.set_spectrum_impl(G.GCF_SPECT_CUFFT)
+    elif args.spectrum == "fused":
+        ctx.set_spectrum_impl(G.GCF_SPECT_FUSED)
+    else:
+        try:
+            ctx.set_spectrum_impl(G.GCF_SPECT_FUSED)
+        except G.GcfError:
+            ctx.set_spectrum_impl(G.GCF_SPECT_CUFFT)
+    op = G.make_optics(pixel_size=PX)
+
+    # ---- device-resident inputs -------------------------------------------------
+    for _ in range(args.warmup):
+        ctx.run_series(imgs, op, order, is_tomo=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    dev_ms, stage = 0.0, {}
+    launches = 0
+    results = None
+    for _ in range(args.steps):
+        results = ctx.run_series(imgs, op, order, is_tomo=True)
+        st = ctx.stage_times()
+        dev_ms += st["total"]
+        for k, v in st.items():
+            stage[k] = stage.get(k, 0.0) + v
+        launches += ctx.launch_count()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    t_step = max_over_ranks(dev_ms / args.steps, world)
+    value = world * args.n_tilts / (t_step / 1000.0)
+
+    # ---- end to end: pinned host inputs, H2D + results D2H inside the timed region ----
+    host = [im.cpu().pin_memory() for im in imgs]
+    for _ in range(max(1, min(args.warmup, 2))):
+        ctx.run_series(host, op, order, is_tomo=True)
+    barrier(world)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        ctx.run_series(host, op, order, is_tomo=True)
+        e2e_ms += ctx.stage_times()["total"]
+    barrier(world)
+    t_e2e = max_over_ranks(e2e_ms / args.steps, world)
+    e2e = world * args.n_tilts / (t_e2e / 1000.0)
+    h2d = sum(int(im.numel()) * 4 for im in imgs)
+    d2h = args.n_tilts * 40
+
+    # ---- roofline of the spectrum stage (HBM-bound: 4 W H bytes per micrograph) ----
+    pk = peaks()
+    spec_ms = stage.get("spectrum", 0.0) / args.steps
+    algo_bytes = args.n_tilts * 4 * args.size * args.size
+    achieved = algo_bytes / (spec_ms / 1000.0) / 1e9 if spec_ms > 0 else 0.0
+    roof = {"kernel": "tile spectrum stage (all tiles of the series, one step)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": pk.get("hbm_gbs"),
+            "unit": "GB/s", "frac": round(achieved / pk.get("hbm_gbs", 6650.0), 4),
+            "traffic": None, "peak_source": "fallback" if pk.get("_fallback") else "measured",
+            "algorithmic_bytes_per_step": algo_bytes}
+
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "micrographs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"tilt series {args.n_tilts} x {args.size}^2 float32 @ {PX} A/px, "
+                                   "3 e/A^2, df 30000 A + tilt gradient, astig 0-800 A; "
+                                   "CFindSeriesCtfs policy (zero tilt full, rest refined)",
+                       "tile": 512, "spectrum": ["fused", "cufft"][0 if args.spectrum == "fused" else 1]
+                       if args.spectrum != "auto" else "auto",
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (2.75 GB per step)"},
+            "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage.items()},
+            "e2e": {"value": round(e2e, 2), "unit": "micrographs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(t_e2e, 3)},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        host_np = [h.numpy() for h in host]
+        line["cpu_baseline"] = cpu_baseline(host_np, order)
+    if rank == 0:
+        r0 = results[order[0]]
+        line["sample_result"] = {"zero_tilt": {"df_min": round(r0.df_min, 1), "df_max": round(r0.df_max, 1),
+                                               "azimuth": round(r0.azimuth, 2), "score": round(r0.score, 4)},
+                                 "truth": {"df_min": round(specs[order[0]].df_min, 1),
+                                           "df_max": round(specs[order[0]].df_max, 1),
+                                           "azimuth": round(specs[order[0]].azimuth_deg, 2)}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -103,6 +103,14 @@ struct gcf_ctx {
 
     std::map<std::tuple<int, int, int>, FftPlan> plans;   // (kind, a, b)
 
+    // fused spectrum
+    DBuf<float2> tw512;
+    DBuf<FusedImageDesc> f_desc;
+    DBuf<int4> f_items;
+    DBuf<int> f_first;
+    DBuf<float> f_inv, f_partial;
+    int fused_clusters = 0;
+
     // CFindCtf2D call-shape state
     gcf_optics optics{};
     bool have_setup = false;
@@ -239,6 +247,14 @@ gcf_status build_tile_tables(gcf_ctx* ctx)
     ctx->lp_radius = R;
     CK(ctx->lp_h.ensure(h.size()));
     CK(cudaMemcpy(ctx->lp_h.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    // exp(-2 pi i t / T), t < T: twiddles of the fused tile FFT
+    std::vector<float2> tw(T);
+    for (int t = 0; t < T; ++t) {
+        double a = -2.0 * M_PI * (double)t / (double)T;
+        tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CK(ctx->tw512.ensure(T));
+    CK(cudaMemcpy(ctx->tw512.p, tw.data(), T * sizeof(float2), cudaMemcpyHostToDevice));
     return GCF_OK;
 }
 
@@ -403,6 +419,60 @@ gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
     return GCF_OK;
 }
 
+// CGenAvgSpectrum::DoIt for all micrographs in one launch of the fused
+// tile-spectrum kernel (tile 512).
+gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float* raw_out)
+{
+    const int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
+    const int kItemTiles = 64;
+    std::vector<FusedImageDesc> d(nm);
+    std::vector<int4> items;
+    std::vector<int> first(nm + 1);
+    std::vector<float> inv(nm);
+    for (int i = 0; i < nm; ++i) {
+        const MicImage& m = mics[i];
+        Layout L = tile_layout(m.w, m.h, T);
+        int nt = L.ntx * L.nty;
+        if (L.ntx <= 0 || L.nty <= 0) return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no tile");
+        d[i].img = m.img;
+        d[i].pitch = m.pitch;
+        d[i].ntx = L.ntx;
+        d[i].offx = L.offx;
+        d[i].offy = L.offy;
+        d[i].stride = L.stride;
+        d[i].vec4 = ((L.offx % 4) == 0 && (L.stride % 4) == 0 && (m.pitch % 4) == 0 &&
+                     ((uintptr_t)m.img % 16) == 0) ? 1 : 0;
+        inv[i] = 1.0f / nt;
+        first[i] = (int)items.size();
+        int nch = (nt + kItemTiles - 1) / kItemTiles;
+        int chunk = (nt + nch - 1) / nch;
+        for (int t0 = 0; t0 < nt; t0 += chunk)
+            items.push_back(make_int4(i, t0, std::min(nt, t0 + chunk), (int)items.size()));
+    }
+    first[nm] = (int)items.size();
+    if (ctx->fused_clusters <= 0) {
+        int n = 0;
+        CK(fused_max_clusters(&n));
+        if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
+        ctx->fused_clusters = n;
+    }
+    int ni = (int)items.size();
+    CK(ctx->f_desc.ensure(nm));
+    CK(ctx->f_items.ensure(ni));
+    CK(ctx->f_first.ensure(nm + 1));
+    CK(ctx->f_inv.ensure(nm));
+    CK(ctx->f_partial.ensure((size_t)ni * cx * T));
+    CK(cudaMemcpyAsync(ctx->f_desc.p, d.data(), nm * sizeof(FusedImageDesc), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->f_items.p, items.data(), ni * sizeof(int4), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->f_inv.p, inv.data(), nm * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    int ncl = std::min(ctx->fused_clusters, ni);
+    CK(launch_fused(ctx->f_desc.p, ctx->f_items.p, ni, ctx->f_first.p, ctx->f_inv.p, nm, ctx->taper.p,
+                    ctx->tw512.p, ctx->f_partial.p, raw_out, ncl, ctx->st));
+    ctx->launches += 2;
+    return GCF_OK;
+}
+
 // CFindCtfBase::GenHalfSpectrum for n micrographs (slots 0..n-1):
 // spectrum, background removal, moments, lowpass, radial average.
 gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
@@ -418,7 +488,11 @@ gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
     CK(ctx->lowpassed.ensure(nm));
     CK(ctx->radial.ensure((size_t)cx * nm));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
-    for (int i = 0; i < nm; ++i) CKS(spectrum_cufft(ctx, mics[i], ctx->raw.p + cmp_n * i));
+    if (ctx->impl == GCF_SPECT_FUSED) {
+        CKS(spectrum_fused(ctx, mics, ctx->raw.p));
+    } else {
+        for (int i = 0; i < nm; ++i) CKS(spectrum_cufft(ctx, mics[i], ctx->raw.p + cmp_n * i));
+    }
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
     launch_bg_horizontal(ctx->raw.p, T, nm, ctx->log_spect, ctx->hsum.p, ctx->st);
     CKL();
@@ -764,7 +838,7 @@ gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
     ctx->dev = gpu;
     ctx->tile = tile_size;
     ctx->log_spect = log_spect ? 1 : 0;
-    ctx->impl = GCF_SPECT_CUFFT;
+    ctx->impl = fused_tile_supported(tile_size) ? GCF_SPECT_FUSED : GCF_SPECT_CUFFT;
     if (cudaSetDevice(gpu) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return GCF_ERR_CUDA;
@@ -827,6 +901,12 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->part.release();
     ctx->d_res.release();
     ctx->d_optics.release();
+    ctx->tw512.release();
+    ctx->f_desc.release();
+    ctx->f_items.release();
+    ctx->f_first.release();
+    ctx->f_inv.release();
+    ctx->f_partial.release();
     for (auto& ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -1046,7 +1126,6 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
         cudaEventDestroy(t1);
         return st;
     }
-    accumulate_stage_times(ctx);
     float pxn = mics[0].px_n;
     const gcf_optics op = *optics;
     auto full_job = [&](int idx) {
@@ -1140,6 +1219,7 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
 done:
     cudaEventRecord(t1, ctx->st);
     cudaEventSynchronize(t1);
+    accumulate_stage_times(ctx);
     float tt = 0;
     cudaEventElapsedTime(&tt, t0, t1);
     ctx->stage_ms[6] = tt;
@@ -1174,7 +1254,6 @@ gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_devi
     std::vector<MicImage> mics;
     gcf_status st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics);
     if (st == GCF_OK) {
-        accumulate_stage_times(ctx);
         std::vector<JobSpec> js(n);
         for (int i = 0; i < n; ++i) {
             std::memset(&js[i], 0, sizeof(JobSpec));
@@ -1193,6 +1272,7 @@ gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_devi
     }
     cudaEventRecord(t1, ctx->st);
     cudaEventSynchronize(t1);
+    if (st == GCF_OK) accumulate_stage_times(ctx);
     float tt = 0;
     cudaEventElapsedTime(&tt, t0, t1);
     ctx->stage_ms[6] = tt;

@@ -114,20 +114,22 @@ void launch_amp_accumulate(const float2* cmp, int tile, int ntiles, double* acc,
 void launch_finalize_raw(const double* acc, int n, double inv, float* raw, cudaStream_t st);
 void launch_fourier_crop(const float2* in, int cx_in, int cy_in, float2* out, int cx_out,
                          int cy_out, cudaStream_t st);
-int  fused_tile_supported(int tile);
-// Fused spectrum: one pass over all tiles of `nimg` images described by
-// `descs` (device), accumulating the averaged amplitude spectrum into raw.
-struct TileImage {
+// gcf_fused.cu: fused tile-spectrum kernel (tile 512).
+struct FusedImageDesc {          // layout must match FusedTab in gcf_fused.cu
     const float* img;
     int pitch;
-    int ntx, nty;
+    int ntx;
     int offx, offy, stride;
-    int tile_base;      // first global tile index of this image
-    float inv_ntiles;
+    int vec4;
 };
-void launch_fused_spectrum(const TileImage* descs, int nimg, int total_tiles, int tile,
-                           const float* taper, const float2* taper_hat, float* raw_out,
-                           float* scratch, int grid, cudaStream_t st);
+int fused_tile_supported(int tile);
+size_t fused_smem_bytes();
+cudaError_t fused_max_clusters(int* n);
+// items: (image, first tile, end tile, item index); first[img]..first[img+1]
+// are the items of image img; inv[img] = 1 / tiles of img.
+cudaError_t launch_fused(const void* descs, const int4* items, int nitems, const int* first,
+                         const float* inv, int nimg, const float* taper, const float2* tw,
+                         float* partial, float* raw, int nclusters, cudaStream_t st);
 
 // gcf_post.cu
 void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,

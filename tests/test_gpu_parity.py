@@ -164,3 +164,41 @@ def test_errors_are_status_codes(gpu_lib):
     ctx.setup(op, 100, 100)
     with pytest.raises(G.GcfError):
         ctx.gen_half_spectrum(small)
+
+
+# ---------------------------------------------------------------------------
+# 512 x 512 tiles: the fused tile-FFT kernel (default) and the cuFFT variant
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("w", [1536, 1538])   # tile starts 16-byte aligned / not aligned
+def test_fused_spectrum_matches_oracle_and_cufft(gpu_lib, oracle, w):
+    G = gpu_lib
+    img = _img(seed=21, w=w, h=1536, df=(17800.0, 18200.0), az=-10.0)
+    op = G.make_optics(pixel_size=PX)
+    fused = G.Context(0, 512, 0)   # fused is the default for 512
+    fused.setup(op, w, 1536)
+    fused.gen_half_spectrum(img)
+    gf = fused.half_spectrum(raw=True).astype(np.float64)
+    cuf = G.Context(0, 512, 0, spectrum_impl=G.GCF_SPECT_CUFFT)
+    cuf.setup(op, w, 1536)
+    cuf.gen_half_spectrum(img)
+    gc = cuf.half_spectrum(raw=True).astype(np.float64)
+    o = oracle.avg_spectrum(img, 512)
+    tol = 1e-4 * np.abs(o) + 1e-5 * o.mean()
+    assert np.all(np.abs(gf - o) <= tol), float((np.abs(gf - o) / np.abs(o)).max())
+    assert np.all(np.abs(gc - o) <= tol), float((np.abs(gc - o) / np.abs(o)).max())
+    r1, r2 = fused.do2d(), cuf.do2d()
+    p = oracle.params(pixel_size=PX, tile_size=512)
+    ores = oracle.find_ctf_image(img, PX, p)
+    _assert_result_close(r1, ores)
+    _assert_result_close(r2, ores)
+
+
+def test_fused_batch_deterministic(gpu_lib):
+    G = gpu_lib
+    imgs = [_img(seed=30 + i, w=1024 + 512 * (i % 2), h=1024, df=(15000.0, 15100.0)) for i in range(3)]
+    ctx = G.Context(0, 512, 0)
+    op = G.make_optics()
+    a = ctx.run_batch(imgs, [PX] * 3, op)
+    b = ctx.run_batch(imgs, [PX] * 3, op)
+    for x, y in zip(a, b):
+        assert x.as_dict() == y.as_dict()
