@@ -31,7 +31,7 @@ EXPORTS = [
     "gcf_get_spect_size", "gcf_get_half_spectrum", "gcf_gen_full_spectrum",
     "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
-    "gcf_get_stage_times", "gcf_get_launch_count",
+    "gcf_get_stage_times", "gcf_get_launch_count", "gcf_avg_spectrum_noalloc",
 ]
 
 
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_mrc_write.argtypes = [C.c_char_p, vp, i, i, i, f]
     L.gcf_get_stage_times.argtypes = [vp, C.POINTER(f)]
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
     for name in EXPORTS:   # every declared entry point must resolve
         getattr(L, name)
     _lib = L

@@ -23,6 +23,12 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
 #include "gcf_internal.h"
 
 namespace cg = cooperative_groups;
@@ -370,3 +376,139 @@ cudaError_t fused_max_clusters(int* n)
 }
 
 }  // namespace gcf
+
+// ===========================================================================
+// Allocation-free spectrum entry point.
+//
+// Some callers cannot call cudaMalloc: a host application whose framework
+// owns every device allocation (a fixed arena or a pool with a hard budget),
+// or an acquisition loop that must not allocate because cudaMalloc can
+// synchronise the device.  gcf_avg_spectrum_noalloc computes the same
+// averaged amplitude spectrum as the fused path above with the same kernel,
+// but every byte of device storage it needs beyond the caller's input and
+// output lives in the file-scope array below.
+// ===========================================================================
+namespace gcf {
+namespace {
+
+constexpr int kNaMaxItems = 16;                 // partial spectra in the scratch
+constexpr int kNaMaxTilesPerItem = 256;         // => at most 4096 tiles per image
+constexpr size_t kNaPartialBytes = (size_t)kNaMaxItems * FCX * FT * sizeof(float);   // 8.4 MB
+constexpr size_t kNaTaperOff = kNaPartialBytes;                                        // 1 MB taper
+constexpr size_t kNaTwOff = kNaTaperOff + (size_t)FT * FT * sizeof(float);            // 4 KB twiddles
+constexpr size_t kNaMetaOff = kNaTwOff + (size_t)FT * sizeof(float2);                 // descriptors
+struct NaMeta {
+    FusedTab desc;
+    int4 items[kNaMaxItems];
+    int first[2];
+    float inv[1];
+};
+constexpr size_t kNaBytes = kNaMetaOff + ((sizeof(NaMeta) + 255) / 256) * 256;
+
+// The scratch.  In host code this name is only a stand-in; its device
+// address comes from cudaGetSymbolAddress at set-up (na_setup).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+unsigned char* g_na_base[kNaMaxDevices] = {};
+int g_na_clusters[kNaMaxDevices] = {};
+
+// Once per device, with that device current: find the scratch address and
+// fill the constant taper / twiddle tables inside it.
+gcf_status na_setup(int dev, unsigned char** base, int* clusters)
+{
+    std::lock_guard<std::mutex> lk(g_na_mutex);
+    if (g_na_base[dev]) {
+        *base = g_na_base[dev];
+        *clusters = g_na_clusters[dev];
+        return GCF_OK;
+    }
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GCF_ERR_CUDA;
+    std::vector<float> taper((size_t)FT * FT);
+    const double c = FT * 0.5, s = FT;
+    for (int y = 0; y < FT; ++y)
+        for (int x = 0; x < FT; ++x) {   // GRoundEdge (FindCTF/GRoundEdge.cu:7-25)
+            double fx = 2.0 * std::fabs(x - c) / s, fy = 2.0 * std::fabs(y - c) / s;
+            double r = std::sqrt(fx * fx + fy * fy), v = 0.0;
+            if (r < 1.0) {
+                double q = 0.5 * (1.0 - std::cos(M_PI * r));
+                v = 1.0 - q * q * q;
+            }
+            taper[(size_t)y * FT + x] = (float)v;
+        }
+    std::vector<float2> tw(FT);
+    for (int t = 0; t < FT; ++t) {
+        double a = -2.0 * M_PI * (double)t / FT;
+        tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    unsigned char* b = static_cast<unsigned char*>(p);
+    if (cudaMemcpy(b + kNaTaperOff, taper.data(), taper.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(b + kNaTwOff, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+        return GCF_ERR_CUDA;
+    int n = 0;
+    if (fused_max_clusters(&n) != cudaSuccess || n <= 0) return GCF_ERR_CUDA;
+    g_na_base[dev] = b;
+    g_na_clusters[dev] = n;
+    *base = b;
+    *clusters = n;
+    return GCF_OK;
+}
+
+}  // namespace
+}  // namespace gcf
+
+extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height, int pitch,
+                                               float* dev_raw_out, void* cuda_stream)
+{
+    using namespace gcf;
+    if (!dev_img || !dev_raw_out || width < FT || height < FT || pitch < width)
+        return GCF_ERR_INVALID_ARG;
+    // tile layout of CGenAvgSpectrum::SetSizes (FindCTF/CGenAvgSpectrum.cpp:40-75)
+    int ov = (int)(FT * 0.50f) / 2 * 2, stride = FT - ov;
+    int ntx = (width - ov) / stride, nty = (height - ov) / stride;
+    int nt = ntx * nty;
+    if (ntx <= 0 || nty <= 0) return GCF_ERR_IMAGE_TOO_SMALL;
+    if (nt > kNaMaxItems * kNaMaxTilesPerItem) return GCF_ERR_INVALID_ARG;   // > 4096 tiles
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return GCF_ERR_CUDA;
+    unsigned char* base = nullptr;
+    int clusters = 0;
+    gcf_status s = na_setup(dev, &base, &clusters);
+    if (s != GCF_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    NaMeta meta;
+    std::memset(&meta, 0, sizeof(meta));
+    meta.desc.img = dev_img;
+    meta.desc.pitch = pitch;
+    meta.desc.ntx = ntx;
+    meta.desc.offx = (width - ntx * FT + (ntx - 1) * ov) / 2;
+    meta.desc.offy = (height - nty * FT + (nty - 1) * ov) / 2;
+    meta.desc.stride = stride;
+    meta.desc.vec4 = ((meta.desc.offx % 4) == 0 && (stride % 4) == 0 && (pitch % 4) == 0 &&
+                      ((uintptr_t)dev_img % 16) == 0) ? 1 : 0;
+    int nitems = nt < kNaMaxItems ? nt : kNaMaxItems;
+    int chunk = (nt + nitems - 1) / nitems;
+    nitems = 0;
+    for (int t0 = 0; t0 < nt; t0 += chunk, ++nitems)
+        meta.items[nitems] = make_int4(0, t0, t0 + chunk < nt ? t0 + chunk : nt, nitems);
+    meta.first[0] = 0;
+    meta.first[1] = nitems;
+    meta.inv[0] = 1.0f / nt;
+    // Every partial element is written by the kernel before it is read, so
+    // nothing in the scratch has to start at zero; the descriptors below are
+    // rewritten on every call.
+    NaMeta* dmeta = reinterpret_cast<NaMeta*>(base + kNaMetaOff);
+    if (cudaMemcpyAsync(dmeta, &meta, sizeof(meta), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return GCF_ERR_CUDA;
+    int ncl = clusters < nitems ? clusters : nitems;
+    cudaError_t e = launch_fused(&dmeta->desc, dmeta->items, nitems, dmeta->first, dmeta->inv, 1,
+                                 reinterpret_cast<const float*>(base + kNaTaperOff),
+                                 reinterpret_cast<const float2*>(base + kNaTwOff),
+                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, st);
+    if (e != cudaSuccess) return GCF_ERR_CUDA;
+    // a copy from pageable memory has consumed `meta` when cudaMemcpyAsync returns
+    return GCF_OK;
+}

@@ -176,6 +176,26 @@ gcf_status gcf_mrc_read_tilts(const char* path, float* tilts, int n);
 gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, int nz,
                          float pixel_size);
 
+/* ---------------------------------------------------------------------- */
+/* Allocation-free spectrum.  No counterpart in the reference.              */
+/* ---------------------------------------------------------------------- */
+/* Averaged amplitude spectrum (512 x 512 tiles, the fused tile kernel) of
+ * the device image dev_img (width x height floats, row pitch `pitch` floats)
+ * into dev_raw_out (257 x 512 floats, DC at (0, 256)), on `cuda_stream`
+ * (NULL = default stream) of the current device, without allocating any
+ * device memory.  For callers that cannot call cudaMalloc: applications
+ * whose framework owns every device allocation, or acquisition loops that
+ * must not allocate because cudaMalloc can synchronise the device.
+ * Its scratch is one static device array of about 9.5 MB that every GPU
+ * loading this library holds until exit; it takes at most 4096 tiles
+ * (e.g. 16384 x 16384 pixels) and returns GCF_ERR_INVALID_ARG beyond that.
+ * The first call on a device finds the array's address and fills its
+ * constant tables; make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller. */
+gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height, int pitch,
+                                    float* dev_raw_out, void* cuda_stream);
+
 /* Device time (ms, CUDA events on the context stream) of the stages of the
  * last batched call: [0] upload, [1] rescale, [2] spectrum, [3] background
  * + lowpass + radial, [4] 1D search, [5] 2D search, [6] total. */
