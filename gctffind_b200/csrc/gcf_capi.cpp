@@ -71,6 +71,8 @@ struct gcf_ctx {
     int log_spect = 0;
     int impl = GCF_SPECT_CUFFT;
     cudaStream_t st = nullptr;
+    cudaStream_t st_copy = nullptr;   // host -> device uploads
+    std::vector<cudaEvent_t> chunk_ev;
     std::string err;
     long long launches = 0;
     float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -109,7 +111,10 @@ struct gcf_ctx {
     DBuf<int4> f_items;
     DBuf<int> f_first;
     DBuf<float> f_inv, f_partial;
+    DBuf<double> f_bsum;
+    DBuf<double*> f_bsum_ptr;
     int fused_clusters = 0;
+    int fused_shape = 0;
 
     // CFindCtf2D call-shape state
     gcf_optics optics{};
@@ -429,19 +434,28 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     std::vector<int4> items;
     std::vector<int> first(nm + 1);
     std::vector<float> inv(nm);
+    std::vector<size_t> boff(nm);
+    size_t nblk = 0;
+    int max_blocks = 0;
     for (int i = 0; i < nm; ++i) {
         const MicImage& m = mics[i];
         Layout L = tile_layout(m.w, m.h, T);
         int nt = L.ntx * L.nty;
         if (L.ntx <= 0 || L.nty <= 0) return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no tile");
         d[i].img = m.img;
+        d[i].bsum = nullptr;   // set below
         d[i].pitch = m.pitch;
         d[i].ntx = L.ntx;
+        d[i].nty = L.nty;
         d[i].offx = L.offx;
         d[i].offy = L.offy;
         d[i].stride = L.stride;
-        d[i].vec4 = ((L.offx % 4) == 0 && (L.stride % 4) == 0 && (m.pitch % 4) == 0 &&
-                     ((uintptr_t)m.img % 16) == 0) ? 1 : 0;
+        d[i].vec = ((L.offx % 2) == 0 && (L.stride % 2) == 0 && (m.pitch % 2) == 0 &&
+                    ((uintptr_t)m.img % 8) == 0) ? 2 : 1;
+        d[i].nbx = L.ntx + 1;
+        boff[i] = nblk;
+        nblk += (size_t)(L.ntx + 1) * (L.nty + 1);
+        max_blocks = std::max(max_blocks, (L.ntx + 1) * (L.nty + 1));
         inv[i] = 1.0f / nt;
         first[i] = (int)items.size();
         int nch = (nt + kItemTiles - 1) / kItemTiles;
@@ -451,12 +465,21 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     }
     first[nm] = (int)items.size();
     if (ctx->fused_clusters <= 0) {
-        int n = 0;
-        CK(fused_max_clusters(&n));
+        int n = 0, shape = 0;
+        CK(fused_max_clusters(&n, &shape));
         if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
         ctx->fused_clusters = n;
+        ctx->fused_shape = shape;
     }
     int ni = (int)items.size();
+    CK(ctx->f_bsum.ensure(nblk));
+    CK(ctx->f_bsum_ptr.ensure(nm));
+    std::vector<double*> bptr(nm);
+    for (int i = 0; i < nm; ++i) {
+        bptr[i] = ctx->f_bsum.p + boff[i];
+        d[i].bsum = bptr[i];
+    }
+    CK(cudaMemcpyAsync(ctx->f_bsum_ptr.p, bptr.data(), nm * sizeof(double*), cudaMemcpyHostToDevice, ctx->st));
     CK(ctx->f_desc.ensure(nm));
     CK(ctx->f_items.ensure(ni));
     CK(ctx->f_first.ensure(nm + 1));
@@ -467,17 +490,17 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     CK(cudaMemcpyAsync(ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->f_inv.p, inv.data(), nm * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
     int ncl = std::min(ctx->fused_clusters, ni);
-    CK(launch_fused(ctx->f_desc.p, ctx->f_items.p, ni, ctx->f_first.p, ctx->f_inv.p, nm, ctx->taper.p,
-                    ctx->tw512.p, ctx->f_partial.p, raw_out, ncl, ctx->st));
-    ctx->launches += 2;
+    CK(launch_fused(ctx->f_desc.p, ctx->f_bsum_ptr.p, max_blocks, ctx->f_items.p, ni, ctx->f_first.p,
+                    ctx->f_inv.p, nm, ctx->taper.p, ctx->tw512.p, ctx->f_partial.p, raw_out, ncl,
+                    ctx->fused_shape, ctx->st));
+    ctx->launches += 3;
     return GCF_OK;
 }
 
-// CFindCtfBase::GenHalfSpectrum for n micrographs (slots 0..n-1):
-// spectrum, background removal, moments, lowpass, radial average.
-gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
+// Buffers of the spectrum stage for nm micrographs.
+gcf_status spectra_alloc(gcf_ctx* ctx, int nm)
 {
-    int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
+    int T = ctx->tile, cx = T / 2 + 1;
     size_t cmp_n = (size_t)cx * T;
     CK(ctx->raw.ensure(cmp_n * nm));
     CK(ctx->ctf0.ensure(cmp_n * nm));
@@ -487,13 +510,30 @@ gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
     CK(ctx->moments.ensure(2 * (size_t)nm));
     CK(ctx->lowpassed.ensure(nm));
     CK(ctx->radial.ensure((size_t)cx * nm));
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    return GCF_OK;
+}
+
+// CGenAvgSpectrum::DoIt for micrographs [first, first + count) of mics, into
+// their raw-spectrum slots.
+gcf_status spectra_chunk(gcf_ctx* ctx, const std::vector<MicImage>& mics, int first, int count)
+{
+    size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
+    if (count <= 0) return GCF_OK;
     if (ctx->impl == GCF_SPECT_FUSED) {
-        CKS(spectrum_fused(ctx, mics, ctx->raw.p));
+        std::vector<MicImage> sub(mics.begin() + first, mics.begin() + first + count);
+        CKS(spectrum_fused(ctx, sub, ctx->raw.p + cmp_n * first));
     } else {
-        for (int i = 0; i < nm; ++i) CKS(spectrum_cufft(ctx, mics[i], ctx->raw.p + cmp_n * i));
+        for (int i = first; i < first + count; ++i) CKS(spectrum_cufft(ctx, mics[i], ctx->raw.p + cmp_n * i));
     }
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    return GCF_OK;
+}
+
+// CFindCtfBase::mRemoveBackground/mLowpass and CFindCtf1D::mCalcRadialAverage
+// for slots 0..nm-1.
+gcf_status spectra_post(gcf_ctx* ctx, int nm)
+{
+    int T = ctx->tile, cx = T / 2 + 1;
+    size_t cmp_n = (size_t)cx * T;
     launch_bg_horizontal(ctx->raw.p, T, nm, ctx->log_spect, ctx->hsum.p, ctx->st);
     CKL();
     launch_bg_vertical(ctx->raw.p, ctx->hsum.p, T, nm, ctx->log_spect, ctx->ctf0.p, ctx->st);
@@ -506,6 +546,19 @@ gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
     launch_radial(ctx->ctf.p, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p, ctx->st);
     CKL();
     ctx->launches += 6;
+    return GCF_OK;
+}
+
+// CFindCtfBase::GenHalfSpectrum for n micrographs (slots 0..n-1):
+// spectrum, background removal, moments, lowpass, radial average.
+gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
+{
+    int nm = (int)mics.size();
+    CKS(spectra_alloc(ctx, nm));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CKS(spectra_chunk(ctx, mics, 0, nm));
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CKS(spectra_post(ctx, nm));
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
     return GCF_OK;
 }
@@ -699,68 +752,99 @@ bool valid_optics(const gcf_optics* o)
 }
 
 // Uploads (if needed), rescales and produces the spectra of n images.
+// One image through CRescaleImage (FindCTF/CRescaleImage.cpp:47-99) to the
+// MicImage the spectrum stage reads.
+gcf_status stage_image(gcf_ctx* ctx, const float* dimg, int w, int h, float px, float* rescale_dst,
+                       MicImage& m, size_t* used)
+{
+    bool copied = false;
+    int nw, nh;
+    float pn;
+    CKS(rescale_device(ctx, dimg, w, h, px, rescale_dst, &nw, &nh, &pn, &copied));
+    *used = 0;
+    if (copied) {
+        m.img = rescale_dst;
+        m.pitch = nw;
+        *used = (size_t)nw * nh;
+    } else {
+        m.img = dimg;
+        m.pitch = w;
+    }
+    m.w = nw;
+    m.h = nh;
+    m.px_n = pn;
+    Layout L = tile_layout(m.w, m.h, ctx->tile);
+    if (L.ntx <= 0 || L.nty <= 0 || m.w < ctx->tile || m.h < ctx->tile)
+        return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no full tile");
+    return GCF_OK;
+}
+
+// Uploads (host inputs), rescales and produces the spectra of n images.
+// Host inputs are uploaded in chunks on a copy stream so that the upload of
+// chunk c+1 overlaps the rescale and spectrum of chunk c.
 gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* ws, const int* hs,
                           const float* pxs, int n, int on_device, std::vector<MicImage>& mics)
 {
-    mics.clear();
+    mics.assign(n, MicImage{});
     size_t tot_raw = 0, tot_new = 0;
-    std::vector<int> nws(n), nhs(n);
-    std::vector<float> pxn(n);
     for (int i = 0; i < n; ++i) {
-        gcf_rescale_dims(ws[i], hs[i], pxs[i], &nws[i], &nhs[i], &pxn[i]);
-        tot_raw += (size_t)ws[i] * hs[i];
-        float bin = 1.2f / pxs[i];
-        if (bin > 1) tot_new += (size_t)nws[i] * nhs[i];
-    }
-    CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    std::vector<const float*> dimg(n);
-    if (!on_device) {
-        CK(ctx->images.ensure(tot_raw));
-        size_t off = 0;
-        for (int i = 0; i < n; ++i) {
-            size_t cnt = (size_t)ws[i] * hs[i];
-            CK(cudaMemcpyAsync(ctx->images.p + off, images[i], cnt * sizeof(float),
-                               cudaMemcpyHostToDevice, ctx->st));
-            dimg[i] = ctx->images.p + off;
-            off += cnt;
-        }
-    } else {
-        for (int i = 0; i < n; ++i) dimg[i] = images[i];
-    }
-    CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    if (tot_new) CK(ctx->rescaled.ensure(tot_new));
-    size_t off = 0;
-    for (int i = 0; i < n; ++i) {
-        MicImage m;
-        bool copied = false;
         int nw, nh;
         float pn;
-        float* dst = tot_new ? ctx->rescaled.p + off : nullptr;
-        CKS(rescale_device(ctx, dimg[i], ws[i], hs[i], pxs[i], dst, &nw, &nh, &pn, &copied));
-        if (copied) {
-            m.img = dst;
-            m.pitch = nw;
-            off += (size_t)nw * nh;
-        } else {
-            m.img = dimg[i];
-            m.pitch = ws[i];
-        }
-        m.w = nw;
-        m.h = nh;
-        m.px_n = pn;
-        Layout L = tile_layout(m.w, m.h, ctx->tile);
-        if (L.ntx <= 0 || L.nty <= 0 || m.w < ctx->tile || m.h < ctx->tile)
-            return fail(ctx, GCF_ERR_IMAGE_TOO_SMALL, "image holds no full tile");
-        mics.push_back(m);
+        gcf_rescale_dims(ws[i], hs[i], pxs[i], &nw, &nh, &pn);
+        tot_raw += (size_t)ws[i] * hs[i];
+        float bin = 1.2f / pxs[i];
+        if (bin > 1) tot_new += (size_t)nw * nh;
     }
-    return spectra(ctx, mics);
+    CKS(spectra_alloc(ctx, n));
+    if (tot_new) CK(ctx->rescaled.ensure(tot_new));
+    if (!on_device) CK(ctx->images.ensure(tot_raw));
+    const int kChunk = on_device ? n : 8;
+    const int nchunks = (n + kChunk - 1) / kChunk;
+    while ((int)ctx->chunk_ev.size() < nchunks) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->chunk_ev.push_back(e);
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    if (!on_device) CK(cudaStreamWaitEvent(ctx->st_copy, ctx->ev[0], 0));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    size_t roff = 0, roff_new = 0;
+    for (int c = 0; c < nchunks; ++c) {
+        int i0 = c * kChunk, i1 = std::min(n, i0 + kChunk);
+        std::vector<const float*> dimg(i1 - i0);
+        if (!on_device) {
+            for (int i = i0; i < i1; ++i) {
+                size_t cnt = (size_t)ws[i] * hs[i];
+                CK(cudaMemcpyAsync(ctx->images.p + roff, images[i], cnt * sizeof(float),
+                                   cudaMemcpyHostToDevice, ctx->st_copy));
+                dimg[i - i0] = ctx->images.p + roff;
+                roff += cnt;
+            }
+            CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st_copy));
+            if (c == nchunks - 1) CK(cudaEventRecord(ctx->ev[1], ctx->st_copy));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
+        } else {
+            for (int i = i0; i < i1; ++i) dimg[i - i0] = images[i];
+            if (c == 0) CK(cudaEventRecord(ctx->ev[1], ctx->st));
+        }
+        for (int i = i0; i < i1; ++i) {
+            size_t used = 0;
+            float* dst = tot_new ? ctx->rescaled.p + roff_new : nullptr;
+            CKS(stage_image(ctx, dimg[i - i0], ws[i], hs[i], pxs[i], dst, mics[i], &used));
+            roff_new += used;
+        }
+        CKS(spectra_chunk(ctx, mics, i0, i1 - i0));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CKS(spectra_post(ctx, n));
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    return GCF_OK;
 }
 
 void accumulate_stage_times(gcf_ctx* ctx)
 {
     float t;
     if (cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]) == cudaSuccess) ctx->stage_ms[0] += t;
-    if (cudaEventElapsedTime(&t, ctx->ev[1], ctx->ev[2]) == cudaSuccess) ctx->stage_ms[1] += t;
     if (cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev[3]) == cudaSuccess) ctx->stage_ms[2] += t;
     if (cudaEventElapsedTime(&t, ctx->ev[3], ctx->ev[4]) == cudaSuccess) ctx->stage_ms[3] += t;
 }
@@ -839,7 +923,9 @@ gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
     ctx->tile = tile_size;
     ctx->log_spect = log_spect ? 1 : 0;
     ctx->impl = fused_tile_supported(tile_size) ? GCF_SPECT_FUSED : GCF_SPECT_CUFFT;
-    if (cudaSetDevice(gpu) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaSetDevice(gpu) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->st_copy, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return GCF_ERR_CUDA;
     }
@@ -858,6 +944,7 @@ void gcf_destroy(gcf_ctx* ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->dev);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    if (ctx->st_copy) cudaStreamSynchronize(ctx->st_copy);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
     for (auto* b : ctx->bands) {
         b->idx.release();
@@ -907,8 +994,12 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->f_first.release();
     ctx->f_inv.release();
     ctx->f_partial.release();
+    ctx->f_bsum.release();
+    ctx->f_bsum_ptr.release();
     for (auto& ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
+    if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }

@@ -2,24 +2,26 @@
 // (CGenAvgSpectrum::DoIt + GCalcMoment2D + GNormalize2D + GRoundEdge +
 //  GCalcSpectrum::DoPad + GAddImages, FindCTF/CGenAvgSpectrum.cpp:77-139).
 //
-// One thread-block cluster of 8 CTAs owns one tile at a time; the tile never
-// leaves the chip:
-//   load    CTA r reads tile rows [64r, 64r+64) (coalesced float4 when the
-//           tile start is 16-byte aligned) into its shared memory and sums
-//           them; the 8 partial sums are combined over distributed shared
-//           memory (DSMEM), so every CTA holds the same tile mean;
-//   rows    each warp transforms two rows at once ((x - mean) * taper as the
-//           real and imaginary parts of one 512-point complex FFT held in
-//           registers, 16 values per lane, radix-16 x radix-32 with one
-//           shared-memory transpose) and splits the result into the two
-//           257-bin half spectra, written back in place;
-//   columns each warp gathers one frequency column (512 rows) straight from
-//           the 8 CTAs' shared memory over DSMEM and transforms it; the
-//           real kx = 0 and kx = 256 columns share one complex FFT;
+// A thread-block cluster of CL CTAs (16, or 8 where 16-CTA clusters do not
+// fit) owns one tile at a time; the tile never leaves the chip:
+//   mean    every tile mean comes from one pass of k_block_sums over the
+//           images (a 512 tile is 2 x 2 blocks of 256 x 256);
+//   rows    each warp reads two tile rows straight from global memory,
+//           forms (x - mean) * taper as the real and imaginary parts of one
+//           512-point complex FFT held in registers (16 values per lane,
+//           radix-16 x radix-32 with one shared-memory transpose), splits
+//           the result into the two rows' 257-bin half spectra and pushes
+//           each bin into the shared memory of the CTA that owns its
+//           frequency column (16-byte DSMEM stores, [column][row]);
+//   columns each warp transforms one frequency column (512 rows) read from
+//           its own CTA's shared memory; the real kx = 0 and kx = 256
+//           columns share one complex FFT;
 //   |F|     amplitudes (DC moved to row 256) accumulate in registers across
 //           all tiles of a work item and are written once.
-// Work items are (image, tile range) pairs; their partial spectra are summed
-// in item order by k_item_reduce, so the result is deterministic.
+// With CL = 16 the column buffer is double-buffered, so one cluster barrier
+// per tile separates writers from readers.  Work items are (image, tile
+// range) pairs; their partial spectra are summed in item order by
+// k_item_reduce, so the result is deterministic.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -39,20 +41,7 @@ namespace {
 
 constexpr int FT = 512;          // tile edge
 constexpr int FCX = FT / 2 + 1;  // 257 half-spectrum columns
-constexpr int FCL = 8;           // CTAs per cluster
-constexpr int FROWS = FT / FCL;  // 64 rows per CTA
-constexpr int FTHR = 256;        // threads per CTA
-constexpr int FWARPS = FTHR / 32;
-constexpr int FNR = 32 / FWARPS;  // column rounds per tile (32 columns per CTA)
-constexpr int FRS = FCX;         // row stride of the row buffer, float2 units
 constexpr int FSCR = 16 * 33;    // per-warp scratch, float2 units
-
-constexpr size_t kRowBytes = (size_t)FROWS * FRS * sizeof(float2);     // 131584
-constexpr size_t kScrBytes = (size_t)FWARPS * FSCR * sizeof(float2);   // 67584
-constexpr size_t kTwBytes = (size_t)FT * sizeof(float2);               // 4096
-constexpr size_t kAccNBytes = (size_t)FT * sizeof(float);              // 2048
-constexpr size_t kPartBytes = 32 * sizeof(double);   // 16 warp sums + CTA sum
-constexpr size_t kFusedSmem = kRowBytes + kScrBytes + kTwBytes + kAccNBytes + kPartBytes;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
@@ -96,26 +85,24 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 {
 #pragma unroll
     for (int n2 = 0; n2 < 4; ++n2) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
-    // v[4 k1 + n2] now holds stage-A output (k1, n2); twiddle W16^(n2 k1)
 #pragma unroll
     for (int k1 = 1; k1 < 4; ++k1)
 #pragma unroll
         for (int n2 = 1; n2 < 4; ++n2) v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w16(n2 * k1));
-    // stage C: DFT over n2 for each k1 -> X[k1 + 4 k2]
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) dft4(v[4 * k1 + 0], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
-    // X[k] now sits in v[P16(k)]: the digit reversal is left to the caller's
-    // compile-time indexing instead of register moves.
 }
 
 // 512-point forward FFT held by one warp.  In: lane l holds x[32 j + l] in
-// v[j].  Out: lane 2m+p holds X[m + 16 k + 256 p] in v[P16(k)].  scr: 528 float2
-// of warp-private shared memory; tw: exp(-2 pi i t / 512), t < 512.
-__device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* tw, int lane)
+// v[j].  Out: lane 2m+p holds X[m + 16 k + 256 p] in v[P16(k)].
+// scr: 528 float2 of warp-private shared memory; twl[k1 * 32 + l] =
+// exp(-2 pi i l k1 / 512); tw32[k] = exp(-2 pi i k / 32).
+__device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* twl,
+                                            const float2* tw32, int lane)
 {
     dft16(v);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) v[P16(k1)] = cmul(v[P16(k1)], tw[(lane * k1) & (FT - 1)]);
+    for (int k1 = 1; k1 < 16; ++k1) v[P16(k1)] = cmul(v[P16(k1)], twl[k1 * 32 + lane]);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) scr[k1 * 33 + lane] = v[P16(k1)];
@@ -124,154 +111,212 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = scr[m * 33 + 2 * q + p];
     dft16(v);
+    const float sg = p ? -1.0f : 1.0f;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         float2 mine = v[P16(k)];
         float2 o;
         o.x = __shfl_xor_sync(0xffffffffu, mine.x, 1);
         o.y = __shfl_xor_sync(0xffffffffu, mine.y, 1);
+        // lane p = 0: E0 + W E1 with E0 = mine, E1 = o;  p = 1: E0 - W E1 with E0 = o, E1 = mine
         float2 e0 = p ? o : mine;
         float2 e1 = p ? mine : o;
-        float2 t = cmul(tw[16 * k], e1);
-        v[P16(k)] = p ? csub(e0, t) : cadd(e0, t);
+        float2 t = cmul(tw32[k], e1);
+        v[P16(k)] = make_float2(fmaf(sg, t.x, e0.x), fmaf(sg, t.y, e0.y));
     }
     __syncwarp();
 }
 
 struct FusedTab {
     const float* img;
+    const double* bsum;   // sums of the stride x stride blocks, [nty + 1][ntx + 1]
     int pitch;
-    int ntx;
+    int ntx, nty;
     int offx, offy, stride;
-    int vec4;   // 1 when every tile row start is 16-byte aligned
+    int vec;              // 2: 8-byte aligned tile rows, 1: 4-byte
+    int nbx;              // ntx + 1
 };
 
-__global__ void __cluster_dims__(FCL, 1, 1) __launch_bounds__(FTHR, 1)
+// Sums of the stride x stride blocks that tile every image (tile = 2 stride,
+// so a tile is 2 x 2 blocks): one pass over the images gives every tile mean
+// of GCalcMoment2D (Util/GCalcMoment2D.cu:10-58) without a second read.
+__global__ void k_block_sums(const FusedTab* __restrict__ imgs, double* const* __restrict__ out)
+{
+    __shared__ double sh[32];
+    const FusedTab im = imgs[blockIdx.y];
+    const int nby = im.nty + 1;
+    const int b = blockIdx.x;
+    if (b >= im.nbx * nby) return;
+    const int bx = b % im.nbx, by = b / im.nbx, S = im.stride;
+    const float* src = im.img + (size_t)(im.offy + by * S) * im.pitch + im.offx + bx * S;
+    double s = 0.0;
+    for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+        int y = k / S, x = k - y * S;
+        s += (double)__ldg(src + (size_t)y * im.pitch + x);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        out[blockIdx.y][b] = t;
+    }
+}
+
+// Compile-time shape of one cluster configuration.
+template <int CL_, int NW_, bool DB_>
+struct FusedShape {
+    static constexpr int CL = CL_;                   // CTAs per cluster
+    static constexpr int NW = NW_;                   // warps per CTA
+    static constexpr bool DB = DB_;                  // double-buffered column buffer
+    static constexpr int THR = NW * 32;
+    static constexpr int R = FT / CL;                // tile rows per CTA
+    static constexpr int C = FT / 2 / CL;            // frequency columns per CTA
+    static constexpr int PW = R / 2 / NW;            // row pairs per warp
+    static constexpr int NR = C / NW;                // column rounds per warp
+    static constexpr int YS = FT + 2;                // column stride of the buffer (16-byte rows, pad)
+    static constexpr size_t BUF = (size_t)C * YS * sizeof(float2);   // this CTA's C columns x 512 rows
+    static constexpr size_t SCR = (size_t)NW * FSCR * sizeof(float2);
+    static constexpr size_t TWL = 16 * 32 * sizeof(float2);
+    static constexpr size_t TW32 = 16 * sizeof(float2);
+    static constexpr size_t ACCN = FT * sizeof(float);
+    static constexpr size_t SMEM = (DB ? 2 : 1) * BUF + SCR + TWL + TW32 + ACCN;
+    static_assert(R % 32 == 0 && PW >= 1 && NR >= 1 && R / 2 == PW * NW && C == NR * NW && C <= 32, "shape");
+};
+using Shape16 = FusedShape<16, 16, true>;   // 16-CTA clusters, 512 threads
+using Shape8 = FusedShape<8, 8, false>;     // 8-CTA clusters, 256 threads
+
+template <class S>
+__global__ void __launch_bounds__(S::THR, 1)
 k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ items, int nitems,
                  const float* __restrict__ taper, const float2* __restrict__ twg,
                  float* __restrict__ partial)
 {
+    constexpr int CL = S::CL, NW = S::NW, R = S::R, C = S::C, PW = S::PW, NR = S::NR, YS = S::YS;
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* rowbuf = reinterpret_cast<float2*>(smem);
-    float2* scr_all = reinterpret_cast<float2*>(smem + kRowBytes);
-    float2* tw = reinterpret_cast<float2*>(smem + kRowBytes + kScrBytes);
-    float* accN = reinterpret_cast<float*>(smem + kRowBytes + kScrBytes + kTwBytes);
-    double* part = reinterpret_cast<double*>(smem + kRowBytes + kScrBytes + kTwBytes + kAccNBytes);
+    float2* colbuf0 = reinterpret_cast<float2*>(smem);
+    float2* scr_all = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF);
+    float2* twl = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF + S::SCR);
+    float2* tw32 = twl + 16 * 32;
+    float* accN = reinterpret_cast<float*>(tw32 + 16);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int r = (int)cluster.block_rank();
-    const int cid = blockIdx.x / FCL;
-    const int ncl = gridDim.x / FCL;
+    const int cid = blockIdx.x / CL;
+    const int ncl = gridDim.x / CL;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m = lane >> 1, p = lane & 1;
     float2* scr = scr_all + warp * FSCR;
-    float* rowf = reinterpret_cast<float*>(rowbuf);
 
-    for (int i = tid; i < FT; i += FTHR) tw[i] = twg[i];
+    // per-lane twiddles exp(-2 pi i l k1 / 512) and the 32-point ones
+    for (int i = tid; i < 16 * 32; i += S::THR) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
+    if (tid < 16) tw32[tid] = twg[16 * tid];
     __syncthreads();
 
+    int par = 0;   // column-buffer parity (double buffering)
     for (int it = cid; it < nitems; it += ncl) {
         const int4 item = items[it];   // (image, first tile, end tile, item index)
         const FusedTab im = imgs[item.x];
-        float acc[FNR][16];
+        float acc[NR][16];
 #pragma unroll
-        for (int a = 0; a < FNR; ++a)
+        for (int a = 0; a < NR; ++a)
 #pragma unroll
             for (int k = 0; k < 16; ++k) acc[a][k] = 0.0f;
-        for (int i = tid; i < FT; i += FTHR) accN[i] = 0.0f;
+        for (int i = tid; i < FT; i += S::THR) accN[i] = 0.0f;
 
         for (int t = item.y; t < item.z; ++t) {
             const int tx = t % im.ntx, ty = t / im.ntx;
-            const float* src = im.img + (size_t)(im.offy + ty * im.stride + r * FROWS) * im.pitch +
+            const float* src = im.img + (size_t)(im.offy + ty * im.stride + r * R) * im.pitch +
                                im.offx + tx * im.stride;
-            cluster.sync();   // peers are done with this CTA's row buffer
-            // ---- load 64 rows, partial sum -------------------------------------
-            double s = 0.0;
-            if (im.vec4) {
-#pragma unroll 4
-                for (int i = 0; i < FROWS * FT / 4 / FTHR; ++i) {
-                    int q = tid + i * FTHR;
-                    int row = q >> 7, c4 = (q & 127) * 4;
-                    float4 x = __ldg(reinterpret_cast<const float4*>(src + (size_t)row * im.pitch + c4));
-                    float* d = rowf + row * (2 * FRS) + c4;
-                    reinterpret_cast<float2*>(d)[0] = make_float2(x.x, x.y);
-                    reinterpret_cast<float2*>(d)[1] = make_float2(x.z, x.w);
-                    s += (double)x.x + (double)x.y + (double)x.z + (double)x.w;
-                }
-            } else {
-                for (int i = 0; i < FROWS * FT / FTHR; ++i) {
-                    int q = tid + i * FTHR;
-                    int row = q >> 9, c = q & (FT - 1);
-                    float x = __ldg(src + (size_t)row * im.pitch + c);
-                    rowf[row * (2 * FRS) + c] = x;
-                    s += (double)x;
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) part[warp] = s;
-            __syncthreads();
-            if (tid == 0) {
-                double b = 0.0;
-                for (int w = 0; w < FWARPS; ++w) b += part[w];
-                part[FWARPS] = b;   // CTA sum
-            }
-            cluster.sync();   // CTA sums visible cluster-wide
-            double tot = 0.0;
-#pragma unroll
-            for (int q = 0; q < FCL; ++q) tot += *cluster.map_shared_rank(part + FWARPS, q);
-            const float mean = (float)(tot / ((double)FT * FT));
+            // tile mean = four block sums / tile area
+            const double* bs = im.bsum + (size_t)ty * im.nbx + tx;
+            const float mean = (float)((bs[0] + bs[1] + bs[im.nbx] + bs[im.nbx + 1]) / ((double)FT * FT));
+            float2* colbuf = colbuf0 + (S::DB ? (size_t)par * (S::BUF / sizeof(float2)) : 0);
+            if (!S::DB) cluster.sync();   // peers are done reading this CTA's column buffer
 
-            // ---- row transforms: two rows per FFT -------------------------------
-#pragma unroll 1
-            for (int pp = warp; pp < FROWS / 2; pp += FWARPS) {
-                const int y0 = 2 * pp, Y0 = r * FROWS + y0;
+            // ---- row transforms: two rows per FFT, rows read straight from global ----
+            float na[16], nb[16];
+            {
+                const float* ga = src + (size_t)(2 * warp) * im.pitch;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    na[j] = __ldg(ga + 32 * j + lane);
+                    nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                }
+            }
+#pragma unroll
+            for (int q4 = 0; q4 < PW; ++q4) {
+                const int pp = warp + q4 * NW;
+                const int y0 = 2 * pp, Y0 = r * R + y0;
+                float ca[16], cb[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    ca[j] = na[j];
+                    cb[j] = nb[j];
+                }
+                if (q4 + 1 < PW) {   // prefetch the next row pair
+                    const float* ga = src + (size_t)(2 * (pp + NW)) * im.pitch;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        na[j] = __ldg(ga + 32 * j + lane);
+                        nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                    }
+                }
                 float2 v[16];
                 const float* ta = taper + (size_t)Y0 * FT;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     int X = 32 * j + lane;
-                    float a = (rowf[y0 * (2 * FRS) + X] - mean) * __ldg(ta + X);
-                    float b = (rowf[(y0 + 1) * (2 * FRS) + X] - mean) * __ldg(ta + FT + X);
-                    v[j] = make_float2(a, b);
+                    v[j] = make_float2((ca[j] - mean) * __ldg(ta + X), (cb[j] - mean) * __ldg(ta + FT + X));
                 }
-                fft512_warp(v, scr, tw, lane);
+                fft512_warp(v, scr, twl, tw32, lane);
 #pragma unroll
                 for (int k = 0; k < 16; ++k) scr[m + 16 * k + 256 * p] = v[P16(k)];
                 __syncwarp();
+                // split into the two rows' half spectra and push bin K of both rows
+                // into the shared memory of CTA K / C (column K % C, rows Y0, Y0 + 1)
 #pragma unroll
-                for (int i = 0; i < 9; ++i) {
-                    int K = lane + 32 * i;
-                    if (K <= FT / 2) {
-                        float2 zk = scr[K], zn = scr[(FT - K) & (FT - 1)];
-                        float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-                        float2 B = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
-                        rowbuf[y0 * FRS + K] = A;
-                        rowbuf[(y0 + 1) * FRS + K] = B;
+                for (int i = 0; i < 8; ++i) {
+                    const int K = lane + 32 * i;
+                    float2 zk = scr[K], zn = scr[(FT - K) & (FT - 1)];
+                    float4 AB = make_float4(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y),
+                                            0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+                    if (K == 0) {   // pack the real DC and Nyquist bins of both rows
+                        float2 zh = scr[FT / 2];
+                        AB = make_float4(zk.x, zh.x, zk.y, zh.y);
                     }
+                    float2* dst = cluster.map_shared_rank(colbuf, K / C) + (size_t)(K % C) * YS + Y0;
+                    *reinterpret_cast<float4*>(dst) = AB;
                 }
                 __syncwarp();
             }
-            cluster.sync();   // every row buffer of the cluster is complete
+            // every column buffer of the cluster is complete (with double
+            // buffering this also tells writers of the other buffer that its
+            // previous readers are done)
+            cluster.sync();
 
-            // ---- column transforms over DSMEM -----------------------------------
-#pragma unroll
-            for (int rho = 0; rho < FNR; ++rho) {
-                const int c = 32 * r + FWARPS * rho + warp;   // 0 = packed (kx 0, kx 256)
-                float2 v[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    // rows 32 j + lane live in CTA j / 2 at local row 32 (j & 1) + lane
-                    const float2* peer = cluster.map_shared_rank(rowbuf, j >> 1);
-                    int lr = 32 * (j & 1) + lane;
-                    if (c == 0) {
-                        v[j] = make_float2(peer[lr * FRS].x, peer[lr * FRS + FT / 2].x);
-                    } else {
-                        v[j] = peer[lr * FRS + c];
-                    }
+            // ---- column transforms from local shared memory ---------------------
+            if (t + 1 < item.z) {   // next tile's rows into L2 while the columns run
+                const int t1 = t + 1, tx1 = t1 % im.ntx, ty1 = t1 / im.ntx;
+                const float* src1 = im.img + (size_t)(im.offy + ty1 * im.stride + r * R) * im.pitch +
+                                    im.offx + tx1 * im.stride;
+                for (int q = tid; q < R * 16; q += S::THR) {   // 128-byte lines
+                    const float* g = src1 + (size_t)(q >> 4) * im.pitch + (q & 15) * 32;
+                    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(g));
                 }
-                fft512_warp(v, scr, tw, lane);
-                if (c != 0) {
+            }
+#pragma unroll
+            for (int rho = 0; rho < NR; ++rho) {
+                const int cl = NW * rho + warp;   // local column
+                const int K = C * r + cl;         // frequency bin; 0 = packed (0, 256)
+                float2 v[16];
+                const float2* col = colbuf + (size_t)cl * YS;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = col[32 * j + lane];
+                fft512_warp(v, scr, twl, tw32, lane);
+                if (K != 0) {
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         float2 z = v[P16(k)];
@@ -283,22 +328,23 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                     __syncwarp();
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
-                        int K = m + 16 * k + 256 * p;
-                        float2 zk = v[P16(k)], zn = scr[(FT - K) & (FT - 1)];
+                        int Kk = m + 16 * k + 256 * p;
+                        float2 zk = v[P16(k)], zn = scr[(FT - Kk) & (FT - 1)];
                         float ax = 0.5f * (zk.x + zn.x), ay = 0.5f * (zk.y - zn.y);
                         float bx = 0.5f * (zk.y + zn.y), by = -0.5f * (zk.x - zn.x);
                         acc[rho][k] += sqrtf(ax * ax + ay * ay);
-                        accN[K] += sqrtf(bx * bx + by * by);
+                        accN[Kk] += sqrtf(bx * bx + by * by);
                     }
                     __syncwarp();
                 }
             }
+            par ^= 1;
         }
         // ---- write this item's partial spectrum (DC moved to row 256) -----------
         float* out = partial + (size_t)item.w * FCX * FT;
 #pragma unroll
-        for (int rho = 0; rho < FNR; ++rho) {
-            const int kx = 32 * r + FWARPS * rho + warp;
+        for (int rho = 0; rho < NR; ++rho) {
+            const int kx = C * r + NW * rho + warp;
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
                 int ky = m + 16 * k + 256 * p;
@@ -310,11 +356,12 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
         if (r == 0 && warp == 0) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
-                int K = m + 16 * k + 256 * p;
-                int yd = (K + FT / 2) & (FT - 1);
-                out[(size_t)yd * FCX + FT / 2] = accN[K];
+                int Kk = m + 16 * k + 256 * p;
+                int yd = (Kk + FT / 2) & (FT - 1);
+                out[(size_t)yd * FCX + FT / 2] = accN[Kk];
             }
         }
+        __syncthreads();
     }
     cluster.sync();   // keep shared memory alive until every peer is done
 }
@@ -332,47 +379,95 @@ __global__ void k_item_reduce(const float* __restrict__ partial, const int* __re
     raw[(size_t)img * n + i] = (float)(s * (double)inv[img]);
 }
 
+template <class S>
+cudaLaunchConfig_t fused_cfg(int nclusters, cudaStream_t st, cudaLaunchAttribute* attr)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nclusters * S::CL, 1, 1);
+    cfg.blockDim = dim3(S::THR, 1, 1);
+    cfg.dynamicSmemBytes = S::SMEM;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = S::CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+template <class S>
+cudaError_t prepare_kernel()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_fused_spectrum<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)S::SMEM);
+    if (e != cudaSuccess) return e;
+    if (S::CL > 8) e = cudaFuncSetAttribute(k_fused_spectrum<S>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+}
+
+template <class S>
+cudaError_t max_clusters(int* n)
+{
+    *n = 0;
+    cudaError_t e = prepare_kernel<S>();
+    if (e != cudaSuccess) return e;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = fused_cfg<S>(64, nullptr, attr);
+    return cudaOccupancyMaxActiveClusters(n, (void*)k_fused_spectrum<S>, &cfg);
+}
+
 }  // namespace
 
 int fused_tile_supported(int tile) { return tile == FT ? 1 : 0; }
 
-size_t fused_smem_bytes() { return kFusedSmem; }
+// Picks the cluster shape that covers the most SMs: 16-CTA clusters (double
+// buffered) when the device can co-schedule them, else 8-CTA clusters.
+cudaError_t fused_max_clusters(int* n, int* shape)
+{
+    int n16 = 0, n8 = 0;
+    if (max_clusters<Shape16>(&n16) != cudaSuccess) {
+        cudaGetLastError();
+        n16 = 0;
+    }
+    cudaError_t e = max_clusters<Shape8>(&n8);
+    if (e != cudaSuccess && n16 == 0) return e;
+    if (n16 * 16 >= n8 * 8 && n16 > 0) {
+        *n = n16;
+        *shape = 16;
+    } else {
+        *n = n8;
+        *shape = 8;
+    }
+    return cudaSuccess;
+}
 
 // Host launcher.  descs/items/first/inv are device arrays prepared by the caller.
-cudaError_t launch_fused(const void* descs, const int4* items, int nitems, const int* first,
-                         const float* inv, int nimg, const float* taper, const float2* tw,
-                         float* partial, float* raw, int nclusters, cudaStream_t st)
+cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
+                         int nitems, const int* first, const float* inv, int nimg, const float* taper,
+                         const float2* tw, float* partial, float* raw, int nclusters, int shape,
+                         cudaStream_t st)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_fused_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kFusedSmem);
-    if (e != cudaSuccess) return e;
     if (nclusters < 1) nclusters = 1;
-    k_fused_spectrum<<<nclusters * FCL, FTHR, kFusedSmem, st>>>(
-        reinterpret_cast<const FusedTab*>(descs), items, nitems, taper, tw, partial);
-    e = cudaGetLastError();
+    k_block_sums<<<dim3(max_blocks, nimg), 256, 0, st>>>(reinterpret_cast<const FusedTab*>(descs), bsum_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cudaLaunchAttribute attr[1];
+    if (shape == 16) {
+        if ((e = prepare_kernel<Shape16>()) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = fused_cfg<Shape16>(nclusters, st, attr);
+        e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16>, reinterpret_cast<const FusedTab*>(descs), items,
+                               nitems, taper, tw, partial);
+    } else {
+        if ((e = prepare_kernel<Shape8>()) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = fused_cfg<Shape8>(nclusters, st, attr);
+        e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape8>, reinterpret_cast<const FusedTab*>(descs), items,
+                               nitems, taper, tw, partial);
+    }
     if (e != cudaSuccess) return e;
     dim3 g((FCX * FT + 255) / 256, nimg);
     k_item_reduce<<<g, 256, 0, st>>>(partial, first, inv, raw);
     return cudaGetLastError();
-}
-
-cudaError_t fused_max_clusters(int* n)
-{
-    cudaError_t e = cudaFuncSetAttribute(k_fused_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kFusedSmem);
-    if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(FCL * 64, 1, 1);
-    cfg.blockDim = dim3(FTHR, 1, 1);
-    cfg.dynamicSmemBytes = kFusedSmem;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = FCL;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(n, (void*)k_fused_spectrum, &cfg);
 }
 
 }  // namespace gcf
@@ -396,9 +491,12 @@ constexpr int kNaMaxTilesPerItem = 256;         // => at most 4096 tiles per ima
 constexpr size_t kNaPartialBytes = (size_t)kNaMaxItems * FCX * FT * sizeof(float);   // 8.4 MB
 constexpr size_t kNaTaperOff = kNaPartialBytes;                                        // 1 MB taper
 constexpr size_t kNaTwOff = kNaTaperOff + (size_t)FT * FT * sizeof(float);            // 4 KB twiddles
-constexpr size_t kNaMetaOff = kNaTwOff + (size_t)FT * sizeof(float2);                 // descriptors
+constexpr size_t kNaBsumOff = kNaTwOff + (size_t)FT * sizeof(float2);                 // block sums
+constexpr int kNaMaxBlocks = 2 * kNaMaxItems * kNaMaxTilesPerItem + 2;                 // (ntx+1)(nty+1)
+constexpr size_t kNaMetaOff = kNaBsumOff + (size_t)kNaMaxBlocks * sizeof(double);      // descriptors
 struct NaMeta {
     FusedTab desc;
+    double* bsum_ptr[1];
     int4 items[kNaMaxItems];
     int first[2];
     float inv[1];
@@ -413,6 +511,7 @@ constexpr int kNaMaxDevices = 64;
 std::mutex g_na_mutex;
 unsigned char* g_na_base[kNaMaxDevices] = {};
 int g_na_clusters[kNaMaxDevices] = {};
+int g_na_shape[kNaMaxDevices] = {};
 
 // Once per device, with that device current: find the scratch address and
 // fill the constant taper / twiddle tables inside it.
@@ -448,10 +547,11 @@ gcf_status na_setup(int dev, unsigned char** base, int* clusters)
             cudaSuccess ||
         cudaMemcpy(b + kNaTwOff, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
         return GCF_ERR_CUDA;
-    int n = 0;
-    if (fused_max_clusters(&n) != cudaSuccess || n <= 0) return GCF_ERR_CUDA;
+    int n = 0, shape = 0;
+    if (fused_max_clusters(&n, &shape) != cudaSuccess || n <= 0) return GCF_ERR_CUDA;
     g_na_base[dev] = b;
     g_na_clusters[dev] = n;
+    g_na_shape[dev] = shape;
     *base = b;
     *clusters = n;
     return GCF_OK;
@@ -481,14 +581,19 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     NaMeta meta;
     std::memset(&meta, 0, sizeof(meta));
+    double* bsum = reinterpret_cast<double*>(base + kNaBsumOff);
     meta.desc.img = dev_img;
+    meta.desc.bsum = bsum;
     meta.desc.pitch = pitch;
     meta.desc.ntx = ntx;
+    meta.desc.nty = nty;
     meta.desc.offx = (width - ntx * FT + (ntx - 1) * ov) / 2;
     meta.desc.offy = (height - nty * FT + (nty - 1) * ov) / 2;
     meta.desc.stride = stride;
-    meta.desc.vec4 = ((meta.desc.offx % 4) == 0 && (stride % 4) == 0 && (pitch % 4) == 0 &&
-                      ((uintptr_t)dev_img % 16) == 0) ? 1 : 0;
+    meta.desc.vec = ((meta.desc.offx % 2) == 0 && (stride % 2) == 0 && (pitch % 2) == 0 &&
+                     ((uintptr_t)dev_img % 8) == 0) ? 2 : 1;
+    meta.desc.nbx = ntx + 1;
+    meta.bsum_ptr[0] = bsum;
     int nitems = nt < kNaMaxItems ? nt : kNaMaxItems;
     int chunk = (nt + nitems - 1) / nitems;
     nitems = 0;
@@ -504,10 +609,11 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
     if (cudaMemcpyAsync(dmeta, &meta, sizeof(meta), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return GCF_ERR_CUDA;
     int ncl = clusters < nitems ? clusters : nitems;
-    cudaError_t e = launch_fused(&dmeta->desc, dmeta->items, nitems, dmeta->first, dmeta->inv, 1,
+    cudaError_t e = launch_fused(&dmeta->desc, dmeta->bsum_ptr, (ntx + 1) * (nty + 1), dmeta->items,
+                                 nitems, dmeta->first, dmeta->inv, 1,
                                  reinterpret_cast<const float*>(base + kNaTaperOff),
                                  reinterpret_cast<const float2*>(base + kNaTwOff),
-                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, st);
+                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, g_na_shape[dev], st);
     if (e != cudaSuccess) return GCF_ERR_CUDA;
     // a copy from pageable memory has consumed `meta` when cudaMemcpyAsync returns
     return GCF_OK;

@@ -117,19 +117,21 @@ void launch_fourier_crop(const float2* in, int cx_in, int cy_in, float2* out, in
 // gcf_fused.cu: fused tile-spectrum kernel (tile 512).
 struct FusedImageDesc {          // layout must match FusedTab in gcf_fused.cu
     const float* img;
+    const double* bsum;
     int pitch;
-    int ntx;
+    int ntx, nty;
     int offx, offy, stride;
-    int vec4;
+    int vec;
+    int nbx;
 };
 int fused_tile_supported(int tile);
-size_t fused_smem_bytes();
-cudaError_t fused_max_clusters(int* n);
+cudaError_t fused_max_clusters(int* n, int* shape);
 // items: (image, first tile, end tile, item index); first[img]..first[img+1]
 // are the items of image img; inv[img] = 1 / tiles of img.
-cudaError_t launch_fused(const void* descs, const int4* items, int nitems, const int* first,
-                         const float* inv, int nimg, const float* taper, const float2* tw,
-                         float* partial, float* raw, int nclusters, cudaStream_t st);
+cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
+                         int nitems, const int* first, const float* inv, int nimg, const float* taper,
+                         const float2* tw, float* partial, float* raw, int nclusters, int shape,
+                         cudaStream_t st);
 
 // gcf_post.cu
 void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,

@@ -196,9 +196,10 @@ gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, in
 gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height, int pitch,
                                     float* dev_raw_out, void* cuda_stream);
 
-/* Device time (ms, CUDA events on the context stream) of the stages of the
- * last batched call: [0] upload, [1] rescale, [2] spectrum, [3] background
- * + lowpass + radial, [4] 1D search, [5] 2D search, [6] total. */
+/* Device time (ms, CUDA events on the context streams) of the stages of the
+ * last batched call: [0] upload of host inputs (it overlaps [2]), [1] 0
+ * (rescale runs inside [2]), [2] rescale + tile spectra, [3] background +
+ * lowpass + radial, [4] 1D search, [5] 2D search, [6] total. */
 gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7]);
 /* Number of kernels this library launched in the last batched call. */
 gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);
