@@ -81,8 +81,7 @@ struct gcf_ctx {
     // per-tile tables
     DBuf<float> taper;
     DBuf<int> rad_off, rad_pix;
-    DBuf<double> lp_h;
-    int lp_radius = 0;
+    DBuf<int> ring_off, ring_pix;
 
     // bands
     std::vector<BandHost*> bands;
@@ -92,11 +91,13 @@ struct gcf_ctx {
     // buffers
     DBuf<float> images, rescaled, tiles;
     DBuf<float2> cmp, rs_cmp, rs_crop;
-    DBuf<double> acc, hsum, lptmp, moments, moments2;
+    DBuf<double> acc, hsum, moments, moments2;
+    DBuf<float> lpfull;
+    DBuf<float2> lpcmp;
     DBuf<float> raw, ctf0, ctf, radial, band_spec, cc_res, full;
     DBuf<int> lowpassed, spec_off, mic_of;
     DBuf<SearchJob> jobs;
-    DBuf<double> sum_ss;
+    DBuf<double> sum_ss, ring_sums;
     DBuf<float4> cand;
     DBuf<float2> cval;
     DBuf<double2> part;
@@ -235,23 +236,31 @@ gcf_status build_tile_tables(gcf_ctx* ctx)
     CK(ctx->rad_pix.ensure(pix.size()));
     CK(cudaMemcpy(ctx->rad_off.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->rad_pix.p, pix.data(), pix.size() * sizeof(int), cudaMemcpyHostToDevice));
-    // Periodic kernel of the B-factor lowpass, B = 10
-    // (FindCTF/CFindCtfBase.cpp:203-206, FindCTF/GLowpass2D.cu:57-70).
-    double a = 10.0 / ((double)T * T + (double)T * T);
-    auto hval = [&](int t) {
-        double sacc = 0.0;
-        for (int k = -T / 2 + 1; k <= T / 2; ++k)
-            sacc += std::exp(-a * (double)k * k) * std::cos(2.0 * M_PI * (double)k * t / T);
-        return sacc / T;
-    };
-    double h0 = hval(0);
-    int R = 1;
-    while (R < T / 2 - 1 && std::fabs(hval(R + 1)) > 1e-17 * h0) ++R;
-    std::vector<double> h(2 * R + 1);
-    for (int t = -R; t <= R; ++t) h[t + R] = hval(t);
-    ctx->lp_radius = R;
-    CK(ctx->lp_h.ensure(h.size()));
-    CK(cudaMemcpy(ctx->lp_h.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    // Integer-radius rings of the half spectrum for the spectral-CC
+    // resolution (GSpectralCC2D, FindCTF/GSpectralCC2D.cu:27-64): a shell
+    // [lo, hi) with integer bounds is exactly the rings lo .. hi-1 of
+    // floor(sqrt(x^2 + |y - cy/2|^2)), evaluated in float as the reference does.
+    {
+        std::vector<std::vector<int>> rings(cx);
+        for (int y = 0; y < cy; ++y) {
+            float fy = fabsf(y - cy * 0.5f);
+            for (int x = 0; x < cx; ++x) {
+                float r = sqrtf((float)(x * x) + fy * fy);
+                int ri = (int)r;
+                if (ri < cx) rings[ri].push_back(y * cx + x);
+            }
+        }
+        std::vector<int> roff(cx + 1), rpix;
+        for (int ri = 0; ri < cx; ++ri) {
+            roff[ri] = (int)rpix.size();
+            rpix.insert(rpix.end(), rings[ri].begin(), rings[ri].end());
+        }
+        roff[cx] = (int)rpix.size();
+        CK(ctx->ring_off.ensure(roff.size()));
+        CK(ctx->ring_pix.ensure(rpix.size()));
+        CK(cudaMemcpy(ctx->ring_off.p, roff.data(), roff.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->ring_pix.p, rpix.data(), rpix.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // exp(-2 pi i t / T), t < T: twiddles of the fused tile FFT
     std::vector<float2> tw(T);
     for (int t = 0; t < T; ++t) {
@@ -366,6 +375,12 @@ gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
     if (kind == 0) {   // batched tile R2C: a = tile, b = batch
         int n[2] = {a, a};
         r = cufftPlanMany(&h, 2, n, nullptr, 1, a * a, nullptr, 1, (a / 2 + 1) * a, CUFFT_R2C, b);
+    } else if (kind == 3 || kind == 4) {   // batched full-spectrum R2C / C2R: a = tile, b = batch
+        int n[2] = {a, a};
+        if (kind == 3)
+            r = cufftPlanMany(&h, 2, n, nullptr, 1, a * a, nullptr, 1, (a / 2 + 1) * a, CUFFT_R2C, b);
+        else
+            r = cufftPlanMany(&h, 2, n, nullptr, 1, (a / 2 + 1) * a, nullptr, 1, a * a, CUFFT_C2R, b);
     } else if (kind == 1) {   // image R2C: a = height, b = width
         r = cufftPlan2d(&h, a, b, CUFFT_R2C);
     } else {   // image C2R: a = height, b = width
@@ -506,7 +521,6 @@ gcf_status spectra_alloc(gcf_ctx* ctx, int nm)
     CK(ctx->ctf0.ensure(cmp_n * nm));
     CK(ctx->ctf.ensure(cmp_n * nm));
     CK(ctx->hsum.ensure(cmp_n * nm));
-    CK(ctx->lptmp.ensure(cmp_n * nm));
     CK(ctx->moments.ensure(2 * (size_t)nm));
     CK(ctx->lowpassed.ensure(nm));
     CK(ctx->radial.ensure((size_t)cx * nm));
@@ -540,12 +554,26 @@ gcf_status spectra_post(gcf_ctx* ctx, int nm)
     CKL();
     launch_moments(ctx->ctf0.p, (int)cmp_n, nm, ctx->moments.p, ctx->st);
     CKL();
-    launch_lowpass(ctx->ctf0.p, T, nm, ctx->moments.p, ctx->lp_h.p, ctx->lp_radius, ctx->lptmp.p,
-                   ctx->ctf.p, ctx->lowpassed.p, ctx->st);
+    // CFindCtfBase::mLowpass (FindCTF/CFindCtfBase.cpp:191-219): full
+    // spectrum, R2C, B-factor 10 (normalised), C2R, half back.
+    CK(ctx->lpfull.ensure((size_t)nm * T * T));
+    CK(ctx->lpcmp.ensure((size_t)nm * cx * T));
+    launch_lp_full(ctx->ctf0.p, T, nm, ctx->lpfull.p, ctx->st);
+    CKL();
+    cufftHandle pf, pi;
+    CKS(get_plan(ctx, 3, T, nm, &pf));
+    CKS(get_plan(ctx, 4, T, nm, &pi));
+    if (cufftExecR2C(pf, ctx->lpfull.p, (cufftComplex*)ctx->lpcmp.p) != CUFFT_SUCCESS)
+        return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (lowpass) failed");
+    launch_lp_filter(ctx->lpcmp.p, T, nm, 10.0, ctx->st);
+    CKL();
+    if (cufftExecC2R(pi, (cufftComplex*)ctx->lpcmp.p, ctx->lpfull.p) != CUFFT_SUCCESS)
+        return fail(ctx, GCF_ERR_CUFFT, "cufftExecC2R (lowpass) failed");
+    launch_lp_extract(ctx->ctf0.p, ctx->lpfull.p, T, nm, ctx->moments.p, ctx->ctf.p, ctx->lowpassed.p, ctx->st);
     CKL();
     launch_radial(ctx->ctf.p, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p, ctx->st);
     CKL();
-    ctx->launches += 6;
+    ctx->launches += 7;
     return GCF_OK;
 }
 
@@ -686,13 +714,15 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         ctx->launches += 2;
     }
     // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)
-    launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->cc_res.p, ctx->st);
+    CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
+    launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p, ctx->ring_sums.p,
+                   ctx->cc_res.p, ctx->st);
     CKL();
     launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
     CKL();
     launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->st);
     CKL();
-    ctx->launches += 3;
+    ctx->launches += 4;
     CK(cudaEventRecord(ctx->ev[7], ctx->st));
     CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost,
                        ctx->st));
@@ -958,7 +988,8 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->taper.release();
     ctx->rad_off.release();
     ctx->rad_pix.release();
-    ctx->lp_h.release();
+    ctx->ring_off.release();
+    ctx->ring_pix.release();
     ctx->d_bands.release();
     ctx->images.release();
     ctx->rescaled.release();
@@ -968,7 +999,8 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->rs_crop.release();
     ctx->acc.release();
     ctx->hsum.release();
-    ctx->lptmp.release();
+    ctx->lpfull.release();
+    ctx->lpcmp.release();
     ctx->moments.release();
     ctx->moments2.release();
     ctx->raw.release();
@@ -983,6 +1015,7 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->mic_of.release();
     ctx->jobs.release();
     ctx->sum_ss.release();
+    ctx->ring_sums.release();
     ctx->cand.release();
     ctx->cval.release();
     ctx->part.release();

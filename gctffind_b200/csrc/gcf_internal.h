@@ -139,8 +139,11 @@ void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, d
 void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic, int log_spect,
                         float* ctf, cudaStream_t st);
 void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st);
-void launch_lowpass(const float* in, int tile, int nmic, const double* moments, const double* h,
-                    int radius, double* tmp, float* out, int* lowpassed, cudaStream_t st);
+// lowpass of CFindCtfBase::mLowpass around a batched R2C / C2R pair
+void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStream_t st);
+void launch_lp_filter(float2* cmp, int tile, int nmic, double bfactor, cudaStream_t st);
+void launch_lp_extract(const float* ctf0, const float* full, int tile, int nmic, const double* moments,
+                       float* out, int* lowpassed, cudaStream_t st);
 void launch_radial(const float* spect, int tile, int nmic, const int* off, const int* pix,
                    float* radial, cudaStream_t st);
 void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, const BandDev* bands,
@@ -149,8 +152,8 @@ void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, cons
 void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_of,
                           const gcf_result* res, const PixOptics* o, const double* moments,
                           float res_lo_freq_dummy, float* full, cudaStream_t st);
-void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, float* cc,
-                    cudaStream_t st);
+void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, const int* ring_off,
+                    const int* ring_pix, double* ring_sums, float* cc, cudaStream_t st);
 
 // gcf_search.cu (candidate kernel) and gcf_control.cu (state machine)
 void launch_eval2d(const EvalArgs& a, int cand_blocks, int max_band_n, cudaStream_t st);

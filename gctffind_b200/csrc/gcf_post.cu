@@ -145,56 +145,59 @@ __device__ __forceinline__ float full_val(const float* half, int tile, int y, in
     return half[(size_t)ys * cx - xd];
 }
 
-// Horizontal pass of the separable, periodic B-factor filter on the full
-// spectrum; output at the columns copied back by mLowpass
-// (FindCTF/CFindCtfBase.cpp:211-218).
-__global__ void k_lowpass_h(const float* __restrict__ in, int tile, const double* __restrict__ mom,
-                            const double* __restrict__ h, int radius, double* __restrict__ tmp,
-                            int* __restrict__ lowpassed)
+// CFindCtfBase::mLowpass (FindCTF/CFindCtfBase.cpp:191-219) around a batched
+// R2C / C2R pair: the full spectrum (DC at column tile/2), the B-factor
+// filter exp(-B (kx^2 + ky^2) / (2 tile^2)) of GLowpass2D::DoBFactor
+// (FindCTF/GLowpass2D.cu:9-23) with the 1/tile^2 of the normalised forward
+// transform, and the copy of columns tile/2 .. tile back into the half
+// spectrum (the last one from the periodic neighbour, column 0).
+__global__ void k_lp_full(const float* __restrict__ ctf0, int tile, float* __restrict__ full)
 {
-    int cx = tile / 2 + 1, hx = cx - 1;
     int m = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tile * tile) return;
+    int y = i / tile, X = i - y * tile;
+    int cx = tile / 2 + 1;
+    full[(size_t)m * tile * tile + i] = full_val(ctf0 + (size_t)m * cx * tile, tile, y, X);
+}
+
+__global__ void k_lp_filter(float2* __restrict__ cmp, int tile, double bfactor)
+{
+    int m = blockIdx.y;
+    int cx = tile / 2 + 1;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cx * tile) return;
+    int y = i / cx, x = i - y * cx;
+    int ky = (y > tile / 2) ? y - tile : y;
+    double scale = -bfactor / ((double)tile * tile + (double)tile * tile);
+    double g = exp(scale * ((double)x * x + (double)ky * ky)) / ((double)tile * tile);
+    float2 v = cmp[(size_t)m * cx * tile + i];
+    cmp[(size_t)m * cx * tile + i] = make_float2((float)(v.x * g), (float)(v.y * g));
+}
+
+// Variance gate of mRemoveBackground (FindCTF/CFindCtfBase.cpp:169-174):
+// micrographs whose background-removed spectrum has variance < 1 keep it
+// unfiltered.
+__global__ void k_lp_extract(const float* __restrict__ ctf0, const float* __restrict__ full, int tile,
+                             const double* __restrict__ mom, float* __restrict__ out,
+                             int* __restrict__ lowpassed)
+{
+    int m = blockIdx.y;
+    int cx = tile / 2 + 1, hx = cx - 1;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mean = mom[2 * m], var = mom[2 * m + 1] - mean * mean;
     bool run = !(var < 1.0);
     if (blockIdx.x == 0 && threadIdx.x == 0) lowpassed[m] = run ? 1 : 0;
-    if (!run || i >= cx * tile) return;
-    int y = i / cx, x = i - y * cx;
-    int X = x + hx;
-    if (X >= tile) X -= tile;
-    const float* half = in + (size_t)m * cx * tile;
-    double s = 0.0;
-    for (int t = -radius; t <= radius; ++t) {
-        int xx = X - t;
-        if (xx < 0) xx += tile;
-        else if (xx >= tile) xx -= tile;
-        s += h[t + radius] * (double)full_val(half, tile, y, xx);
-    }
-    tmp[(size_t)m * cx * tile + i] = s;
-}
-
-__global__ void k_lowpass_v(const float* __restrict__ in, int tile, const double* __restrict__ h,
-                            int radius, const double* __restrict__ tmp,
-                            const int* __restrict__ lowpassed, float* __restrict__ out)
-{
-    int cx = tile / 2 + 1;
-    int m = blockIdx.y;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cx * tile) return;
     size_t base = (size_t)m * cx * tile;
-    if (!lowpassed[m]) {
-        out[base + i] = in[base + i];
+    if (!run) {
+        out[base + i] = ctf0[base + i];
         return;
     }
     int y = i / cx, x = i - y * cx;
-    double s = 0.0;
-    for (int t = -radius; t <= radius; ++t) {
-        int yy = y - t;
-        if (yy < 0) yy += tile;
-        else if (yy >= tile) yy -= tile;
-        s += h[t + radius] * tmp[base + (size_t)yy * cx + x];
-    }
-    out[base + i] = (float)s;
+    int X = x + hx;
+    if (X >= tile) X -= tile;
+    out[base + i] = full[(size_t)m * tile * tile + (size_t)y * tile + X];
 }
 
 // GRadialAvg (FindCTF/GRadialAvg.cu:11-33) with the nearest-pixel sample
@@ -288,24 +291,17 @@ __global__ void k_full_spectrum(const float* __restrict__ ctf, int tile, const i
     full[(size_t)k * tile * tile + i] = v;
 }
 
-// GSpectralCC2D::mGCalc2D (FindCTF/GSpectralCC2D.cu:12-110): per shell b,
-// Pearson CC of the signed CTF and the spectrum in [lo, hi).
-__global__ void k_ctf_res(const float* __restrict__ ctf, int tile, const SearchJob* __restrict__ jobs,
-                          float* __restrict__ cc_out)
+// GSpectralCC2D::mGCalc2D (FindCTF/GSpectralCC2D.cu:12-110) in two steps:
+// sums over the integer-radius rings (one CTF evaluation per pixel), then
+// the Pearson CC of each width-10 shell from its rings.
+__global__ void k_ring_sums(const float* __restrict__ ctf, int tile, const SearchJob* __restrict__ jobs,
+                            const int* __restrict__ ring_off, const int* __restrict__ ring_pix,
+                            double* __restrict__ ring_sums)
 {
-    __shared__ double sh[6 * 32];
-    int b = blockIdx.x, j = blockIdx.y;
+    __shared__ double sh[5 * 32];
+    int ring = blockIdx.x, j = blockIdx.y;
     const SearchJob jb = jobs[j];
     int cx = tile / 2 + 1, cy = tile;
-    const int width = 10;
-    int lo = b - width / 2, hi = lo + width;
-    if (lo < 0) {
-        lo = 0;
-        hi = width;
-    } else if (hi > cx) {
-        lo = cx - width;
-        hi = cx;
-    }
     const PixOptics o = jb.o;
     float dmin = jb.df_mean * (1.0f - jb.ast_ratio) / o.px;
     float dmax = jb.df_mean * (1.0f + jb.ast_ratio) / o.px;
@@ -313,34 +309,53 @@ __global__ void k_ctf_res(const float* __restrict__ ctf, int tile, const SearchJ
     double add = (double)(o.amp_phase + jb.ext_phase * 0.01745329f);
     double az = (double)(jb.ast_angle * 0.01745329f);
     const float* sp = ctf + (size_t)jb.mic * cx * cy;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    for (int y = threadIdx.x; y < cy; y += blockDim.x) {
-        float fy = fabsf(y - cy * 0.5f);
-        if (fy >= hi) continue;
-        for (int x = 0; x < cx && x < hi; ++x) {
-            float r = sqrtf((float)(x * x) + fy * fy);
-            if (r < lo || r >= hi) continue;
-            double c = ctf_at(x, y, cx, cy, o, add, mn, sg, az);
-            double s = sp[(size_t)y * cx + x];
-            v[0] += c * s;
-            v[1] += c;
-            v[2] += s;
-            v[3] += c * c;
-            v[4] += s * s;
-            v[5] += 1.0;
+    double v[5] = {0, 0, 0, 0, 0};
+    for (int k = ring_off[ring] + threadIdx.x; k < ring_off[ring + 1]; k += blockDim.x) {
+        int pix = ring_pix[k];
+        int y = pix / cx, x = pix - y * cx;
+        double c = ctf_at(x, y, cx, cy, o, add, mn, sg, az);
+        double s = sp[pix];
+        v[0] += c * s;
+        v[1] += c;
+        v[2] += s;
+        v[3] += c * c;
+        v[4] += s * s;
+    }
+    block_sum<5>(v, sh);
+    if (threadIdx.x == 0) {
+        double* out = ring_sums + ((size_t)j * cx + ring) * 6;
+        for (int q = 0; q < 5; ++q) out[q] = v[q];
+        out[5] = (double)(ring_off[ring + 1] - ring_off[ring]);
+    }
+}
+
+__global__ void k_shell_cc(int tile, const double* __restrict__ ring_sums, float* __restrict__ cc_out)
+{
+    int j = blockIdx.x;
+    int cx = tile / 2 + 1;
+    const int width = 10;
+    for (int b = threadIdx.x; b < cx; b += blockDim.x) {
+        int lo = b - width / 2, hi = lo + width;
+        if (lo < 0) {
+            lo = 0;
+            hi = width;
+        } else if (hi > cx) {
+            lo = cx - width;
+            hi = cx;
         }
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int ring = lo; ring < hi; ++ring)
+            for (int q = 0; q < 6; ++q) v[q] += ring_sums[((size_t)j * cx + ring) * 6 + q];
+        float out = 0.0f;
+        if (v[5] > 0) {
+            double n = v[5];
+            double cs = v[0] / n, mc = v[1] / n, ms = v[2] / n, sc = v[3] / n, ss = v[4] / n;
+            sc -= mc * mc;
+            ss -= ms * ms;
+            if (sc > 0 && ss > 0) out = (float)((cs - mc * ms) / sqrt(sc * ss));
+        }
+        cc_out[(size_t)j * cx + b] = out;
     }
-    block_sum<6>(v, sh);
-    if (threadIdx.x != 0) return;
-    float out = 0.0f;
-    if (v[5] > 0) {
-        double n = v[5];
-        double mc = v[1] / n, ms = v[2] / n, cs = v[0] / n, sc = v[3] / n, ss = v[4] / n;
-        sc -= mc * mc;
-        ss -= ms * ms;
-        if (sc > 0 && ss > 0) out = (float)((cs - mc * ms) / sqrt(sc * ss));
-    }
-    cc_out[(size_t)j * cx + b] = out;
 }
 
 }  // namespace
@@ -378,13 +393,25 @@ void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStrea
     k_moments<<<nmic, 512, 0, st>>>(spect, n, out2);
 }
 
-void launch_lowpass(const float* in, int tile, int nmic, const double* moments, const double* h,
-                    int radius, double* tmp, float* out, int* lowpassed, cudaStream_t st)
+void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStream_t st)
+{
+    dim3 grid((tile * tile + 255) / 256, nmic);
+    k_lp_full<<<grid, 256, 0, st>>>(ctf0, tile, full);
+}
+
+void launch_lp_filter(float2* cmp, int tile, int nmic, double bfactor, cudaStream_t st)
 {
     int n = (tile / 2 + 1) * tile;
     dim3 grid((n + 255) / 256, nmic);
-    k_lowpass_h<<<grid, 256, 0, st>>>(in, tile, moments, h, radius, tmp, lowpassed);
-    k_lowpass_v<<<grid, 256, 0, st>>>(in, tile, h, radius, tmp, lowpassed, out);
+    k_lp_filter<<<grid, 256, 0, st>>>(cmp, tile, bfactor);
+}
+
+void launch_lp_extract(const float* ctf0, const float* full, int tile, int nmic, const double* moments,
+                       float* out, int* lowpassed, cudaStream_t st)
+{
+    int n = (tile / 2 + 1) * tile;
+    dim3 grid((n + 255) / 256, nmic);
+    k_lp_extract<<<grid, 256, 0, st>>>(ctf0, full, tile, moments, out, lowpassed);
 }
 
 void launch_radial(const float* spect, int tile, int nmic, const int* off, const int* pix,
@@ -412,12 +439,13 @@ void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_o
     k_full_spectrum<<<grid, 256, 0, st>>>(ctf, tile, mic_of, res, o, moments, full);
 }
 
-void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, float* cc,
-                    cudaStream_t st)
+void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, const int* ring_off,
+                    const int* ring_pix, double* ring_sums, float* cc, cudaStream_t st)
 {
     if (njobs <= 0) return;
     dim3 grid(tile / 2 + 1, njobs);
-    k_ctf_res<<<grid, 256, 0, st>>>(ctf, tile, jobs, cc);
+    k_ring_sums<<<grid, 128, 0, st>>>(ctf, tile, jobs, ring_off, ring_pix, ring_sums);
+    k_shell_cc<<<njobs, 128, 0, st>>>(tile, ring_sums, cc);
 }
 
 }  // namespace gcf
