@@ -8,5 +8,5 @@ mirrors the reference's CFindCtf2D / CCTFTheory interface over it, and
 from .api import (  # noqa: F401
     CCTFTheory, CFindCtf2D, Context, GcfError, Item, Optics, Result, GCF_SPECT_CUFFT,
     GCF_SPECT_FUSED, EXPORTS, LIB_PATH, CLI_PATH, load_library, make_optics, mrc_info, mrc_read,
-    mrc_read_tilts, mrc_write, rescale_dims, series_order,
+    mrc_read_tilts, mrc_write, rescale_dims, series_order, write_ctf_file,
 )

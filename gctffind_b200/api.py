@@ -32,6 +32,7 @@ EXPORTS = [
     "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
     "gcf_get_stage_times", "gcf_get_launch_count", "gcf_avg_spectrum_noalloc",
+    "gcf_write_ctf_file",
 ]
 
 
@@ -108,6 +109,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_get_stage_times.argtypes = [vp, C.POINTER(f)]
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
+    L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
     for name in EXPORTS:   # every declared entry point must resolve
         getattr(L, name)
     _lib = L
@@ -366,6 +368,17 @@ def mrc_read_tilts(path: str, n: int) -> np.ndarray:
     out = np.zeros(n, np.float32)
     _check(L.gcf_mrc_read_tilts(path.encode(), out.ctypes.data, n))
     return out
+
+
+def write_ctf_file(path: str, results, tilts=None, names=None, is_tomo: bool = False):
+    """CSaveCtfResults::SaveCTF (+ SaveImod for tilt series)."""
+    L = load_library()
+    n = len(results)
+    res = (Result * n)(*results)
+    t = np.ascontiguousarray(tilts if tilts is not None else np.zeros(n), np.float32)
+    nm = (C.c_char_p * n)(*[(x or "").encode() for x in (names or [""] * n)])
+    _check(L.gcf_write_ctf_file(path.encode(), res, t.ctypes.data, C.cast(nm, C.c_void_p), n,
+                                1 if is_tomo else 0))
 
 
 def mrc_write(path: str, data: np.ndarray, pixel_size: float = 1.0):

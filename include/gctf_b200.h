@@ -177,6 +177,16 @@ gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, in
                          float pixel_size);
 
 /* ---------------------------------------------------------------------- */
+/* Result files (CSaveCtfResults::SaveCTF / SaveImod,                       */
+/* CSaveCtfResults.cpp:34-117)                                              */
+/* ---------------------------------------------------------------------- */
+/* Writes the CTF text file (header + one row per image, 0-based index)
+ * and, when is_tomo, "<path without extension>_Imod.txt" with defocus in
+ * nm.  tilts and names may be NULL (0 and "" then). */
+gcf_status gcf_write_ctf_file(const char* path, const gcf_result* results, const float* tilts,
+                              const char* const* names, int n, int is_tomo);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free spectrum.  No counterpart in the reference.              */
 /* ---------------------------------------------------------------------- */
 /* Averaged amplitude spectrum (512 x 512 tiles, the fused tile kernel) of
