@@ -123,6 +123,7 @@ struct gcf_ctx {
     bool have_spectrum = false;
     int img_w = 0, img_h = 0;
     float phase_deg = 0.0f, phase_range = 0.0f;
+    float held_phase = 0.0f;   // CFindDefocus2D::m_fExtPhase between Do2D / Refine calls
     int cur_lowpassed = 0;
 };
 
@@ -599,6 +600,7 @@ struct JobSpec {
     float px_n;
     float phase_deg, phase_range;     // Do2D: CFindCtfBase::m_fExtPhase / m_fPhaseRange
     float rin[8];                     // Refine: {df, df_range, ast, ast_range, ang, ang_range, ph, ph_range}
+    float held_phase;                 // extra phase the search object holds on entry (0 after Setup1)
 };
 
 // CFindDefocus2D::Setup3 + Refine (FindCTF/CFindDefocus2D.cpp:98-151) on the host.
@@ -608,7 +610,7 @@ void refine_init(SearchJob& J, const float* rin)
     J.ast_ratio = rin[2];
     J.ast_angle = rin[4];
     J.phase_range[0] = rin[6];
-    J.ext_phase = rin[6];
+    J.ext_phase = J.held_phase;   // replaced by phase_range[0] after the astigmatism grid
     float h = 0.5f * rin[1];
     J.df_range[0] = fmaxf(J.df_mean - h, 3000.0f);
     J.df_range[1] = J.df_mean + h;
@@ -646,6 +648,7 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         J.o = make_optics(s.optics, s.px_n);
         J.phase_range_in = fmaxf(s.phase_range, 0.0f);
         J.ext_phase_in = s.phase_deg;
+        J.held_phase = s.held_phase;
         J.step = STEP_CC0;
         if (s.mode == 1) {
             refine_init(J, s.rin);
@@ -1104,6 +1107,7 @@ gcf_status gcf_setup(gcf_ctx* ctx, const gcf_optics* optics, int width, int heig
     ctx->have_spectrum = false;
     ctx->phase_deg = 0.0f;
     ctx->phase_range = 0.0f;
+    ctx->held_phase = 0.0f;   // Setup1 creates a new CFindDefocus2D
     return GCF_OK;
 }
 
@@ -1154,9 +1158,11 @@ gcf_status gcf_do2d(gcf_ctx* ctx, gcf_result* out)
     s.px_n = ctx->optics.pixel_size;
     s.phase_deg = ctx->phase_deg;
     s.phase_range = ctx->phase_range;
+    s.held_phase = ctx->held_phase;
     std::vector<gcf_result> r;
     CKS(run_search(ctx, {s}, r));
     *out = r[0];
+    ctx->held_phase = r[0].ext_phase;
     return GCF_OK;
 }
 
@@ -1174,9 +1180,11 @@ gcf_status gcf_refine(gcf_ctx* ctx, const float df[2], const float ast[2], const
     s.px_n = ctx->optics.pixel_size;
     float rin[8] = {df[0], df[1], ast[0], ast[1], ang[0], ang[1], ph[0], ph[1]};
     std::memcpy(s.rin, rin, sizeof(rin));
+    s.held_phase = ctx->held_phase;
     std::vector<gcf_result> r;
     CKS(run_search(ctx, {s}, r));
     *out = r[0];
+    ctx->held_phase = r[0].ext_phase;
     return GCF_OK;
 }
 
@@ -1320,7 +1328,11 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
             int new_ref = cur_ref;
             if (res[cur_ref].score < res[idx].score) new_ref = idx;
             if (res[idx].score <= 0) {
-                st = run_search(ctx, {full_job(idx)}, r);
+                // same CFindCtf2D object as the refine: its search starts at
+                // the phase the refine ended with
+                JobSpec fj = full_job(idx);
+                fj.held_phase = res[idx].ext_phase;
+                st = run_search(ctx, {fj}, r);
                 if (st != GCF_OK) goto done;
                 res[idx] = r[0];
                 new_ref = idx;

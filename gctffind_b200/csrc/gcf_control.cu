@@ -520,7 +520,7 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
         sJ.ast_angle = 0.0f;
         sJ.phase_range[0] = b2.ph;
         sJ.phase_range[1] = prange;
-        sJ.ext_phase = b2.ph;
+        sJ.ext_phase = sJ.held_phase;   // replaced by phase_range[0] after the astigmatism grid
         sJ.df_range[0] = mu * 0.9f;
         sJ.df_range[1] = mu * 1.1f;
         sJ.ast_range[0] = 0.0f;

@@ -57,6 +57,14 @@ struct SearchJob {
     float phase_range_in;   // CFindCtfBase::m_fPhaseRange (Do2D)
     float ext_phase_in;     // CFindCtfBase::m_fExtPhase   (Do2D)
     float res_lo, res_hi;   // 1D band, Fourier pixels [lo, hi)
+    // CFindDefocus2D::m_fExtPhase as the search object holds it on entry:
+    // Setup3 does not set it, and mIterate evaluates its first CC and the
+    // whole astigmatism grid at this phase before replacing it with
+    // m_afPhaseRange[0] (FindCTF/CFindDefocus2D.cpp:98-108,153-165).  It is 0
+    // for an object that Setup1 has just created, else the phase the
+    // previous search on the same object ended with.
+    float held_phase;
+    int pad2;
     // CFindDefocus2D state
     float df_mean, ast_ratio, ast_angle, ext_phase, cc_max, old_cc;
     float phase_range[2], df_range[2], ast_range[2], ang_range[2];

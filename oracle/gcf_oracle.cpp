@@ -1050,7 +1050,7 @@ extern "C" int orc_search(const double* ctf, int tile, float px_n, const orc_par
         s.ast_ratio = 0.0f;
         s.ast_angle = 0.0f;
         s.phase_range[0] = ph1;
-        s.ext_phase = ph1;
+        s.ext_phase = p->held_phase;   // mIterate replaces it by phase_range[0] after mFindAstig
         s.phase_range[1] = fmaxf(p->ext_phase_range, 0.0f);
         s.df_range[0] = s.df_mean * 0.9f;
         s.df_range[1] = s.df_mean * 1.1f;
@@ -1064,7 +1064,7 @@ extern "C" int orc_search(const double* ctf, int tile, float px_n, const orc_par
         s.ast_ratio = refine_in[2];
         s.ast_angle = refine_in[4];
         s.phase_range[0] = refine_in[6];
-        s.ext_phase = refine_in[6];
+        s.ext_phase = p->held_phase;
         float h = 0.5f * refine_in[1];
         s.df_range[0] = fmaxf(s.df_mean - h, 3000.0f);
         s.df_range[1] = s.df_mean + h;
@@ -1161,6 +1161,8 @@ extern "C" int orc_series(const float* const* imgs, int n, int w, int h, const o
         orc_rescale(imgs[idx], w, h, p->pixel_size, scaled.data(), 0);
         orc_result* r = &res[idx];
         bool full = (k == 0);
+        orc_params pk = *p;    // CFindSeriesCtfs::mSetupFindCtf: Setup1 per package
+        pk.held_phase = 0.0f;
         if (!full) {
             const orc_result* rp = &res[ref];
             float rin[8] = {0};
@@ -1178,14 +1180,18 @@ extern "C" int orc_series(const float* const* imgs, int n, int w, int h, const o
                 rin[5] = 30.0f;
                 if (p->ext_phase_range > 0) rin[7] = 40.0f;
             }
-            if (orc_find_ctf_image(scaled.data(), nw, nh, nw, pxn, p, 1, rin, r, nullptr, nullptr,
+            if (orc_find_ctf_image(scaled.data(), nw, nh, nw, pxn, &pk, 1, rin, r, nullptr, nullptr,
                                    nullptr))
                 return -1;
             if (res[ref].score < r->score) ref = idx;
             if (r->score <= 0) full = true;
         }
         if (full) {
-            if (orc_find_ctf_image(scaled.data(), nw, nh, nw, pxn, p, 0, nullptr, r, nullptr,
+            // Setup1 made a new search object for this package; a fallback
+            // after a refine reuses it and starts at the refine's phase
+            orc_params pf = pk;
+            if (k > 0) pf.held_phase = r->ext_phase;
+            if (orc_find_ctf_image(scaled.data(), nw, nh, nw, pxn, &pf, 0, nullptr, r, nullptr,
                                    nullptr, nullptr))
                 return -1;
             ref = idx;

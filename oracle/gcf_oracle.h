@@ -45,6 +45,10 @@ typedef struct {
     float ext_phase_range; /* -ExtPhase v1 (search range, deg; <=0 = none) */
     int   tile_size;       /* -TileSize    */
     int   log_spect;       /* -LogSpect    */
+    float held_phase;      /* CFindDefocus2D::m_fExtPhase on entry to DoIt/Refine (deg):
+                              Setup3 leaves it alone, mIterate evaluates its first CC
+                              and the astigmatism grid there; 0 for a search object
+                              Setup1 has just created */
 } orc_params;
 
 int  orc_num_threads(int n);           /* set OpenMP threads (n<=0: keep); returns current */

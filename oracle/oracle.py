@@ -29,13 +29,16 @@ class OrcResult(C.Structure):
 class OrcParams(C.Structure):
     _fields_ = [("kv", C.c_float), ("cs_mm", C.c_float), ("amp_contrast", C.c_float),
                 ("pixel_size", C.c_float), ("ext_phase_deg", C.c_float),
-                ("ext_phase_range", C.c_float), ("tile_size", C.c_int), ("log_spect", C.c_int)]
+                ("ext_phase_range", C.c_float), ("tile_size", C.c_int), ("log_spect", C.c_int),
+                ("held_phase", C.c_float)]
 
 
 def params(kv=300.0, cs_mm=2.7, amp_contrast=0.07, pixel_size=1.0, ext_phase_deg=0.0,
-           ext_phase_range=0.0, tile_size=512, log_spect=0) -> OrcParams:
+           ext_phase_range=0.0, tile_size=512, log_spect=0, held_phase=0.0) -> OrcParams:
+    """held_phase: the extra phase (deg) the reference's search object holds
+    when Do2D / Refine starts (0 for a freshly set-up object)."""
     return OrcParams(kv, cs_mm, amp_contrast, pixel_size, ext_phase_deg, ext_phase_range,
-                     tile_size, log_spect)
+                     tile_size, log_spect, held_phase)
 
 
 def build(force: bool = False) -> str:
