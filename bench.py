@@ -39,6 +39,10 @@ N_TILTS = 41
 SIZE = 4096
 PX = 1.35
 METRIC = "4096^2 micrographs/s (tilt series, plain FP32 search)"
+# DRAM bytes (read + write) of one micrograph's share of k_fused_spectrum,
+# from ncu dram__bytes_read.sum + dram__bytes_write.sum on a 3-micrograph
+# launch of the same kernel divided by 3 (profiles/k_fused_spectrum_3x4096.md)
+TILE_KERNEL_TRAFFIC_PER_MICROGRAPH = (338_597_376 + 3_934_208) // 3
 
 
 def parse():
@@ -310,6 +314,7 @@ def main():
     dev_ms, stage = 0.0, {}
     launches = 0
     results = None
+    torch.cuda.nvtx.range_push("device_steps")   # lets ncu --nvtx-include select the timed launches
     for _ in range(args.steps):
         results = ctx.run_series(imgs, op, order, is_tomo=True)
         st = ctx.stage_times()
@@ -318,6 +323,7 @@ def main():
             stage[k] = stage.get(k, 0.0) + v
         launches += ctx.launch_count()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     clocks = clk.stop()
     barrier(world)
     t_step = max_over_ranks(dev_ms / args.steps, world)
@@ -329,25 +335,45 @@ def main():
         ctx.run_series(host, op, order, is_tomo=True)
     barrier(world)
     e2e_ms = 0.0
+    torch.cuda.nvtx.range_push("e2e_steps")
     for _ in range(args.steps):
         ctx.run_series(host, op, order, is_tomo=True)
         e2e_ms += ctx.stage_times()["total"]
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     t_e2e = max_over_ranks(e2e_ms / args.steps, world)
     e2e = world * args.n_tilts / (t_e2e / 1000.0)
     h2d = sum(int(im.numel()) * 4 for im in imgs)
     d2h = args.n_tilts * 40
 
-    # ---- roofline of the spectrum stage (HBM-bound: 4 W H bytes per micrograph) ----
+    # ---- roofline of the dominant kernel: the fused tile-spectrum kernel,
+    # one launch per step over all micrographs of the series ----
     pk = peaks()
-    spec_ms = stage.get("spectrum", 0.0) / args.steps
-    algo_bytes = args.n_tilts * 4 * args.size * args.size
-    achieved = algo_bytes / (spec_ms / 1000.0) / 1e9 if spec_ms > 0 else 0.0
-    roof = {"kernel": "tile spectrum stage (all tiles of the series, one step)",
+    kern_ms = stage.get("tile_kernel", 0.0) / args.steps
+    T = 512
+    ov = T // 2
+    nt1 = ((args.size - ov) // (T - ov)) ** 2            # tiles per micrograph
+    nch = -(-nt1 // 64)                                   # work items per micrograph
+    img_bytes = args.n_tilts * 4 * args.size * args.size  # every pixel read once
+    part_bytes = args.n_tilts * nch * (T // 2 + 1) * T * 4  # per-item partial spectra written
+    algo_bytes = img_bytes + part_bytes
+    # real 2D FFT of a T x T tile: 2.5 T^2 log2(T^2) flops, plus mean removal,
+    # taper, |F| and accumulation (~6 flops per pixel)
+    tile_flops = 2.5 * T * T * 2 * 9 + 6 * T * T
+    algo_flops = args.n_tilts * nt1 * tile_flops
+    sec = kern_ms / 1000.0
+    achieved = algo_bytes / sec / 1e9 if sec > 0 else 0.0
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # nominal FP32 FMA rate at max clock
+    roof = {"kernel": "k_fused_spectrum (one launch: all tiles of the series)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": pk.get("hbm_gbs"),
             "unit": "GB/s", "frac": round(achieved / pk.get("hbm_gbs", 6650.0), 4),
-            "traffic": None, "peak_source": "fallback" if pk.get("_fallback") else "measured",
-            "algorithmic_bytes_per_step": algo_bytes}
+            "traffic": TILE_KERNEL_TRAFFIC_PER_MICROGRAPH * args.n_tilts if TILE_KERNEL_TRAFFIC_PER_MICROGRAPH else None,
+            "peak_source": "fallback" if pk.get("_fallback") else "measured",
+            "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(kern_ms, 3),
+            "compute": {"flops_per_launch": algo_flops,
+                        "achieved_tflops": round(algo_flops / sec / 1e12, 2) if sec > 0 else 0.0,
+                        "fp32_peak_tflops": round(fp32_peak, 1), "peak_source": "nominal FP32 FMA",
+                        "frac": round(algo_flops / sec / 1e12 / fp32_peak, 4) if sec > 0 else 0.0}}
 
     line = {"metric": METRIC, "value": round(value, 2), "unit": "micrographs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 3),

@@ -6,7 +6,7 @@ mirrors the reference's CFindCtf2D / CCTFTheory interface over it, and
 ``bin/GCtfFind`` is the drop-in command line.
 """
 from .api import (  # noqa: F401
-    CCTFTheory, CFindCtf2D, Context, GcfError, Item, Optics, Result, GCF_SPECT_CUFFT,
+    CCTFTheory, CFindCtf2D, Context, CtfParam, GcfError, Item, Optics, Result, GCF_SPECT_CUFFT,
     GCF_SPECT_FUSED, EXPORTS, LIB_PATH, CLI_PATH, load_library, make_optics, mrc_info, mrc_read,
     mrc_read_tilts, mrc_write, rescale_dims, series_order, write_ctf_file,
 )

@@ -33,6 +33,10 @@ EXPORTS = [
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
     "gcf_get_stage_times", "gcf_get_launch_count", "gcf_avg_spectrum_noalloc",
     "gcf_write_ctf_file",
+    "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
+    "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
+    "gcf_ctf_phase_shift", "gcf_ctf_defocus", "gcf_ctf_frequency", "gcf_ctf_nth_zero",
+    "gcf_ctf_equal",
 ]
 
 
@@ -58,6 +62,14 @@ class Result(C.Structure):
     def __repr__(self):
         return "Result(%s)" % ", ".join("%s=%.4f" % (k, v) if isinstance(v, float) else
                                         "%s=%s" % (k, v) for k, v in self.as_dict().items())
+
+
+class CtfParam(C.Structure):
+    """CCTFParam (FindCTF/CFindCTFInc.h:8-29): lengths in pixels, angles in radian."""
+    _fields_ = [("wavelength", C.c_float), ("cs", C.c_float), ("amp_contrast", C.c_float),
+                ("amp_phase", C.c_float), ("ext_phase", C.c_float), ("df_max", C.c_float),
+                ("df_min", C.c_float), ("azimuth", C.c_float), ("ast_tol", C.c_float),
+                ("pixel_size", C.c_float)]
 
 
 class Item(C.Structure):
@@ -110,6 +122,18 @@ def load_library(path: str = LIB_PATH):
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
+    P = C.POINTER(CtfParam)
+    L.gcf_ctf_setup.argtypes = [P, f, f, f, f, f, f]
+    L.gcf_ctf_set_ext_phase.argtypes = [P, f, i]
+    L.gcf_ctf_get_ext_phase.argtypes = [P, i, C.POINTER(f)]
+    L.gcf_ctf_set_defocus.argtypes = [P, f, f, f]
+    L.gcf_ctf_set_defocus_px.argtypes = [P, f, f, f]
+    L.gcf_ctf_change_pixel_size.argtypes = [P, f]
+    for name in ("gcf_ctf_evaluate", "gcf_ctf_phase_shift", "gcf_ctf_frequency"):
+        getattr(L, name).argtypes = [P, f, f, C.POINTER(f)]
+    L.gcf_ctf_defocus.argtypes = [P, f, C.POINTER(f)]
+    L.gcf_ctf_nth_zero.argtypes = [P, i, f, C.POINTER(f)]
+    L.gcf_ctf_equal.argtypes = [P, P, f, C.POINTER(i)]
     for name in EXPORTS:   # every declared entry point must resolve
         getattr(L, name)
     _lib = L
@@ -275,7 +299,7 @@ class Context:
     def stage_times(self):
         t = (C.c_float * 7)()
         _check(self.L.gcf_get_stage_times(self._h, t), self._h)
-        keys = ["upload", "rescale", "spectrum", "post", "search1d", "search2d", "total"]
+        keys = ["upload", "tile_kernel", "spectrum", "post", "search1d", "search2d", "total"]
         return dict(zip(keys, list(t)))
 
     def launch_count(self) -> int:
@@ -288,15 +312,89 @@ class Context:
 # Reference-shaped classes
 # ---------------------------------------------------------------------------
 class CCTFTheory:
-    """Optics holder with CCTFTheory::Setup's signature (FindCTF/CCTFTheory.cpp:69-86)."""
+    """CCTFTheory (FindCTF/CCTFTheory.cpp:9-301) over the library's host CTF
+    math: same method names, units and float/double arithmetic."""
 
     def __init__(self):
+        self.param = CtfParam()
+        self.param.pixel_size = 1.0
         self.optics = make_optics()
 
+    def _f(self, fn, *args):
+        out = C.c_float()
+        _check(fn(C.byref(self.param), *args, C.byref(out)))
+        return out.value
+
     def Setup(self, fKv, fCs, fAmpContrast, fPixelSize, fAstTol=100.0, fExtPhase=0.0):
-        # fExtPhase in radian as in the reference; stored in degrees for the ABI.
+        """fExtPhase in radian, as in the reference."""
+        L = load_library()
+        _check(L.gcf_ctf_setup(C.byref(self.param), fKv, fCs, fAmpContrast, fPixelSize, fAstTol,
+                               fExtPhase))
         self.optics = make_optics(fKv, fCs, fAmpContrast, fPixelSize,
-                                  float(np.degrees(fExtPhase)), 0.0)
+                                  float(np.float32(fExtPhase) / np.float32(0.017453)), 0.0)
+
+    def SetExtPhase(self, fExtPhase, bDegree):
+        _check(load_library().gcf_ctf_set_ext_phase(C.byref(self.param), fExtPhase, int(bDegree)))
+
+    def GetExtPhase(self, bDegree):
+        L = load_library()
+        out = C.c_float()
+        _check(L.gcf_ctf_get_ext_phase(C.byref(self.param), int(bDegree), C.byref(out)))
+        return out.value
+
+    def SetPixelSize(self, fPixSize):
+        self.param.pixel_size = fPixSize
+
+    def ChangePixelSize(self, fNewPixSize):
+        _check(load_library().gcf_ctf_change_pixel_size(C.byref(self.param), fNewPixSize))
+
+    def SetDefocus(self, fDefocusMin, fDefocusMax, fAstAzimuth):
+        _check(load_library().gcf_ctf_set_defocus(C.byref(self.param), fDefocusMin, fDefocusMax,
+                                                  fAstAzimuth))
+
+    def SetDefocusInPixel(self, fDefocusMin, fDefocusMax, fAstAzimuth):
+        _check(load_library().gcf_ctf_set_defocus_px(C.byref(self.param), fDefocusMin, fDefocusMax,
+                                                     fAstAzimuth))
+
+    def GetParam(self, bCopy=False):
+        if not bCopy:
+            return self.param
+        c = CtfParam()
+        C.pointer(c)[0] = self.param
+        return c
+
+    def SetParam(self, param: CtfParam):
+        C.pointer(self.param)[0] = param
+
+    def Evaluate(self, fFreq, fAzimuth):
+        return self._f(load_library().gcf_ctf_evaluate, fFreq, fAzimuth)
+
+    def CalcPhaseShift(self, fFreq, fAzimuth):
+        return self._f(load_library().gcf_ctf_phase_shift, fFreq, fAzimuth)
+
+    def CalcDefocus(self, fAzimuth):
+        return self._f(load_library().gcf_ctf_defocus, fAzimuth)
+
+    def CalcFrequency(self, fPhaseShift, fAzimuth):
+        return self._f(load_library().gcf_ctf_frequency, fPhaseShift, fAzimuth)
+
+    def CalcNthZero(self, iNthZero, fAzimuth):
+        return self._f(load_library().gcf_ctf_nth_zero, int(iNthZero), fAzimuth)
+
+    def EqualTo(self, other: "CCTFTheory", fDfTol):
+        out = C.c_int()
+        _check(load_library().gcf_ctf_equal(C.byref(self.param), C.byref(other.param), fDfTol,
+                                            C.byref(out)))
+        return bool(out.value)
+
+    def GetPixelSize(self):
+        return self.param.pixel_size
+
+    def GetCopy(self):
+        c = CCTFTheory()
+        c.SetParam(self.param)
+        c.optics = Optics(*[getattr(self.optics, k) for k, _ in Optics._fields_])
+        return c
 
 
 class CFindCtf2D:

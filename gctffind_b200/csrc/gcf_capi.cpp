@@ -77,6 +77,8 @@ struct gcf_ctx {
     long long launches = 0;
     float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t ev[8] = {};
+    std::vector<cudaEvent_t> kev;   // begin/end pairs around fused tile-kernel launches
+    int kev_used = 0;
 
     // per-tile tables
     DBuf<float> taper;
@@ -506,9 +508,17 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     CK(cudaMemcpyAsync(ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->f_inv.p, inv.data(), nm * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
     int ncl = std::min(ctx->fused_clusters, ni);
+    if (ctx->kev_used > 256) ctx->kev_used = 0;   // calls that never read their stage times
+    while ((int)ctx->kev.size() < ctx->kev_used + 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ctx->kev.push_back(e);
+    }
+    cudaEvent_t e0 = ctx->kev[ctx->kev_used], e1 = ctx->kev[ctx->kev_used + 1];
+    ctx->kev_used += 2;
     CK(launch_fused(ctx->f_desc.p, ctx->f_bsum_ptr.p, max_blocks, ctx->f_items.p, ni, ctx->f_first.p,
                     ctx->f_inv.p, nm, ctx->taper.p, ctx->tw512.p, ctx->f_partial.p, raw_out, ncl,
-                    ctx->fused_shape, ctx->st));
+                    ctx->fused_shape, ctx->st, e0, e1));
     ctx->launches += 3;
     return GCF_OK;
 }
@@ -877,6 +887,9 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
 void accumulate_stage_times(gcf_ctx* ctx)
 {
     float t;
+    for (int i = 0; i + 1 < ctx->kev_used; i += 2)
+        if (cudaEventElapsedTime(&t, ctx->kev[i], ctx->kev[i + 1]) == cudaSuccess) ctx->stage_ms[1] += t;
+    ctx->kev_used = 0;
     if (cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]) == cudaSuccess) ctx->stage_ms[0] += t;
     if (cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev[3]) == cudaSuccess) ctx->stage_ms[2] += t;
     if (cudaEventElapsedTime(&t, ctx->ev[3], ctx->ev[4]) == cudaSuccess) ctx->stage_ms[3] += t;
@@ -1035,6 +1048,7 @@ void gcf_destroy(gcf_ctx* ctx)
     for (auto& ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
+    for (auto& ev : ctx->kev) cudaEventDestroy(ev);
     if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -1244,6 +1258,7 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
         if (!images[i]) return GCF_ERR_INVALID_ARG;
     CKS(set_device(ctx));
     for (float& t : ctx->stage_ms) t = 0.0f;
+    ctx->kev_used = 0;
     ctx->launches = 0;
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));
@@ -1382,6 +1397,7 @@ gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_devi
     }
     CKS(set_device(ctx));
     for (float& t : ctx->stage_ms) t = 0.0f;
+    ctx->kev_used = 0;
     ctx->launches = 0;
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));

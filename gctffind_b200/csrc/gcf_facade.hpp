@@ -28,13 +28,16 @@ inline void gcf_check(gcf_status s, gcf_ctx* ctx = nullptr)
     throw CGcfError(s, msg);
 }
 
-// CCTFTheory::Setup(kV, Cs, amplitude contrast, pixel size, astigmatism
-// tolerance, extra phase in radian).
+// CCTFTheory (FindCTF/CCTFTheory.cpp:9-301): the CTF parameters in pixels
+// and radian (gcf_ctf_param has CCTFParam's fields in order) plus the
+// optics the search takes.
 class CCTFTheory {
 public:
+    CCTFTheory() { m_param.pixel_size = 1.0f; }
+    // fExtPhase in radian, as in the reference.
     void Setup(float fKv, float fCs, float fAmpContrast, float fPixelSize, float fAstTol, float fExtPhase)
     {
-        (void)fAstTol;
+        gcf_check(gcf_ctf_setup(&m_param, fKv, fCs, fAmpContrast, fPixelSize, fAstTol, fExtPhase));
         m_optics.kv = fKv;
         m_optics.cs_mm = fCs;
         m_optics.amp_contrast = fAmpContrast;
@@ -42,8 +45,45 @@ public:
         m_optics.ext_phase_deg = fExtPhase / 0.017453f;
         m_optics.ext_phase_range = 0.0f;
     }
-    float GetPixelSize() const { return m_optics.pixel_size; }
+    void SetExtPhase(float fExtPhase, bool bDegree) { gcf_check(gcf_ctf_set_ext_phase(&m_param, fExtPhase, bDegree)); }
+    float GetExtPhase(bool bDegree) const { return get(gcf_ctf_get_ext_phase, bDegree ? 1 : 0); }
+    void SetPixelSize(float fPixSize) { m_param.pixel_size = fPixSize; }
+    void ChangePixelSize(float fNewPixSize) { gcf_check(gcf_ctf_change_pixel_size(&m_param, fNewPixSize)); }
+    void SetDefocus(float fDfMin, float fDfMax, float fAstAzimuth)
+    {
+        gcf_check(gcf_ctf_set_defocus(&m_param, fDfMin, fDfMax, fAstAzimuth));
+    }
+    void SetDefocusInPixel(float fDfMin, float fDfMax, float fAstAzimuth)
+    {
+        gcf_check(gcf_ctf_set_defocus_px(&m_param, fDfMin, fDfMax, fAstAzimuth));
+    }
+    void SetParam(const gcf_ctf_param* p) { m_param = *p; }
+    gcf_ctf_param* GetParam() { return &m_param; }
+    float Evaluate(float fFreq, float fAzimuth) const { return get(gcf_ctf_evaluate, fFreq, fAzimuth); }
+    float CalcPhaseShift(float fFreq, float fAzimuth) const { return get(gcf_ctf_phase_shift, fFreq, fAzimuth); }
+    float CalcDefocus(float fAzimuth) const { return get(gcf_ctf_defocus, fAzimuth); }
+    float CalcFrequency(float fPhase, float fAzimuth) const { return get(gcf_ctf_frequency, fPhase, fAzimuth); }
+    float CalcNthZero(int iNthZero, float fAzimuth) const { return get(gcf_ctf_nth_zero, iNthZero, fAzimuth); }
+    bool EqualTo(const CCTFTheory* other, float fDfTol) const
+    {
+        int eq = 0;
+        gcf_check(gcf_ctf_equal(&m_param, &other->m_param, fDfTol, &eq));
+        return eq != 0;
+    }
+    float GetPixelSize() const { return m_param.pixel_size; }
+    CCTFTheory* GetCopy() const { return new CCTFTheory(*this); }
+
+    gcf_ctf_param m_param{};
     gcf_optics m_optics{300.0f, 2.7f, 0.07f, 1.0f, 0.0f, 0.0f};
+
+private:
+    template <class F, class... A>
+    float get(F fn, A... a) const
+    {
+        float v = 0.0f;
+        gcf_check(fn(&m_param, a..., &v));
+        return v;
+    }
 };
 
 // CFindCtf2D: Setup1 -> Setup2 -> GenHalfSpectrum -> SetPhase -> Do2D or

@@ -446,12 +446,13 @@ cudaError_t fused_max_clusters(int* n, int* shape)
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
                          int nitems, const int* first, const float* inv, int nimg, const float* taper,
                          const float2* tw, float* partial, float* raw, int nclusters, int shape,
-                         cudaStream_t st)
+                         cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
 {
     if (nclusters < 1) nclusters = 1;
     k_block_sums<<<dim3(max_blocks, nimg), 256, 0, st>>>(reinterpret_cast<const FusedTab*>(descs), bsum_out);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (ev0 && (e = cudaEventRecord(ev0, st)) != cudaSuccess) return e;
     cudaLaunchAttribute attr[1];
     if (shape == 16) {
         if ((e = prepare_kernel<Shape16>()) != cudaSuccess) return e;
@@ -465,6 +466,7 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
                                nitems, taper, tw, partial);
     }
     if (e != cudaSuccess) return e;
+    if (ev1 && (e = cudaEventRecord(ev1, st)) != cudaSuccess) return e;
     dim3 g((FCX * FT + 255) / 256, nimg);
     k_item_reduce<<<g, 256, 0, st>>>(partial, first, inv, raw);
     return cudaGetLastError();
@@ -613,7 +615,8 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
                                  nitems, dmeta->first, dmeta->inv, 1,
                                  reinterpret_cast<const float*>(base + kNaTaperOff),
                                  reinterpret_cast<const float2*>(base + kNaTwOff),
-                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, g_na_shape[dev], st);
+                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, g_na_shape[dev], st,
+                                 nullptr, nullptr);
     if (e != cudaSuccess) return GCF_ERR_CUDA;
     // a copy from pageable memory has consumed `meta` when cudaMemcpyAsync returns
     return GCF_OK;

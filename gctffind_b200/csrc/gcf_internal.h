@@ -139,7 +139,7 @@ cudaError_t fused_max_clusters(int* n, int* shape);
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
                          int nitems, const int* first, const float* inv, int nimg, const float* taper,
                          const float2* tw, float* partial, float* raw, int nclusters, int shape,
-                         cudaStream_t st);
+                         cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 
 // gcf_post.cu
 void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,

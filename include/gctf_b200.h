@@ -123,6 +123,49 @@ gcf_status gcf_gen_full_spectrum(gcf_ctx* ctx, const gcf_result* res, float* hos
 gcf_status gcf_get_radial_average(gcf_ctx* ctx, float* host_out);
 
 /* ---------------------------------------------------------------------- */
+/* CTF theory (CCTFTheory / CCTFParam, FindCTF/CCTFTheory.cpp:9-301,         */
+/* FindCTF/CFindCTFInc.h:8-91): host math, no GPU, bit-identical to the      */
+/* reference's float/double arithmetic.                                      */
+/* ---------------------------------------------------------------------- */
+/* Field order and units of CCTFParam: lengths in pixels, angles in radian. */
+typedef struct {
+    float wavelength;    /* pixel                                   */
+    float cs;            /* spherical aberration, pixel             */
+    float amp_contrast;  /* fraction                                */
+    float amp_phase;     /* atan(Ac / sqrt(1 - Ac^2)), radian       */
+    float ext_phase;     /* extra phase mod pi, radian              */
+    float df_max;        /* pixel                                   */
+    float df_min;        /* pixel                                   */
+    float azimuth;       /* astigmatism azimuth, radian             */
+    float ast_tol;       /* pixel                                   */
+    float pixel_size;    /* Angstrom                                */
+} gcf_ctf_param;
+
+/* CCTFTheory::Setup(kV, Cs mm, Ac, pixel A, astigmatism tolerance A,
+ * extra phase radian); clears the defocus. */
+gcf_status gcf_ctf_setup(gcf_ctf_param* p, float kv, float cs_mm, float amp_contrast,
+                         float pixel_size, float ast_tol, float ext_phase_rad);
+gcf_status gcf_ctf_set_ext_phase(gcf_ctf_param* p, float phase, int degree);
+gcf_status gcf_ctf_get_ext_phase(const gcf_ctf_param* p, int degree, float* out);
+/* CCTFTheory::SetDefocus (Angstrom) / SetDefocusInPixel. */
+gcf_status gcf_ctf_set_defocus(gcf_ctf_param* p, float df_min_a, float df_max_a, float azimuth_rad);
+gcf_status gcf_ctf_set_defocus_px(gcf_ctf_param* p, float df_min_px, float df_max_px,
+                                  float azimuth_rad);
+gcf_status gcf_ctf_change_pixel_size(gcf_ctf_param* p, float new_pixel_size);
+/* CCTFTheory::Evaluate: -sin(phase shift) at a relative frequency in
+ * [-0.5, 0.5] (1/pixel) along `azimuth` (radian). */
+gcf_status gcf_ctf_evaluate(const gcf_ctf_param* p, float freq, float azimuth, float* out);
+gcf_status gcf_ctf_phase_shift(const gcf_ctf_param* p, float freq, float azimuth, float* out);
+/* CCTFTheory::CalcDefocus: defocus (pixel) along an azimuth. */
+gcf_status gcf_ctf_defocus(const gcf_ctf_param* p, float azimuth, float* out);
+/* CCTFTheory::CalcFrequency / CalcNthZero: relative frequency where the
+ * phase shift reaches `phase` (n pi); 0 if none. */
+gcf_status gcf_ctf_frequency(const gcf_ctf_param* p, float phase, float azimuth, float* out);
+gcf_status gcf_ctf_nth_zero(const gcf_ctf_param* p, int n, float azimuth, float* out);
+/* CCTFTheory::EqualTo: *out = 1 when p and q agree within the tolerances. */
+gcf_status gcf_ctf_equal(const gcf_ctf_param* p, const gcf_ctf_param* q, float df_tol, int* out);
+
+/* ---------------------------------------------------------------------- */
 /* Rescale (CRescaleImage, FindCTF/CRescaleImage.cpp:47-99)                  */
 /* ---------------------------------------------------------------------- */
 void       gcf_rescale_dims(int width, int height, float pixel_size, int* new_width,
@@ -207,9 +250,10 @@ gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height,
                                     float* dev_raw_out, void* cuda_stream);
 
 /* Device time (ms, CUDA events on the context streams) of the stages of the
- * last batched call: [0] upload of host inputs (it overlaps [2]), [1] 0
- * (rescale runs inside [2]), [2] rescale + tile spectra, [3] background +
- * lowpass + radial, [4] 1D search, [5] 2D search, [6] total. */
+ * last batched call: [0] upload of host inputs (it overlaps [2]), [1] the
+ * fused tile-spectrum kernel launches alone (inside [2]; 0 for the cuFFT
+ * variant), [2] rescale + tile spectra, [3] background + lowpass + radial,
+ * [4] 1D search, [5] 2D search, [6] total. */
 gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7]);
 /* Number of kernels this library launched in the last batched call. */
 gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);

@@ -224,4 +224,34 @@ int gref_single(const float* image, int width, int height, float kv, float cs_mm
     return e == cudaSuccess ? 0 : (int)e;
 }
 
+
+// CCTFTheory host math (FindCTF/CCTFTheory.cpp) on arrays of inputs; needs
+// no GPU.  param_out: the 10 CCTFParam floats after Setup + SetDefocus.
+// For k < n: evaluate / phase_shift / defocus at (freq[k], azimuth[k]);
+// frequency at (phase[k], azimuth[k]); zeros[k] = CalcNthZero(k + 1,
+// azimuth[k]).
+void gref_ctf_theory(float kv, float cs_mm, float amp_contrast, float pixel_size, float ast_tol,
+                     float ext_phase_rad, float df_min, float df_max, float azimuth_rad, int n,
+                     const float* freq, const float* azimuth, const float* phase, float* evaluate,
+                     float* phase_shift, float* defocus, float* frequency, float* zeros,
+                     float* param_out)
+{
+    CCTFTheory* t = new CCTFTheory;
+    t->Setup(kv, cs_mm, amp_contrast, pixel_size, ast_tol, ext_phase_rad);
+    t->SetDefocus(df_min, df_max, azimuth_rad);
+    for (int k = 0; k < n; ++k) {
+        evaluate[k] = t->Evaluate(freq[k], azimuth[k]);
+        phase_shift[k] = t->CalcPhaseShift(freq[k], azimuth[k]);
+        defocus[k] = t->CalcDefocus(azimuth[k]);
+        frequency[k] = t->CalcFrequency(phase[k], azimuth[k]);
+        zeros[k] = t->CalcNthZero(k + 1, azimuth[k]);
+    }
+    CCTFParam* p = t->GetParam(false);
+    float v[10] = {p->m_fWavelength, p->m_fCs,      p->m_fAmpContrast, p->m_fAmpPhaseShift,
+                   p->m_fExtPhase,   p->m_fDefocusMax, p->m_fDefocusMin, p->m_fAstAzimuth,
+                   p->m_fAstTol,     p->m_fPixelSize};
+    memcpy(param_out, v, sizeof(v));
+    delete t;
+}
+
 }  // extern "C"

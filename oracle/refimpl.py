@@ -4,7 +4,7 @@
 TEST INFRASTRUCTURE ONLY: the parity tests, the golden-fixture script and
 bench.py's reference arm use this module; the product package
 (gctffind_b200) never imports it.  The library runs the reference's CUDA
-kernels, so every call needs a GPU.
+kernels, so every call but ctf_theory (host math) needs a GPU.
 """
 from __future__ import annotations
 
@@ -54,6 +54,8 @@ def lib():
                               C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p, _F, C.c_int]
     L.gref_single.restype = C.c_int
+    L.gref_ctf_theory.argtypes = [C.c_float] * 9 + [C.c_int] + [_F] * 9
+    L.gref_ctf_theory.restype = None
     _lib = L
     return L
 
@@ -116,3 +118,20 @@ def single(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_
     return {"new_size": (nw, nh), "new_pixel_size": npx.value,
             "rescaled": resc[: nw * nh].reshape(nh, nw), "raw_half": raw, "ctf_half": ctf,
             "full": full, "result": out}
+
+
+def ctf_theory(kv, cs_mm, amp_contrast, pixel_size, ast_tol, ext_phase_rad, df_min, df_max,
+               azimuth_rad, freq, azimuth, phase):
+    """The reference's CCTFTheory on arrays (host code: no GPU needed)."""
+    freq = np.ascontiguousarray(freq, np.float32)
+    azimuth = np.ascontiguousarray(azimuth, np.float32)
+    phase = np.ascontiguousarray(phase, np.float32)
+    n = len(freq)
+    outs = [np.zeros(n, np.float32) for _ in range(5)]
+    param = np.zeros(10, np.float32)
+    lib().gref_ctf_theory(kv, cs_mm, amp_contrast, pixel_size, ast_tol, ext_phase_rad, df_min,
+                          df_max, azimuth_rad, n, freq, azimuth, phase, *outs, param)
+    keys = ["evaluate", "phase_shift", "defocus", "frequency", "zeros"]
+    d = dict(zip(keys, outs))
+    d["param"] = param
+    return d
