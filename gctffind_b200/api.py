@@ -28,6 +28,7 @@ GCF_SPECT_CUFFT = 1
 EXPORTS = [
     "gcf_create", "gcf_destroy", "gcf_strerror", "gcf_last_error", "gcf_set_spectrum_impl",
     "gcf_setup", "gcf_gen_half_spectrum", "gcf_set_phase", "gcf_do2d", "gcf_refine",
+    "gcf_do1d", "gcf_refine1d",
     "gcf_get_spect_size", "gcf_get_half_spectrum", "gcf_gen_full_spectrum",
     "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
@@ -37,6 +38,7 @@ EXPORTS = [
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
     "gcf_ctf_phase_shift", "gcf_ctf_defocus", "gcf_ctf_frequency", "gcf_ctf_nth_zero",
     "gcf_ctf_equal",
+    "gcf_background1d", "gcf_remove_background1d", "gcf_remove_background2d",
 ]
 
 
@@ -104,6 +106,8 @@ def load_library(path: str = LIB_PATH):
     L.gcf_do2d.argtypes = [vp, C.POINTER(Result)]
     L.gcf_refine.argtypes = [vp, C.POINTER(f), C.POINTER(f), C.POINTER(f), C.POINTER(f),
                              C.POINTER(Result)]
+    L.gcf_do1d.argtypes = [vp, C.POINTER(Result)]
+    L.gcf_refine1d.argtypes = [vp, f, f, C.POINTER(Result)]
     L.gcf_get_spect_size.argtypes = [vp, C.POINTER(i), i]
     L.gcf_get_half_spectrum.argtypes = [vp, i, vp]
     L.gcf_gen_full_spectrum.argtypes = [vp, C.POINTER(Result), vp]
@@ -122,6 +126,9 @@ def load_library(path: str = LIB_PATH):
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
+    L.gcf_background1d.argtypes = [vp, vp, i, i, vp, C.POINTER(i)]
+    L.gcf_remove_background1d.argtypes = [vp, vp, i, vp, i, i, i]
+    L.gcf_remove_background2d.argtypes = [vp, vp, i, vp, i, i, i]
     P = C.POINTER(CtfParam)
     L.gcf_ctf_setup.argtypes = [P, f, f, f, f, f, f]
     L.gcf_ctf_set_ext_phase.argtypes = [P, f, i]
@@ -234,6 +241,40 @@ class Context:
         _check(self.L.gcf_refine(self._h, arr(df_mean), arr(ast_ratio), arr(ast_angle),
                                  arr(ext_phase), C.byref(r)), self._h)
         return r
+
+    def do1d(self) -> Result:
+        r = Result()
+        _check(self.L.gcf_do1d(self._h, C.byref(r)), self._h)
+        return r
+
+    def refine1d(self, init_df: float, df_range: float) -> Result:
+        r = Result()
+        _check(self.L.gcf_refine1d(self._h, init_df, df_range, C.byref(r)), self._h)
+        return r
+
+    # -- GBackground1D (host numpy arrays) -------------------------------------
+    def background1d(self, spectrum):
+        """(background, start) of a 1D spectrum."""
+        sp = np.ascontiguousarray(spectrum, np.float32)
+        bg = np.zeros_like(sp)
+        st = C.c_int()
+        _check(self.L.gcf_background1d(self._h, sp.ctypes.data, len(sp), 0, bg.ctypes.data,
+                                       C.byref(st)), self._h)
+        return bg, st.value
+
+    def remove_background1d(self, spectrum, background, start):
+        sp = np.array(spectrum, np.float32)
+        bg = np.ascontiguousarray(background, np.float32)
+        _check(self.L.gcf_remove_background1d(self._h, sp.ctypes.data, len(sp), bg.ctypes.data,
+                                              len(bg), int(start), 0), self._h)
+        return sp
+
+    def remove_background2d(self, half_spectrum, background, start):
+        sp = np.array(half_spectrum, np.float32)
+        bg = np.ascontiguousarray(background, np.float32)
+        _check(self.L.gcf_remove_background2d(self._h, sp.ctypes.data, sp.shape[0], bg.ctypes.data,
+                                              len(bg), int(start), 0), self._h)
+        return sp
 
     def half_spectrum(self, raw: bool) -> np.ndarray:
         out = np.zeros((self.tile_size, self.tile_size // 2 + 1), np.float32)
@@ -398,7 +439,8 @@ class CCTFTheory:
 
 
 class CFindCtf2D:
-    """CFindCtf2D call shape (FindCTF/CFindCTFInc.h:605-623) on a Context."""
+    """CFindCtf2D call shape (FindCTF/CFindCTFInc.h:581-615, with the Do1D /
+    Refine1D of its CFindCtf1D base) on a Context."""
 
     def __init__(self, tile_size: int = 512, log_spect: int = 0, gpu: int = 0, ctx=None):
         self.ctx = ctx or Context(gpu, tile_size, log_spect)
@@ -429,6 +471,13 @@ class CFindCtf2D:
 
     def Refine(self, afDfMean, afAstRatio, afAstAngle, afExtPhase):
         self._take(self.ctx.refine(afDfMean, afAstRatio, afAstAngle, afExtPhase))
+
+    # CFindCtf1D (FindCTF/CFindCtf1D.cpp:49-67), the base of CFindCtf2D
+    def Do1D(self):
+        self._take(self.ctx.do1d())
+
+    def Refine1D(self, fInitDf, fDfRange):
+        self._take(self.ctx.refine1d(fInitDf, fDfRange))
 
     def GenFullSpectrum(self):
         return self.ctx.full_spectrum(self._result)

@@ -127,6 +127,10 @@ struct gcf_ctx {
     float phase_deg = 0.0f, phase_range = 0.0f;
     float held_phase = 0.0f;   // CFindDefocus2D::m_fExtPhase between Do2D / Refine calls
     int cur_lowpassed = 0;
+
+    // GBackground1D
+    DBuf<float> bg_spec, bg_curve;
+    DBuf<int> bg_start;
 };
 
 namespace {
@@ -611,6 +615,7 @@ struct JobSpec {
     float phase_deg, phase_range;     // Do2D: CFindCtfBase::m_fExtPhase / m_fPhaseRange
     float rin[8];                     // Refine: {df, df_range, ast, ast_range, ang, ang_range, ph, ph_range}
     float held_phase;                 // extra phase the search object holds on entry (0 after Setup1)
+    float r1d_df, r1d_range;          // Refine1D: initial defocus and window (Angstrom)
 };
 
 // CFindDefocus2D::Setup3 + Refine (FindCTF/CFindDefocus2D.cpp:98-151) on the host.
@@ -645,7 +650,7 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     std::vector<SearchJob> jh(nj);
     std::vector<int> soff(nj);
     int tot = 0, max_band = 0;
-    bool any_full = false, any_grid = false, any_phase = false;
+    bool any_full = false, any_grid = false, any_phase = false, any_1d = false;
     for (int j = 0; j < nj; ++j) {
         const JobSpec& s = specs[j];
         SearchJob& J = jh[j];
@@ -659,8 +664,12 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         J.phase_range_in = fmaxf(s.phase_range, 0.0f);
         J.ext_phase_in = s.phase_deg;
         J.held_phase = s.held_phase;
+        J.r1d_df = s.r1d_df;
+        J.r1d_range = s.r1d_range;
         J.step = STEP_CC0;
-        if (s.mode == 1) {
+        if (s.mode >= 2) {
+            any_1d = true;
+        } else if (s.mode == 1) {
             refine_init(J, s.rin);
             if (J.ast_range[1] - J.ast_range[0] >= (float)1e-20 ||
                 J.ang_range[1] - J.ang_range[0] >= (float)1e-20)
@@ -707,7 +716,7 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     a.max_chunks = max_chunks;
     a.njobs = nj;
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
-    if (any_full) {
+    if (any_full || any_1d) {
         launch_search1d(ctx->jobs.p, nj, ctx->radial.p, cx, ctx->cand.p, ctx->cval.p, ctx->st);
         CKL();
         ctx->launches += 1;
@@ -717,7 +726,9 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[6], ctx->st));
     // Upper bound of non-empty steps: CC0 + astigmatism grid + 19 x 4 refinements.
-    int pairs = 2 + 19 * ((any_grid ? 2 : 0) + 1 + (any_phase ? 1 : 0));
+    bool any_2d = false;
+    for (const JobSpec& s : specs) any_2d = any_2d || s.mode <= 1;
+    int pairs = any_2d ? 2 + 19 * ((any_grid ? 2 : 0) + 1 + (any_phase ? 1 : 0)) : 0;
     for (int k = 0; k < pairs; ++k) {
         int cb = (k == 0) ? 1 : (k == 1 && any_grid) ? (kMaxCand / kEvalCB + 3) / 4 : 4;
         launch_eval2d(a, cb, max_band, ctx->st);
@@ -726,16 +737,19 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         CKL();
         ctx->launches += 2;
     }
-    // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)
-    CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
-    launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p, ctx->ring_sums.p,
-                   ctx->cc_res.p, ctx->st);
-    CKL();
-    launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
-    CKL();
+    if (any_2d) {
+        // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)
+        CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
+        launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p,
+                       ctx->ring_sums.p, ctx->cc_res.p, ctx->st);
+        CKL();
+        launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
+        CKL();
+        ctx->launches += 3;
+    }
     launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->st);
     CKL();
-    ctx->launches += 4;
+    ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[7], ctx->st));
     CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost,
                        ctx->st));
@@ -1177,7 +1191,41 @@ gcf_status gcf_do2d(gcf_ctx* ctx, gcf_result* out)
     CKS(run_search(ctx, {s}, r));
     *out = r[0];
     ctx->held_phase = r[0].ext_phase;
+    ctx->phase_deg = r[0].ext_phase;   // CFindCtf2D::mGetResults sets m_fExtPhase
     return GCF_OK;
+}
+
+// CFindCtf1D::Do1D / Refine1D (FindCTF/CFindCtf1D.cpp:49-67): the radial
+// average of the current spectrum, then the brute-force defocus (x phase)
+// searches; m_fExtPhase takes the found phase.
+static gcf_status run_1d(gcf_ctx* ctx, int mode, float init_df, float df_range, gcf_result* out)
+{
+    if (!ctx || !out) return GCF_ERR_INVALID_ARG;
+    if (!ctx->have_spectrum) return fail(ctx, GCF_ERR_STATE, "no spectrum: call gcf_gen_half_spectrum");
+    CKS(set_device(ctx));
+    JobSpec s;
+    std::memset(&s, 0, sizeof(s));
+    s.mic = 0;
+    s.mode = mode;
+    s.optics = ctx->optics;
+    s.px_n = ctx->optics.pixel_size;
+    s.phase_deg = ctx->phase_deg;
+    s.phase_range = ctx->phase_range;
+    s.r1d_df = init_df;
+    s.r1d_range = df_range;
+    std::vector<gcf_result> r;
+    CKS(run_search(ctx, {s}, r));
+    *out = r[0];
+    ctx->phase_deg = r[0].ext_phase;
+    return GCF_OK;
+}
+
+gcf_status gcf_do1d(gcf_ctx* ctx, gcf_result* out) { return run_1d(ctx, 2, 0.0f, 0.0f, out); }
+
+gcf_status gcf_refine1d(gcf_ctx* ctx, float init_df, float df_range, gcf_result* out)
+{
+    if (!(df_range >= 0.0f) || !(init_df > 0.0f)) return GCF_ERR_INVALID_ARG;
+    return run_1d(ctx, 3, init_df, df_range, out);
 }
 
 gcf_status gcf_refine(gcf_ctx* ctx, const float df[2], const float ast[2], const float ang[2],
@@ -1199,7 +1247,74 @@ gcf_status gcf_refine(gcf_ctx* ctx, const float df[2], const float ast[2], const
     CKS(run_search(ctx, {s}, r));
     *out = r[0];
     ctx->held_phase = r[0].ext_phase;
+    ctx->phase_deg = r[0].ext_phase;
     return GCF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// GBackground1D (FindCTF/GBackground1D.cu:61-169)
+// ---------------------------------------------------------------------------
+gcf_status gcf_background1d(gcf_ctx* ctx, const float* spectrum, int n, int on_device,
+                            float* background, int* start)
+{
+    if (!ctx || !spectrum || !background || !start || n <= 0 || n > kMaxBackgroundBins)
+        return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    const float* d_in = spectrum;
+    float* d_out = background;
+    if (!on_device) {
+        CK(ctx->bg_spec.ensure(n));
+        CK(ctx->bg_curve.ensure(n));
+        CK(cudaMemcpyAsync(ctx->bg_spec.p, spectrum, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        d_in = ctx->bg_spec.p;
+        d_out = ctx->bg_curve.p;
+    }
+    CK(ctx->bg_start.ensure(1));
+    CK(launch_background1d(d_in, n, d_out, ctx->bg_start.p, ctx->st));
+    ctx->launches += 1;
+    if (!on_device)
+        CK(cudaMemcpyAsync(background, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(start, ctx->bg_start.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+static gcf_status remove_bg(gcf_ctx* ctx, float* spec, size_t spec_n, int n_or_tile, bool two_d,
+                            const float* bg, int bg_n, int start, int on_device)
+{
+    if (!ctx || !spec || !bg || n_or_tile <= 0 || bg_n <= 0) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    float* d_spec = spec;
+    const float* d_bg = bg;
+    if (!on_device) {
+        CK(ctx->bg_spec.ensure(spec_n));
+        CK(ctx->bg_curve.ensure(bg_n));
+        CK(cudaMemcpyAsync(ctx->bg_spec.p, spec, spec_n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->bg_curve.p, bg, bg_n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        d_spec = ctx->bg_spec.p;
+        d_bg = ctx->bg_curve.p;
+    }
+    if (two_d) CK(launch_remove_background2d(d_spec, n_or_tile, d_bg, bg_n, start, ctx->st));
+    else CK(launch_remove_background1d(d_spec, n_or_tile, d_bg, bg_n, start, ctx->st));
+    ctx->launches += 1;
+    if (!on_device)
+        CK(cudaMemcpyAsync(spec, d_spec, spec_n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_remove_background1d(gcf_ctx* ctx, float* spectrum, int n, const float* background,
+                                   int bg_n, int start, int on_device)
+{
+    return remove_bg(ctx, spectrum, (size_t)std::max(n, 0), n, false, background, bg_n, start, on_device);
+}
+
+gcf_status gcf_remove_background2d(gcf_ctx* ctx, float* half_spectrum, int tile,
+                                   const float* background, int bg_n, int start, int on_device)
+{
+    if (tile <= 0 || tile % 2) return GCF_ERR_INVALID_ARG;
+    return remove_bg(ctx, half_spectrum, (size_t)(tile / 2 + 1) * tile, tile, true, background, bg_n,
+                     start, on_device);
 }
 
 gcf_status gcf_get_spect_size(gcf_ctx* ctx, int size[2], int half)

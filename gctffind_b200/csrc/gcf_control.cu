@@ -332,6 +332,7 @@ __global__ void k_update2d(SearchJob* __restrict__ jobs, const BandDev* __restri
     float4* cj = cand + (size_t)j * kMaxCand;
     float2* vj = cval + (size_t)j * kMaxCand;
     if (init) {
+        if (sJ.mode >= 2) return;   // 1D-only job, finished by k_search1d
         // fresh job: pending step is CC0 with one candidate
         if (threadIdx.x == 0) {
             sJ.step = STEP_CC0;
@@ -454,7 +455,7 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     const int j = blockIdx.x;
     if (threadIdx.x == 0) sJ = jobs[j];
     __syncthreads();
-    if (sJ.mode != 0) return;
+    if (sJ.mode == 1) return;   // Refine has no 1D stage
     const PixOptics o = sJ.o;
     const float* rad = radial + (size_t)sJ.mic * cx;
     // CFindDefocus1D::mCorrelate band (FindCTF/CFindDefocus1D.cpp:128-137)
@@ -490,13 +491,22 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     // CFindCtf1D::mFindDefocus (FindCTF/CFindCtf1D.cpp:73-90)
     float ext = sJ.ext_phase_in, prange = sJ.phase_range_in;
     float px2 = o.px * o.px;
-    float dfr[2] = {3000.0f * px2, 30000.0f * px2};
-    float phr[2];
-    phr[0] = fmaxf(ext - prange / 2, 0.0f);
-    phr[1] = fminf(phr[0] + prange, 150.0f);
-    Brute b1 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr, phr, shm);
+    Brute b1;
+    float range;
+    if (sJ.mode == 3) {
+        // CFindCtf1D::Refine1D (FindCTF/CFindCtf1D.cpp:58-67): refine pass only,
+        // around the given defocus and the current extra phase
+        b1 = Brute{sJ.r1d_df, ext, 0.0f};
+        range = sJ.r1d_range;
+    } else {
+        float dfr[2] = {3000.0f * px2, 30000.0f * px2};
+        float phr[2];
+        phr[0] = fmaxf(ext - prange / 2, 0.0f);
+        phr[1] = fminf(phr[0] + prange, 150.0f);
+        b1 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr, phr, shm);
+        range = fmaxf(0.3f * b1.df, 3000.0f);   // CFindCtf1D::Do1D (FindCTF/CFindCtf1D.cpp:49-56)
+    }
     // CFindCtf1D::mRefineDefocus (FindCTF/CFindCtf1D.cpp:92-111)
-    float range = fmaxf(0.3f * b1.df, 3000.0f);
     float mindf = 3000.0f * o.px * o.px;
     float dfr2[2];
     dfr2[0] = fmaxf(b1.df - range / 2, mindf);
@@ -506,6 +516,17 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     phr2[0] = fmaxf(b1.ph - pr / 2, 0.0f);
     phr2[1] = fminf(0.0f + pr, 150.0f);   // the reference reads the zero-initialised bound
     Brute b2 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr2, phr2, shm);
+    if (sJ.mode >= 2) {   // Do1D / Refine1D alone: no 2D search follows
+        if (threadIdx.x == 0) {
+            sJ.df_1d = b2.df;
+            sJ.phase_1d = b2.ph;
+            sJ.score_1d = b2.cc;
+            sJ.step = STEP_DONE;
+            sJ.ncand = 0;
+            jobs[j] = sJ;
+        }
+        return;
+    }
     float2* vj = cval + (size_t)j * kMaxCand;
     __shared__ int s_n;
     if (threadIdx.x == 0) {
@@ -570,6 +591,20 @@ __global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const i
     if (j >= njobs) return;
     const SearchJob& J = jobs[j];
     gcf_result r;
+    if (J.mode >= 2) {   // CFindCtf1D results: m_fDfMin = m_fDfMax = 1D defocus
+        r.df_min = J.df_1d;
+        r.df_max = J.df_1d;
+        r.azimuth = 0.0f;
+        r.ext_phase = J.phase_1d;
+        r.score = J.score_1d;
+        r.ctf_res = 0.0f;
+        r.df_1d = J.df_1d;
+        r.phase_1d = J.phase_1d;
+        r.score_1d = J.score_1d;
+        r.lowpassed = lowpassed ? lowpassed[J.mic] : 0;
+        out[j] = r;
+        return;
+    }
     r.df_min = J.df_mean * (1.0f - J.ast_ratio);
     r.df_max = J.df_mean * (1.0f + J.ast_ratio);
     r.azimuth = J.ast_angle;

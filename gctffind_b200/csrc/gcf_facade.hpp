@@ -99,6 +99,7 @@ public:
     CFindCtf2D& operator=(const CFindCtf2D&) = delete;
 
     void Setup1(CCTFTheory* pCtfTheory) { m_optics = pCtfTheory->m_optics; }
+    // Same object for code written against CFindCtf1D.
     void Setup2(const int* piImgSize)
     {
         m_aiImgSize[0] = piImgSize[0];
@@ -128,6 +129,17 @@ public:
                 const float afExtPhase[2])
     {
         gcf_check(gcf_refine(m_ctx, afDfMean, afAstRatio, afAstAngle, afExtPhase, &m_result), m_ctx);
+        mGetResults();
+    }
+    // CFindCtf1D::Do1D / Refine1D (FindCTF/CFindCtf1D.cpp:49-67).
+    void Do1D()
+    {
+        gcf_check(gcf_do1d(m_ctx, &m_result), m_ctx);
+        mGetResults();
+    }
+    void Refine1D(float fInitDf, float fDfRange)
+    {
+        gcf_check(gcf_refine1d(m_ctx, fInitDf, fDfRange, &m_result), m_ctx);
         mGetResults();
     }
     // Caller frees with delete[] (FindCTF/CFindCtfBase.cpp:118-133).
@@ -167,5 +179,7 @@ private:
     gcf_result m_result{};
     int m_aiImgSize[2] = {0, 0};
 };
+
+using CFindCtf1D = CFindCtf2D;
 
 }  // namespace GCTFFind

@@ -51,7 +51,7 @@ struct SearchJob {
     // inputs
     int mic;            // spectrum slot
     int band;           // band-table slot
-    int mode;           // 0 = Do2D (after the 1D search), 1 = Refine
+    int mode;           // 0 = Do2D (after the 1D search), 1 = Refine, 2 = Do1D, 3 = Refine1D
     int pad0;
     PixOptics o;
     float phase_range_in;   // CFindCtfBase::m_fPhaseRange (Do2D)
@@ -64,6 +64,7 @@ struct SearchJob {
     // for an object that Setup1 has just created, else the phase the
     // previous search on the same object ended with.
     float held_phase;
+    float r1d_df, r1d_range;   // Refine1D: initial defocus and window, Angstrom
     int pad2;
     // CFindDefocus2D state
     float df_mean, ast_ratio, ast_angle, ext_phase, cc_max, old_cc;
@@ -173,5 +174,13 @@ void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, in
                          cudaStream_t st);
 void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out,
                     cudaStream_t st);
+
+// gcf_background.cu: GBackground1D
+constexpr int kMaxBackgroundBins = 12288;   // one block's shared memory (48 KB)
+cudaError_t launch_background1d(const float* spec, int n, float* bg, int* start, cudaStream_t st);
+cudaError_t launch_remove_background1d(float* spec, int n, const float* bg, int bg_n, int start,
+                                       cudaStream_t st);
+cudaError_t launch_remove_background2d(float* spec, int tile, const float* bg, int bg_n, int start,
+                                       cudaStream_t st);
 
 }  // namespace gcf

@@ -105,6 +105,36 @@ gcf_status gcf_do2d(gcf_ctx* ctx, gcf_result* out);
 gcf_status gcf_refine(gcf_ctx* ctx, const float df_mean[2], const float ast_ratio[2],
                       const float ast_angle[2], const float ext_phase[2], gcf_result* out);
 
+/* CFindCtf1D::Do1D (FindCTF/CFindCtf1D.cpp:49-56): radial average, brute-
+ * force defocus x extra-phase search, refinement; out->df_min = df_max =
+ * the 1D defocus, out->ext_phase / score its phase and CC.  Like the
+ * reference it moves the context's extra phase (SetPhase) to the result. */
+gcf_status gcf_do1d(gcf_ctx* ctx, gcf_result* out);
+/* CFindCtf1D::Refine1D (FindCTF/CFindCtf1D.cpp:58-67): the refinement pass
+ * alone around init_df (Angstrom) over df_range, centred on the context's
+ * extra phase. */
+gcf_status gcf_refine1d(gcf_ctx* ctx, float init_df, float df_range, gcf_result* out);
+
+/* GBackground1D (FindCTF/GBackground1D.cu:61-169).  The reference keeps
+ * this 1D background model without calling it; it is offered here behind
+ * the same three operations.  `on_device` says whether every array
+ * argument is device memory (else host).  n <= 12288 bins. */
+/* DoIt + mFindStart: start = first bin from 2 on where the spectrum falls to
+ * the least-squares line fitted over bins [n/5, n - n/5) (n/5 if none);
+ * background[i] = mean of the start/2*2-1 bins centred on i (mirrored at
+ * the end) for i >= start, 0 below. */
+gcf_status gcf_background1d(gcf_ctx* ctx, const float* spectrum, int n, int on_device,
+                            float* background, int* start);
+/* Remove1D: spectrum[i] -= background[i] for start <= i < min(n, bg_n),
+ * 0 for i < start (in place). */
+gcf_status gcf_remove_background1d(gcf_ctx* ctx, float* spectrum, int n, const float* background,
+                                   int bg_n, int start, int on_device);
+/* Remove2D: on a tile x (tile/2+1) half spectrum (DC at (0, tile/2)),
+ * subtract the background at radius r (pixels, linear interpolation;
+ * background[bg_n-1] from r >= bg_n - 1), 0 inside r < start (in place). */
+gcf_status gcf_remove_background2d(gcf_ctx* ctx, float* half_spectrum, int tile,
+                                   const float* background, int bg_n, int start, int on_device);
+
 /* CFindCtfBase::GetSpectSize (FindCTF/CFindCtfBase.cpp:102-107). */
 gcf_status gcf_get_spect_size(gcf_ctx* ctx, int size[2], int half);
 

@@ -1024,6 +1024,34 @@ extern "C" int orc_search1d(const double* ctf, int tile, float px_n, const orc_p
     return 0;
 }
 
+/* CFindCtf1D::Refine1D (FindCTF/CFindCtf1D.cpp:58-67): the refinement pass
+ * alone around init_df, centred on the current extra phase. */
+extern "C" int orc_refine1d(const double* ctf, int tile, float px_n, const orc_params* p,
+                            float init_df, float df_range, float* df, float* phase, float* score)
+{
+    int cx = tile / 2 + 1;
+    PixOptics o = make_optics(p, px_n);
+    float rr[2];
+    res_range_of(px_n, rr);
+    std::vector<double> radial(cx);
+    orc_radial_average(ctf, tile, radial.data());
+    float prange = fmaxf(p->ext_phase_range, 0.0f);
+    float mindf = 3000.0f * px_n * px_n;
+    float dfr2[2];
+    dfr2[0] = fmaxf(init_df - df_range / 2, mindf);
+    dfr2[1] = dfr2[0] + df_range;
+    float pr = 0.2f * prange;
+    float phr2[2] = {0.0f, 0.0f};
+    phr2[0] = fmax(p->ext_phase_deg - pr / 2, 0.0f);
+    phr2[1] = fmin(phr2[1] + pr, 150.0f);   // reads the zero-initialised [1]
+    float out[3];
+    brute_1d(radial.data(), cx, o, rr, dfr2, phr2, out);
+    *df = out[0];
+    *phase = out[1];
+    *score = out[2];
+    return 0;
+}
+
 extern "C" int orc_search(const double* ctf, int tile, float px_n, const orc_params* p, int mode,
                           const float* refine_in, orc_result* res)
 {
@@ -1198,4 +1226,87 @@ extern "C" int orc_series(const float* const* imgs, int n, int w, int h, const o
         }
     }
     return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* GBackground1D (FindCTF/GBackground1D.cu:13-169)                          */
+/* ------------------------------------------------------------------------ */
+
+/* DoIt + mFindStart (:95-169): double line fit over [n/5, n - n/5), first
+ * bin from 2 where the spectrum is at or below the line, moving average of
+ * width start/2*2-1 mirrored at the end. */
+extern "C" int orc_background1d(const float* spec, int n, float* bg, int* start_out)
+{
+    if (n <= 0) return -1;
+    int i0 = n / 5, i1 = n - i0;
+    double dx = 0, dy = 0, dx2 = 0, dxy = 0;
+    for (int i = i0; i < i1; ++i) {
+        dx += i;
+        dx2 += (i * i);
+        dy += spec[i];
+        dxy += (i * spec[i]);
+    }
+    int cnt = i1 - i0;
+    dx /= cnt;
+    dy /= cnt;
+    dx2 /= cnt;
+    dxy /= cnt;
+    double a = (dx * dy - dxy) / (dx * dx - dx2);
+    double b = dy - a * dx;
+    int start = i0;
+    for (int i = 2; i < n; ++i) {
+        double y = a * i + b;
+        if (y < spec[i]) continue;
+        start = i;
+        break;
+    }
+    int win = start / 2 * 2 - 1;
+    for (int i = 0; i < n; ++i) {
+        if (i < start) {
+            bg[i] = 0.0f;
+            continue;
+        }
+        float m = 0.0f;
+        for (int j = 0; j < win; ++j) {
+            int k = i + j - win / 2;
+            if (k >= n) k = 2 * n - 1 - k;
+            m += spec[k];
+        }
+        bg[i] = m / win;
+    }
+    *start_out = start;
+    return 0;
+}
+
+/* Remove1D (:13-30): bins >= bg_n are left alone (the reference sends them
+ * all to bin bg_n - 1 at once, a write race). */
+extern "C" void orc_remove_bg1d(float* spec, int n, const float* bg, int bg_n, int start)
+{
+    for (int i = 0; i < n; ++i) {
+        if (i < start) spec[i] = 0.0f;
+        else if (i < bg_n) spec[i] -= bg[i];
+    }
+}
+
+/* Remove2D (:32-59) on a tile x (tile/2+1) half spectrum. */
+extern "C" void orc_remove_bg2d(float* spec, int tile, const float* bg, int bg_n, int start)
+{
+    int cx = tile / 2 + 1;
+    for (int y = 0; y < tile; ++y) {
+        int yc = y - tile / 2;
+        for (int x = 0; x < cx; ++x) {
+            float* v = spec + (size_t)y * cx + x;
+            float r = sqrtf((float)(x * x + yc * yc));
+            if (r < start) {
+                *v = 0.0f;
+                continue;
+            }
+            if (r >= (bg_n - 1)) {
+                *v -= bg[bg_n - 1];
+                continue;
+            }
+            int ir = (int)r;
+            *v -= bg[ir] * (ir + 1 - r) + bg[ir + 1] * (r - ir);
+        }
+    }
 }

@@ -107,6 +107,9 @@ int orc_search(const double* ctf, int tile, float px_n, const orc_params* p,
 /* CFindCtf1D::Do1D on a given ctf spectrum (FindCTF/CFindCtf1D.cpp:49-59). */
 int orc_search1d(const double* ctf, int tile, float px_n, const orc_params* p,
                  float* df, float* phase, float* score);
+/* CFindCtf1D::Refine1D: refinement pass around init_df over df_range (A). */
+int orc_refine1d(const double* ctf, int tile, float px_n, const orc_params* p, float init_df,
+                 float df_range, float* df, float* phase, float* score);
 
 /* CSpectrumImage (FindCTF/CSpectrumImage.cpp:21-71): tile x tile float. */
 void orc_full_spectrum(const double* ctf, int tile, float px_n, const orc_params* p,
@@ -117,6 +120,12 @@ void orc_full_spectrum(const double* ctf, int tile, float px_n, const orc_params
  * tilt-series refine windows.  Results are written at res[image index]. */
 int orc_series(const float* const* imgs, int n, int w, int h, const orc_params* p,
                const int* order, int is_tomo, orc_result* res);
+
+/* GBackground1D: start bin and moving-average background of a 1D spectrum,
+ * and its removal from a 1D spectrum / a half spectrum (float, in place). */
+int  orc_background1d(const float* spec, int n, float* bg, int* start);
+void orc_remove_bg1d(float* spec, int n, const float* bg, int bg_n, int start);
+void orc_remove_bg2d(float* spec, int tile, const float* bg, int bg_n, int start);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,14 @@ def lib():
                              C.POINTER(OrcResult)]
     L.orc_search1d.argtypes = [_D, C.c_int, C.c_float, C.POINTER(OrcParams),
                                C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.orc_refine1d.argtypes = [_D, C.c_int, C.c_float, C.POINTER(OrcParams), C.c_float, C.c_float,
+                               C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.orc_background1d.argtypes = [_F, C.c_int, _F, C.POINTER(C.c_int)]
+    L.orc_background1d.restype = C.c_int
+    L.orc_remove_bg1d.argtypes = [_F, C.c_int, _F, C.c_int, C.c_int]
+    L.orc_remove_bg1d.restype = None
+    L.orc_remove_bg2d.argtypes = [_F, C.c_int, _F, C.c_int, C.c_int]
+    L.orc_remove_bg2d.restype = None
     L.orc_full_spectrum.argtypes = [_D, C.c_int, C.c_float, C.POINTER(OrcParams),
                                     C.POINTER(OrcResult), _F]
     L.orc_series.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int,
@@ -193,6 +201,13 @@ def search1d(ctf_spect: np.ndarray, px_n: float, p: OrcParams):
     return df.value, ph.value, sc.value
 
 
+def refine1d(ctf_spect: np.ndarray, px_n: float, p: OrcParams, init_df: float, df_range: float):
+    df, ph, sc = C.c_float(), C.c_float(), C.c_float()
+    lib().orc_refine1d(np.ascontiguousarray(ctf_spect, np.float64), ctf_spect.shape[0], px_n,
+                       C.byref(p), init_df, df_range, C.byref(df), C.byref(ph), C.byref(sc))
+    return df.value, ph.value, sc.value
+
+
 def full_spectrum(ctf_spect, px_n, p, res) -> np.ndarray:
     tile = ctf_spect.shape[0]
     out = np.zeros((tile, tile), np.float32)
@@ -239,3 +254,24 @@ def series(imgs: list, p: OrcParams, order: list, is_tomo: bool):
     if rc != 0:
         raise ValueError("oracle series failed")
     return [res[i] for i in range(len(arrs))]
+
+
+def background1d(spectrum):
+    """GBackground1D::DoIt: (background, start)."""
+    sp = np.ascontiguousarray(spectrum, np.float32)
+    bg = np.zeros_like(sp)
+    st = C.c_int()
+    lib().orc_background1d(sp, len(sp), bg, C.byref(st))
+    return bg, st.value
+
+
+def remove_bg1d(spectrum, bg, start):
+    sp = np.array(spectrum, np.float32)
+    lib().orc_remove_bg1d(sp, len(sp), np.ascontiguousarray(bg, np.float32), len(bg), int(start))
+    return sp
+
+
+def remove_bg2d(half, bg, start):
+    sp = np.array(half, np.float32)
+    lib().orc_remove_bg2d(sp, sp.shape[0], np.ascontiguousarray(bg, np.float32), len(bg), int(start))
+    return sp

@@ -254,4 +254,101 @@ void gref_ctf_theory(float kv, float cs_mm, float amp_contrast, float pixel_size
     delete t;
 }
 
+
+// CFindCtf1D::Do1D (refine_1d = 0) or Refine1D(init_df, df_range)
+// (FindCTF/CFindCtf1D.cpp:49-67) on one micrograph after SetPhase;
+// result: 1D defocus, extra phase, CC.
+int gref_single1d(const float* image, int width, int height, float kv, float cs_mm,
+                  float amp_contrast, float pixel_size, float ext_phase_deg, float ext_phase_range,
+                  int tile, int log_spect, int gpu, int refine_1d, float init_df, float df_range,
+                  float* result, int quiet)
+{
+    if (!image || !result) return -1;
+    cudaError_t e = cudaSetDevice(gpu);
+    if (e != cudaSuccess) return (int)e;
+    StdoutMute mute(quiet != 0);
+    CInput* in = CInput::GetInstance();
+    in->m_fKv = kv;
+    in->m_fCs = cs_mm;
+    in->m_fAmpContrast = amp_contrast;
+    in->m_fPixSize = pixel_size;
+    in->m_afExtPhase[0] = ext_phase_deg;
+    in->m_afExtPhase[1] = ext_phase_range;
+    in->m_iTileSize = tile;
+    in->m_iLogSpect = log_spect;
+    size_t px = (size_t)width * height;
+    float* host = new float[px];
+    memcpy(host, image, px * sizeof(float));
+    int raw_size[2] = {width, height};
+    CRescaleImage* rescale = new CRescaleImage;
+    CCTFTheory* theory = new CCTFTheory;
+    CFindCtf1D* find = new CFindCtf1D;
+    rescale->Setup(raw_size, pixel_size);
+    rescale->DoIt(host);
+    theory->Setup(kv, cs_mm, amp_contrast, rescale->m_fPixSizeN, 100.0f, ext_phase_deg * 0.017453f);
+    find->Setup1(theory);
+    find->Setup2(rescale->m_aiNewSize);
+    find->GenHalfSpectrum(rescale->GetScaledImg());
+    find->SetPhase(ext_phase_deg, ext_phase_range > 0.0f ? ext_phase_range : 0.0f);
+    if (refine_1d) find->Refine1D(init_df, df_range);
+    else find->Do1D();
+    result[0] = find->m_fDfMin;
+    result[1] = find->m_fExtPhase;
+    result[2] = find->m_fScore;
+    delete find;
+    delete theory;
+    delete rescale;
+    delete[] host;
+    cudaDeviceSynchronize();
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+
+// GBackground1D (FindCTF/GBackground1D.cu): DoIt on a host 1D spectrum of
+// n bins -> start and background (read back through Remove1D on zeros);
+// then Remove2D on a tile x (tile/2+1) half spectrum and Remove1D on an
+// m-bin spectrum (m <= n), both copied in and out.
+int gref_background1d(const float* spec, int n, float* bg_out, int* start_out, const float* half_in,
+                      int tile, float* half_out, const float* spec1d_in, int m, float* spec1d_out,
+                      int gpu)
+{
+    if (!spec || n <= 0 || !bg_out || !start_out || m > n) return -1;
+    cudaError_t e = cudaSetDevice(gpu);
+    if (e != cudaSuccess) return (int)e;
+    float* host = new float[n];
+    memcpy(host, spec, n * sizeof(float));
+    GBackground1D* b = new GBackground1D;
+    b->DoIt(host, n);
+    *start_out = b->m_iStart;
+    float* d = 0;
+    cudaMalloc(&d, sizeof(float) * n);
+    cudaMemset(d, 0, sizeof(float) * n);
+    b->Remove1D(d, n);
+    cudaMemcpy(bg_out, d, sizeof(float) * n, cudaMemcpyDefault);
+    for (int i = 0; i < n; ++i) bg_out[i] = 0.0f - bg_out[i];
+    cudaFree(d);
+    if (half_in && half_out && tile > 0) {
+        size_t hn = (size_t)(tile / 2 + 1) * tile;
+        cudaMalloc(&d, sizeof(float) * hn);
+        cudaMemcpy(d, half_in, sizeof(float) * hn, cudaMemcpyDefault);
+        int size[2] = {tile / 2 + 1, tile};
+        b->Remove2D(d, size);
+        cudaMemcpy(half_out, d, sizeof(float) * hn, cudaMemcpyDefault);
+        cudaFree(d);
+    }
+    if (spec1d_in && spec1d_out && m > 0) {
+        cudaMalloc(&d, sizeof(float) * m);
+        cudaMemcpy(d, spec1d_in, sizeof(float) * m, cudaMemcpyDefault);
+        b->Remove1D(d, m);
+        cudaMemcpy(spec1d_out, d, sizeof(float) * m, cudaMemcpyDefault);
+        cudaFree(d);
+    }
+    delete b;
+    delete[] host;
+    cudaDeviceSynchronize();
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
 }  // extern "C"

@@ -54,6 +54,12 @@ def lib():
                               C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p, _F, C.c_int]
     L.gref_single.restype = C.c_int
+    L.gref_single1d.argtypes = [_F, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] * 4 + \
+        [C.c_float, C.c_float, _F, C.c_int]
+    L.gref_single1d.restype = C.c_int
+    L.gref_background1d.argtypes = [_F, C.c_int, _F, C.POINTER(C.c_int), C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    L.gref_background1d.restype = C.c_int
     L.gref_ctf_theory.argtypes = [C.c_float] * 9 + [C.c_int] + [_F] * 9
     L.gref_ctf_theory.restype = None
     _lib = L
@@ -118,6 +124,40 @@ def single(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_
     return {"new_size": (nw, nh), "new_pixel_size": npx.value,
             "rescaled": resc[: nw * nh].reshape(nh, nw), "raw_half": raw, "ctf_half": ctf,
             "full": full, "result": out}
+
+
+def single1d(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_deg=0.0,
+             ext_phase_range=0.0, tile=512, log_spect=0, gpu=0, refine=None, quiet=True):
+    """CFindCtf1D::Do1D, or Refine1D(*refine) with refine = (init_df, range),
+    on one micrograph.  Returns (defocus, extra phase, CC)."""
+    img = np.ascontiguousarray(image, np.float32)
+    h, w = img.shape
+    out = np.zeros(3, np.float32)
+    r0, r1 = (0.0, 0.0) if refine is None else refine
+    rc = lib().gref_single1d(img, w, h, kv, cs_mm, amp_contrast, pixel_size, ext_phase_deg,
+                             ext_phase_range, tile, log_spect, gpu, 0 if refine is None else 1,
+                             r0, r1, out, 1 if quiet else 0)
+    if rc != 0:
+        raise RuntimeError(f"reference single1d failed: {rc}")
+    return tuple(float(x) for x in out)
+
+
+def background1d(spectrum, half=None, spec1d=None, gpu=0):
+    """GBackground1D::DoIt on a 1D spectrum, then Remove2D on `half` and
+    Remove1D on `spec1d`.  Returns (background, start, half_out, spec1d_out)."""
+    sp = np.ascontiguousarray(spectrum, np.float32)
+    n = len(sp)
+    bg = np.zeros(n, np.float32)
+    st = C.c_int()
+    hin = None if half is None else np.ascontiguousarray(half, np.float32)
+    hout = None if half is None else np.zeros_like(hin)
+    s1 = None if spec1d is None else np.ascontiguousarray(spec1d, np.float32)
+    s1o = None if spec1d is None else np.zeros_like(s1)
+    rc = lib().gref_background1d(sp, n, bg, C.byref(st), _ptr(hin), 0 if hin is None else hin.shape[0],
+                                 _ptr(hout), _ptr(s1), 0 if s1 is None else len(s1), _ptr(s1o), gpu)
+    if rc != 0:
+        raise RuntimeError(f"reference background1d failed: {rc}")
+    return bg, st.value, hout, s1o
 
 
 def ctf_theory(kv, cs_mm, amp_contrast, pixel_size, ast_tol, ext_phase_rad, df_min, df_max,

@@ -88,6 +88,23 @@ def test_do2d_matches_oracle(case):
     assert _ang_diff(r.azimuth, 20.0) < 3.0
 
 
+def test_do1d_refine1d_match_oracle(case, oracle):
+    """CFindCtf1D::Do1D / Refine1D on the GPU spectrum vs the oracle's 1D
+    searches on the same spectrum: same grid point, CC within 1e-4."""
+    ctx = case["ctx"]
+    g_ctf = ctx.half_spectrum(raw=False).astype(np.float64)
+    ctx.set_phase(0.0, 0.0)
+    r1 = ctx.do1d()
+    df, ph, sc = oracle.search1d(g_ctf, PX, case["p"])
+    assert r1.df_min == r1.df_max == pytest.approx(df, abs=0.01)
+    assert r1.score == pytest.approx(sc, abs=1e-4)
+    ctx.set_phase(0.0, 0.0)
+    r2 = ctx.refine1d(14000.0, 4000.0)
+    df2, ph2, sc2 = oracle.refine1d(g_ctf, PX, case["p"], 14000.0, 4000.0)
+    assert r2.df_min == pytest.approx(df2, abs=0.01)
+    assert r2.score == pytest.approx(sc2, abs=1e-4)
+
+
 def test_do2d_search_on_oracle_spectrum(case, oracle):
     # search alone: both sides on (nearly) the same spectrum
     r = case["ctx"].do2d()
@@ -202,3 +219,32 @@ def test_fused_batch_deterministic(gpu_lib):
     b = ctx.run_batch(imgs, [PX] * 3, op)
     for x, y in zip(a, b):
         assert x.as_dict() == y.as_dict()
+
+
+def _bg_curves(case):
+    x = np.arange(257, dtype=np.float64)
+    yield (1000 * np.exp(-x / 40) + 50 * np.cos(x / 3) ** 2 + 20).astype(np.float32)
+    yield case["ctx"].radial_average().astype(np.float32)
+    rng = np.random.default_rng(9)
+    yield (500 / (1 + x / 10) + rng.uniform(0, 30, 257)).astype(np.float32)
+    yield (2000 * np.exp(-np.arange(1025) / 150) + 5).astype(np.float32)
+
+
+def test_background1d_matches_oracle(case, oracle):
+    """GBackground1D: start and background bit-identical to the oracle
+    (same double fit order, same float window sums), Remove1D identical,
+    Remove2D to one float rounding (FMA in the interpolation)."""
+    ctx = case["ctx"]
+    for sp in _bg_curves(case):
+        bg, st = ctx.background1d(sp)
+        obg, ost = oracle.background1d(sp)
+        assert st == ost
+        assert np.array_equal(bg, obg)
+        r1 = ctx.remove_background1d(sp, bg, st)
+        assert np.array_equal(r1, oracle.remove_bg1d(sp, obg, ost))
+    half = case["ctx"].half_spectrum(raw=True)
+    sp = case["ctx"].radial_average().astype(np.float32)
+    bg, st = ctx.background1d(sp)
+    g2 = ctx.remove_background2d(half, bg, st)
+    o2 = oracle.remove_bg2d(half, bg, st)
+    assert np.allclose(g2, o2, rtol=1e-6, atol=1e-6 * np.abs(half).max())

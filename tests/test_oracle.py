@@ -217,3 +217,25 @@ def test_series_policy_refines_around_best(oracle):
     assert res[0].df_1d == 0 and res[2].df_1d == 0   # refined
     for r in res:
         assert abs(0.5 * (r.df_min + r.df_max) - 20000) < 400
+
+
+def test_background1d_known_answers(oracle):
+    # GBackground1D::mFindStart / DoIt (FindCTF/GBackground1D.cu:95-169):
+    # a spectrum above its fitted line until bin 30 starts there; the
+    # background is the centred moving average of width start/2*2-1.
+    n = 257
+    x = np.arange(n, dtype=np.float64)
+    sp = np.where(x < 30, 1000.0 - x, 100.0 - 0.1 * x).astype(np.float32)
+    bg, st = oracle.background1d(sp)
+    i0, i1 = n // 5, n - n // 5
+    xs = x[i0:i1]
+    a, b = np.polyfit(xs, sp[i0:i1].astype(np.float64), 1)
+    exp_start = next(i for i in range(2, n) if a * i + b >= sp[i])
+    assert st == exp_start
+    w = st // 2 * 2 - 1
+    for i in (st, st + 7, n - 3):
+        ks = [k if k < n else 2 * n - 1 - k for k in range(i - w // 2, i - w // 2 + w)]
+        assert abs(bg[i] - sp[ks].astype(np.float64).mean()) < 1e-3
+    assert np.all(bg[:st] == 0)
+    r = oracle.remove_bg1d(sp, bg, st)
+    assert np.all(r[:st] == 0) and np.allclose(r[st:], sp[st:] - bg[st:])

@@ -122,6 +122,31 @@ def test_single_micrograph_matches_reference(gpu_lib, ref, case):
     _close(res, [float(x) for x in R["result"]])
 
 
+@pytest.mark.parametrize("phase", [(0.0, 0.0), (30.0, 60.0)], ids=["no_phase", "phase_search"])
+def test_do1d_and_refine1d_match_reference(gpu_lib, ref, phase):
+    """CFindCtf1D::Do1D and Refine1D: same grid point as the reference (the
+    1D grids are float expressions evaluated identically), CC to 1e-4."""
+    G = gpu_lib
+    img = _img(2048, 2048, 1.35, (17000.0, 17400.0), 30.0, 701, phase=phase[0] + 5.0)
+    ctx = G.Context(0, 512, 0)
+    ctx.setup(G.make_optics(pixel_size=1.35, ext_phase_deg=phase[0], ext_phase_range=phase[1]),
+              2048, 2048)
+    ctx.gen_half_spectrum(img)
+    ctx.set_phase(*phase)
+    r1 = ctx.do1d()
+    ctx.set_phase(*phase)
+    r2 = ctx.refine1d(16000.0, 5000.0)
+    ctx.close()
+    d1, p1, c1 = ref.single1d(img, 1.35, ext_phase_deg=phase[0], ext_phase_range=phase[1])
+    d2, p2, c2 = ref.single1d(img, 1.35, ext_phase_deg=phase[0], ext_phase_range=phase[1],
+                              refine=(16000.0, 5000.0))
+    for r, (d, p, c) in ((r1, (d1, p1, c1)), (r2, (d2, p2, c2))):
+        assert r.df_min == r.df_max
+        assert abs(r.df_min - d) <= 10.0, (r, d, p, c)      # 10 A: the finest 1D step
+        assert abs(r.ext_phase - p) <= 1e-3 + (phase[1] / 36.0), (r, d, p, c)
+        assert abs(r.score - c) <= 1e-4, (r, d, p, c)
+
+
 def test_phase_plate_set_matches_reference(gpu_lib, ref):
     """Micrographs (not a tilt series) with extra-phase search: Do2D, then
     refines whose windows include the phase, each starting from a newly set
@@ -175,3 +200,29 @@ def test_ctf_file_matches_reference_writer(gpu_lib, ref, tmp_path):
     G.write_ctf_file(mine_txt, results, tilts=tilts, names=["ts.mrc"] * 3, is_tomo=True)
     assert open(mine_txt).read() == open(ref_txt).read()
     assert open(str(tmp_path / "mine_Imod.txt")).read() == open(str(tmp_path / "ref_Imod.txt")).read()
+
+
+def test_background1d_matches_reference(gpu_lib, ref):
+    """GBackground1D DoIt / Remove1D / Remove2D: start and background
+    bit-identical to the reference; the removals to one float rounding."""
+    G = gpu_lib
+    img = _img(1024, 1024, 1.35, (15000.0, 15400.0), 30.0, 801)
+    ctx = G.Context(0, 512, 0)
+    ctx.setup(G.make_optics(pixel_size=1.35), 1024, 1024)
+    ctx.gen_half_spectrum(img)
+    radial = ctx.radial_average().astype(np.float32)
+    half = ctx.half_spectrum(raw=True)
+    x = np.arange(513, dtype=np.float64)
+    curves = [radial, (1000 * np.exp(-x / 60) + 40 * np.cos(x / 4) ** 2 + 10).astype(np.float32)]
+    for sp in curves:
+        bg, st = ctx.background1d(sp)
+        rbg, rst, rhalf, r1 = ref.background1d(sp, half=half if len(sp) == 257 else None,
+                                               spec1d=sp)
+        assert st == rst
+        assert np.array_equal(bg, rbg)
+        m1 = ctx.remove_background1d(sp, bg, st)
+        assert np.allclose(m1, r1, rtol=1e-6, atol=1e-6 * np.abs(sp).max())
+        if rhalf is not None:
+            m2 = ctx.remove_background2d(half, bg, st)
+            assert np.allclose(m2, rhalf, rtol=1e-6, atol=1e-6 * np.abs(half).max())
+    ctx.close()
