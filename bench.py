@@ -149,7 +149,8 @@ def make_series(rank, n_tilts, size, device):
     specs = synth.tilt_series_specs(n_tilts=n_tilts, step_deg=3.0, size=size, pixel_size=PX,
                                     dose=3.0, df0=30000.0, seed=1 + rank)
     imgs = [synth.make_micrograph(s, device=device) for s in specs]
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     return specs, imgs
 
 
