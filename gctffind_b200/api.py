@@ -27,6 +27,7 @@ GCF_SPECT_CUFFT = 1
 # Every symbol include/gctf_b200.h declares.
 EXPORTS = [
     "gcf_create", "gcf_destroy", "gcf_strerror", "gcf_last_error", "gcf_set_spectrum_impl",
+    "gcf_set_fused_shape",
     "gcf_setup", "gcf_gen_half_spectrum", "gcf_set_phase", "gcf_do2d", "gcf_refine",
     "gcf_do1d", "gcf_refine1d",
     "gcf_get_spect_size", "gcf_get_half_spectrum", "gcf_gen_full_spectrum",
@@ -100,6 +101,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_last_error.argtypes = [vp]
     L.gcf_last_error.restype = C.c_char_p
     L.gcf_set_spectrum_impl.argtypes = [vp, i]
+    L.gcf_set_fused_shape.argtypes = [vp, i]
     L.gcf_setup.argtypes = [vp, C.POINTER(Optics), i, i]
     L.gcf_gen_half_spectrum.argtypes = [vp, vp, i, i]
     L.gcf_set_phase.argtypes = [vp, f, f]
@@ -215,6 +217,10 @@ class Context:
 
     def set_spectrum_impl(self, impl: int):
         _check(self.L.gcf_set_spectrum_impl(self._h, impl), self._h)
+
+    def set_fused_shape(self, shape: int):
+        """0 (auto), 8, 816 or 16: cluster shape of the fused tile kernel."""
+        _check(self.L.gcf_set_fused_shape(self._h, shape), self._h)
 
     # -- CFindCtf2D shape ------------------------------------------------------
     def setup(self, optics: Optics, width: int, height: int):

@@ -118,6 +118,7 @@ struct gcf_ctx {
     DBuf<double*> f_bsum_ptr;
     int fused_clusters = 0;
     int fused_shape = 0;
+    int fused_shape_req = 0;   // 0: pick by SM coverage
 
     // CFindCtf2D call-shape state
     gcf_optics optics{};
@@ -487,8 +488,9 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     }
     first[nm] = (int)items.size();
     if (ctx->fused_clusters <= 0) {
-        int n = 0, shape = 0;
-        CK(fused_max_clusters(&n, &shape));
+        int n = 0, shape = ctx->fused_shape_req;
+        if (shape) CK(fused_clusters_of(shape, &n));
+        else CK(fused_max_clusters(&n, &shape));
         if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
         ctx->fused_clusters = n;
         ctx->fused_shape = shape;
@@ -1122,6 +1124,14 @@ gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int w, int h, float px, i
                              nw * sizeof(float), nh, cudaMemcpyDeviceToHost, ctx->st));
     }
     CK(cudaStreamSynchronize(ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape)
+{
+    if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16)) return GCF_ERR_INVALID_ARG;
+    ctx->fused_shape_req = shape;
+    ctx->fused_clusters = 0;   // recomputed at the next launch
     return GCF_OK;
 }
 

@@ -41,7 +41,8 @@ namespace {
 
 constexpr int FT = 512;          // tile edge
 constexpr int FCX = FT / 2 + 1;  // 257 half-spectrum columns
-constexpr int FSCR = 16 * 33;    // per-warp scratch, float2 units
+constexpr int FSCR = 16 * 34;    // per-warp scratch, float2 units
+constexpr int FROW = 34;         // transpose row stride: 64-bit accesses of either side hit distinct banks
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
@@ -76,6 +77,11 @@ __device__ __forceinline__ float2 w16(int m)
     }
 }
 
+// Slot of spectrum bin K (0..511) in the warp scratch when a whole FFT
+// output is staged: bins 256..511 are shifted by 8 slots, so the 16-lane
+// halves of the (m + 16 k + 256 p) stores hit distinct banks.
+__device__ __forceinline__ int sslot(int K) { return K + ((K >> 8) << 3); }
+
 // Position of output k of dft16 in its register array.
 __host__ __device__ constexpr int P16(int k) { return (k & 3) * 4 + (k >> 2); }
 
@@ -95,7 +101,7 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 
 // 512-point forward FFT held by one warp.  In: lane l holds x[32 j + l] in
 // v[j].  Out: lane 2m+p holds X[m + 16 k + 256 p] in v[P16(k)].
-// scr: 528 float2 of warp-private shared memory; twl[k1 * 32 + l] =
+// scr: FSCR float2 of warp-private shared memory; twl[k1 * 32 + l] =
 // exp(-2 pi i l k1 / 512); tw32[k] = exp(-2 pi i k / 32).
 __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* twl,
                                             const float2* tw32, int lane)
@@ -105,11 +111,11 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
     for (int k1 = 1; k1 < 16; ++k1) v[P16(k1)] = cmul(v[P16(k1)], twl[k1 * 32 + lane]);
     __syncwarp();
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) scr[k1 * 33 + lane] = v[P16(k1)];
+    for (int k1 = 0; k1 < 16; ++k1) scr[k1 * FROW + lane] = v[P16(k1)];
     __syncwarp();
     const int m = lane >> 1, p = lane & 1;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = scr[m * 33 + 2 * q + p];
+    for (int q = 0; q < 16; ++q) v[q] = scr[m * FROW + 2 * q + p];
     dft16(v);
     const float sg = p ? -1.0f : 1.0f;
 #pragma unroll
@@ -140,7 +146,11 @@ struct FusedTab {
 // Sums of the stride x stride blocks that tile every image (tile = 2 stride,
 // so a tile is 2 x 2 blocks): one pass over the images gives every tile mean
 // of GCalcMoment2D (Util/GCalcMoment2D.cu:10-58) without a second read.
-__global__ void k_block_sums(const FusedTab* __restrict__ imgs, double* const* __restrict__ out)
+// Each warp sums whole block rows with 16-byte loads when the rows are
+// 16-byte aligned (4 independent FP64 partial sums per lane keep several
+// loads in flight); otherwise it falls back to 4-byte loads.
+__global__ void __launch_bounds__(256) k_block_sums(const FusedTab* __restrict__ imgs,
+                                                    double* const* __restrict__ out)
 {
     __shared__ double sh[32];
     const FusedTab im = imgs[blockIdx.y];
@@ -149,28 +159,46 @@ __global__ void k_block_sums(const FusedTab* __restrict__ imgs, double* const* _
     if (b >= im.nbx * nby) return;
     const int bx = b % im.nbx, by = b / im.nbx, S = im.stride;
     const float* src = im.img + (size_t)(im.offy + by * S) * im.pitch + im.offx + bx * S;
-    double s = 0.0;
-    for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
-        int y = k / S, x = k - y * S;
-        s += (double)__ldg(src + (size_t)y * im.pitch + x);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool v4 = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (im.pitch % 4 == 0) && (S % 4 == 0);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    if (v4) {
+        const int q = S / 4;   // float4 per block row
+        for (int y = warp; y < S; y += nw) {
+            const float4* row = reinterpret_cast<const float4*>(src + (size_t)y * im.pitch);
+            for (int x = lane; x < q; x += 32) {
+                float4 v = __ldg(row + x);
+                s0 += (double)v.x;
+                s1 += (double)v.y;
+                s2 += (double)v.z;
+                s3 += (double)v.w;
+            }
+        }
+    } else {
+        for (int y = warp; y < S; y += nw) {
+            const float* row = src + (size_t)y * im.pitch;
+            for (int x = lane; x < S; x += 32) s0 += (double)__ldg(row + x);
+        }
     }
+    double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    if (lane == 0) sh[warp] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        for (int w = 0; w < nw; ++w) t += sh[w];
         out[blockIdx.y][b] = t;
     }
 }
 
 // Compile-time shape of one cluster configuration.
-template <int CL_, int NW_, bool DB_>
+template <int CL_, int NW_, bool DB_, bool PF_ = true>
 struct FusedShape {
     static constexpr int CL = CL_;                   // CTAs per cluster
     static constexpr int NW = NW_;                   // warps per CTA
     static constexpr bool DB = DB_;                  // double-buffered column buffer
+    static constexpr bool PF = PF_;                  // register prefetch of the next row pair
     static constexpr int THR = NW * 32;
     static constexpr int R = FT / CL;                // tile rows per CTA
     static constexpr int C = FT / 2 / CL;            // frequency columns per CTA
@@ -185,8 +213,9 @@ struct FusedShape {
     static constexpr size_t SMEM = (DB ? 2 : 1) * BUF + SCR + TWL + TW32 + ACCN;
     static_assert(R % 32 == 0 && PW >= 1 && NR >= 1 && R / 2 == PW * NW && C == NR * NW && C <= 32, "shape");
 };
-using Shape16 = FusedShape<16, 16, true>;   // 16-CTA clusters, 512 threads
-using Shape8 = FusedShape<8, 8, false>;     // 8-CTA clusters, 256 threads
+using Shape16 = FusedShape<16, 16, true>;         // 16-CTA clusters, 512 threads
+using Shape8 = FusedShape<8, 8, false>;           // 8-CTA clusters, 256 threads
+using Shape8W16 = FusedShape<8, 16, false, false>;  // 8-CTA clusters, 512 threads, 128 registers
 
 template <class S>
 __global__ void __launch_bounds__(S::THR, 1)
@@ -237,8 +266,10 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
             if (!S::DB) cluster.sync();   // peers are done reading this CTA's column buffer
 
             // ---- row transforms: two rows per FFT, rows read straight from global ----
-            float na[16], nb[16];
-            {
+            // S::PF: the next row pair is loaded into registers while this one
+            // is transformed (for 8-warp CTAs, whose 255 registers allow it)
+            float na[S::PF ? 16 : 1], nb[S::PF ? 16 : 1];
+            if constexpr (S::PF) {
                 const float* ga = src + (size_t)(2 * warp) * im.pitch;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
@@ -251,17 +282,26 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                 const int pp = warp + q4 * NW;
                 const int y0 = 2 * pp, Y0 = r * R + y0;
                 float ca[16], cb[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    ca[j] = na[j];
-                    cb[j] = nb[j];
-                }
-                if (q4 + 1 < PW) {   // prefetch the next row pair
-                    const float* ga = src + (size_t)(2 * (pp + NW)) * im.pitch;
+                if constexpr (S::PF) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        na[j] = __ldg(ga + 32 * j + lane);
-                        nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                        ca[j] = na[j];
+                        cb[j] = nb[j];
+                    }
+                    if (q4 + 1 < PW) {   // prefetch the next row pair
+                        const float* ga = src + (size_t)(2 * (pp + NW)) * im.pitch;
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            na[j] = __ldg(ga + 32 * j + lane);
+                            nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                        }
+                    }
+                } else {
+                    const float* ga = src + (size_t)y0 * im.pitch;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        ca[j] = __ldg(ga + 32 * j + lane);
+                        cb[j] = __ldg(ga + im.pitch + 32 * j + lane);
                     }
                 }
                 float2 v[16];
@@ -273,18 +313,18 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                 }
                 fft512_warp(v, scr, twl, tw32, lane);
 #pragma unroll
-                for (int k = 0; k < 16; ++k) scr[m + 16 * k + 256 * p] = v[P16(k)];
+                for (int k = 0; k < 16; ++k) scr[sslot(m + 16 * k + 256 * p)] = v[P16(k)];
                 __syncwarp();
                 // split into the two rows' half spectra and push bin K of both rows
                 // into the shared memory of CTA K / C (column K % C, rows Y0, Y0 + 1)
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     const int K = lane + 32 * i;
-                    float2 zk = scr[K], zn = scr[(FT - K) & (FT - 1)];
+                    float2 zk = scr[sslot(K)], zn = scr[sslot((FT - K) & (FT - 1))];
                     float4 AB = make_float4(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y),
                                             0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
                     if (K == 0) {   // pack the real DC and Nyquist bins of both rows
-                        float2 zh = scr[FT / 2];
+                        float2 zh = scr[sslot(FT / 2)];
                         AB = make_float4(zk.x, zh.x, zk.y, zh.y);
                     }
                     float2* dst = cluster.map_shared_rank(colbuf, K / C) + (size_t)(K % C) * YS + Y0;
@@ -324,12 +364,12 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                     }
                 } else {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) scr[m + 16 * k + 256 * p] = v[P16(k)];
+                    for (int k = 0; k < 16; ++k) scr[sslot(m + 16 * k + 256 * p)] = v[P16(k)];
                     __syncwarp();
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         int Kk = m + 16 * k + 256 * p;
-                        float2 zk = v[P16(k)], zn = scr[(FT - Kk) & (FT - 1)];
+                        float2 zk = v[P16(k)], zn = scr[sslot((FT - Kk) & (FT - 1))];
                         float ax = 0.5f * (zk.x + zn.x), ay = 0.5f * (zk.y - zn.y);
                         float bx = 0.5f * (zk.y + zn.y), by = -0.5f * (zk.x - zn.x);
                         acc[rho][k] += sqrtf(ax * ax + ay * ay);
@@ -442,6 +482,19 @@ cudaError_t fused_max_clusters(int* n, int* shape)
     return cudaSuccess;
 }
 
+// Co-resident clusters of one shape: 8 (8 CTAs x 8 warps), 816 (8 CTAs x 16
+// warps, 128 registers), 16 (16 CTAs x 16 warps, double buffered).
+cudaError_t fused_clusters_of(int shape, int* n)
+{
+    *n = 0;
+    switch (shape) {
+    case 8: return max_clusters<Shape8>(n);
+    case 816: return max_clusters<Shape8W16>(n);
+    case 16: return max_clusters<Shape16>(n);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 // Host launcher.  descs/items/first/inv are device arrays prepared by the caller.
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
                          int nitems, const int* first, const float* inv, int nimg, const float* taper,
@@ -459,6 +512,11 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
         cudaLaunchConfig_t cfg = fused_cfg<Shape16>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16>, reinterpret_cast<const FusedTab*>(descs), items,
                                nitems, taper, tw, partial);
+    } else if (shape == 816) {
+        if ((e = prepare_kernel<Shape8W16>()) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = fused_cfg<Shape8W16>(nclusters, st, attr);
+        e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape8W16>, reinterpret_cast<const FusedTab*>(descs),
+                               items, nitems, taper, tw, partial);
     } else {
         if ((e = prepare_kernel<Shape8>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape8>(nclusters, st, attr);

@@ -135,6 +135,7 @@ struct FusedImageDesc {          // layout must match FusedTab in gcf_fused.cu
 };
 int fused_tile_supported(int tile);
 cudaError_t fused_max_clusters(int* n, int* shape);
+cudaError_t fused_clusters_of(int shape, int* n);   // shape 8, 816 or 16
 // items: (image, first tile, end tile, item index); first[img]..first[img+1]
 // are the items of image img; inv[img] = 1 / tiles of img.
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,

@@ -79,6 +79,10 @@ const char* gcf_strerror(gcf_status s);
 /* Last error detail of this context (CUDA/cuFFT message), never NULL. */
 const char* gcf_last_error(gcf_ctx* ctx);
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
+/* Cluster shape of the fused tile kernel: 0 = the shape that keeps the most
+ * SMs busy (default), 8 = 8 CTAs x 8 warps, 816 = 8 CTAs x 16 warps,
+ * 16 = 16 CTAs x 16 warps.  For tuning; results do not depend on it. */
+gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape);
 
 /* ---------------------------------------------------------------------- */
 /* CFindCtf2D call shape (FindCTF/CFindCTFInc.h:541-623)                    */
