@@ -452,7 +452,18 @@ gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
 gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float* raw_out)
 {
     const int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
-    const int kItemTiles = 64;
+    if (ctx->fused_clusters <= 0) {
+        int n = 0, shape = ctx->fused_shape_req;
+        if (shape) CK(fused_clusters_of(shape, &n));
+        else CK(fused_max_clusters(&n, &shape));
+        if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
+        ctx->fused_clusters = n;
+        ctx->fused_shape = shape;
+    }
+    // Work items: each micrograph's tiles in runs of at most 32 (every item's
+    // |F| sums live in registers until it ends).  The split depends on the
+    // micrograph alone, so its spectrum does not depend on the batch it is in.
+    const int kItemTiles = 32;
     std::vector<FusedImageDesc> d(nm);
     std::vector<int4> items;
     std::vector<int> first(nm + 1);
@@ -487,14 +498,6 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
             items.push_back(make_int4(i, t0, std::min(nt, t0 + chunk), (int)items.size()));
     }
     first[nm] = (int)items.size();
-    if (ctx->fused_clusters <= 0) {
-        int n = 0, shape = ctx->fused_shape_req;
-        if (shape) CK(fused_clusters_of(shape, &n));
-        else CK(fused_max_clusters(&n, &shape));
-        if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
-        ctx->fused_clusters = n;
-        ctx->fused_shape = shape;
-    }
     int ni = (int)items.size();
     CK(ctx->f_bsum.ensure(nblk));
     CK(ctx->f_bsum_ptr.ensure(nm));
@@ -560,22 +563,24 @@ gcf_status spectra_chunk(gcf_ctx* ctx, const std::vector<MicImage>& mics, int fi
 }
 
 // CFindCtfBase::mRemoveBackground/mLowpass and CFindCtf1D::mCalcRadialAverage
-// for slots 0..nm-1.
-gcf_status spectra_post(gcf_ctx* ctx, int nm)
+// for slots first .. first + nm - 1.
+gcf_status spectra_post(gcf_ctx* ctx, int nm, int first = 0)
 {
     int T = ctx->tile, cx = T / 2 + 1;
     size_t cmp_n = (size_t)cx * T;
-    launch_bg_horizontal(ctx->raw.p, T, nm, ctx->log_spect, ctx->hsum.p, ctx->st);
+    if (nm <= 0) return GCF_OK;
+    const size_t o = (size_t)first * cmp_n;
+    launch_bg_horizontal(ctx->raw.p + o, T, nm, ctx->log_spect, ctx->hsum.p + o, ctx->st);
     CKL();
-    launch_bg_vertical(ctx->raw.p, ctx->hsum.p, T, nm, ctx->log_spect, ctx->ctf0.p, ctx->st);
+    launch_bg_vertical(ctx->raw.p + o, ctx->hsum.p + o, T, nm, ctx->log_spect, ctx->ctf0.p + o, ctx->st);
     CKL();
-    launch_moments(ctx->ctf0.p, (int)cmp_n, nm, ctx->moments.p, ctx->st);
+    launch_moments(ctx->ctf0.p + o, (int)cmp_n, nm, ctx->moments.p + 2 * (size_t)first, ctx->st);
     CKL();
     // CFindCtfBase::mLowpass (FindCTF/CFindCtfBase.cpp:191-219): full
     // spectrum, R2C, B-factor 10 (normalised), C2R, half back.
     CK(ctx->lpfull.ensure((size_t)nm * T * T));
     CK(ctx->lpcmp.ensure((size_t)nm * cx * T));
-    launch_lp_full(ctx->ctf0.p, T, nm, ctx->lpfull.p, ctx->st);
+    launch_lp_full(ctx->ctf0.p + o, T, nm, ctx->lpfull.p, ctx->st);
     CKL();
     cufftHandle pf, pi;
     CKS(get_plan(ctx, 3, T, nm, &pf));
@@ -586,9 +591,11 @@ gcf_status spectra_post(gcf_ctx* ctx, int nm)
     CKL();
     if (cufftExecC2R(pi, (cufftComplex*)ctx->lpcmp.p, ctx->lpfull.p) != CUFFT_SUCCESS)
         return fail(ctx, GCF_ERR_CUFFT, "cufftExecC2R (lowpass) failed");
-    launch_lp_extract(ctx->ctf0.p, ctx->lpfull.p, T, nm, ctx->moments.p, ctx->ctf.p, ctx->lowpassed.p, ctx->st);
+    launch_lp_extract(ctx->ctf0.p + o, ctx->lpfull.p, T, nm, ctx->moments.p + 2 * (size_t)first,
+                      ctx->ctf.p + o, ctx->lowpassed.p + first, ctx->st);
     CKL();
-    launch_radial(ctx->ctf.p, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p, ctx->st);
+    launch_radial(ctx->ctf.p + o, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p + (size_t)first * cx,
+                  ctx->st);
     CKL();
     ctx->launches += 7;
     return GCF_OK;
@@ -1367,43 +1374,29 @@ gcf_status gcf_gen_full_spectrum(gcf_ctx* ctx, const gcf_result* res, float* hos
     return full_spectra(ctx, {0}, {*res}, {ctx->optics.pixel_size}, ctx->optics, host_out);
 }
 
-gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w, int h,
-                          int on_device, const gcf_optics* optics, const int* order, int is_tomo,
-                          gcf_result* results, float* full_out)
-{
-    if (!ctx || !images || n <= 0 || w <= 0 || h <= 0 || !valid_optics(optics) || !order ||
-        !results)
-        return GCF_ERR_INVALID_ARG;
-    std::vector<int> seen(n, 0);
-    for (int k = 0; k < n; ++k) {
-        if (order[k] < 0 || order[k] >= n || seen[order[k]]) return GCF_ERR_INVALID_ARG;
-        seen[order[k]] = 1;
-    }
-    for (int i = 0; i < n; ++i)
-        if (!images[i]) return GCF_ERR_INVALID_ARG;
-    CKS(set_device(ctx));
-    for (float& t : ctx->stage_ms) t = 0.0f;
-    ctx->kev_used = 0;
-    ctx->launches = 0;
-    cudaEvent_t t0, t1;
-    CK(cudaEventCreate(&t0));
-    CK(cudaEventCreate(&t1));
-    CK(cudaEventRecord(t0, ctx->st));
-    std::vector<int> ws(n, w), hs(n, h);
-    std::vector<float> pxs(n, optics->pixel_size);
-    std::vector<MicImage> mics;
-    gcf_status st = prepare_images(ctx, images, ws.data(), hs.data(), pxs.data(), n, on_device, mics);
-    if (st != GCF_OK) {
-        cudaEventDestroy(t0);
-        cudaEventDestroy(t1);
-        return st;
-    }
-    float pxn = mics[0].px_n;
-    const gcf_optics op = *optics;
-    auto full_job = [&](int idx) {
+namespace {
+
+// The CFindSeriesCtfs package loop (CFindSeriesCtfs.cpp:50-213) over slots
+// in processing order: slot 0 gets the full search, every later slot is
+// refined around the best-scoring earlier one, a refine with score <= 0
+// falls back to the full search.  Refines are issued speculatively as one
+// batch over a range of slots around the current best; when the best
+// changes, the rest of the range is re-run around the new one, so the
+// results equal the sequential loop.
+struct SeriesLoop {
+    gcf_ctx* ctx;
+    gcf_optics op;
+    float pxn;
+    int is_tomo;
+    std::vector<gcf_result> res;
+    std::vector<int> ref_used;   // slot whose result seeded this slot's refine
+    int cur_ref = -1;
+
+    JobSpec full_job(int slot) const
+    {
         JobSpec s;
         std::memset(&s, 0, sizeof(s));
-        s.mic = idx;
+        s.mic = slot;
         s.mode = 0;
         s.optics = op;
         s.px_n = pxn;
@@ -1411,12 +1404,14 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
         s.phase_deg = op.ext_phase_deg;
         s.phase_range = fmaxf(op.ext_phase_range, 0.0f);
         return s;
-    };
-    auto refine_job = [&](int idx, const gcf_result& rp) {
+    }
+
+    JobSpec refine_job(int slot, const gcf_result& rp) const
+    {
         // CFindSeriesCtfs::mProcessRefine (CFindSeriesCtfs.cpp:168-199)
         JobSpec s;
         std::memset(&s, 0, sizeof(s));
-        s.mic = idx;
+        s.mic = slot;
         s.mode = 1;
         s.optics = op;
         s.px_n = pxn;
@@ -1434,48 +1429,46 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
             if (op.ext_phase_range > 0) s.rin[7] = 40.0f;
         }
         return s;
-    };
-    std::vector<gcf_result> res(n);
-    std::vector<int> ref_used(n, -1);   // ref image whose result seeded this refine
-    std::vector<gcf_result> r;
-    // package 0 of the processing order: full search
-    st = run_search(ctx, {full_job(order[0])}, r);
-    if (st != GCF_OK) goto done;
-    res[order[0]] = r[0];
+    }
+
+    // Packages k0 .. k1-1, whose spectra are ready.
+    gcf_status run(int k0, int k1)
     {
-        int cur_ref = order[0];
-        int k = 1;
+        std::vector<gcf_result> r;
+        int k = k0;
+        if (k == 0 && k < k1) {
+            CKS(run_search(ctx, {full_job(0)}, r));
+            res[0] = r[0];
+            cur_ref = 0;
+            ++k;
+        }
         bool batch_valid = false;
-        while (k < n) {
+        while (k < k1) {
             if (!batch_valid) {
-                // speculative batch: refine every remaining package around cur_ref
                 std::vector<JobSpec> js;
-                for (int q = k; q < n; ++q) js.push_back(refine_job(order[q], res[cur_ref]));
-                st = run_search(ctx, js, r);
-                if (st != GCF_OK) goto done;
-                for (int q = k; q < n; ++q) {
-                    res[order[q]] = r[q - k];
-                    ref_used[order[q]] = cur_ref;
+                for (int q = k; q < k1; ++q) js.push_back(refine_job(q, res[cur_ref]));
+                CKS(run_search(ctx, js, r));
+                for (int q = k; q < k1; ++q) {
+                    res[q] = r[q - k];
+                    ref_used[q] = cur_ref;
                 }
                 batch_valid = true;
             }
-            int idx = order[k];
-            if (ref_used[idx] != cur_ref) {
+            if (ref_used[k] != cur_ref) {
                 batch_valid = false;
                 continue;
             }
             // mProcessPackage / mProcessRefine ref update (CFindSeriesCtfs.cpp:133-146, :200-203)
             int new_ref = cur_ref;
-            if (res[cur_ref].score < res[idx].score) new_ref = idx;
-            if (res[idx].score <= 0) {
+            if (res[cur_ref].score < res[k].score) new_ref = k;
+            if (res[k].score <= 0) {
                 // same CFindCtf2D object as the refine: its search starts at
                 // the phase the refine ended with
-                JobSpec fj = full_job(idx);
-                fj.held_phase = res[idx].ext_phase;
-                st = run_search(ctx, {fj}, r);
-                if (st != GCF_OK) goto done;
-                res[idx] = r[0];
-                new_ref = idx;
+                JobSpec fj = full_job(k);
+                fj.held_phase = res[k].ext_phase;
+                CKS(run_search(ctx, {fj}, r));
+                res[k] = r[0];
+                new_ref = k;
             }
             if (new_ref != cur_ref) {
                 cur_ref = new_ref;
@@ -1483,16 +1476,123 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
             }
             ++k;
         }
+        return GCF_OK;
     }
-    if (full_out) {
+};
+
+// Host images: uploads in processing order on the copy stream (the first
+// package alone, then chunks of 8), and after each chunk its spectra,
+// post-processing and package searches, so only the last chunk's work
+// follows the last copy.
+gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, int w, int h,
+                           float px, std::vector<MicImage>& mics, SeriesLoop& loop)
+{
+    const int n = (int)imgs.size();
+    mics.assign(n, MicImage{});
+    int nw, nh;
+    float pn;
+    gcf_rescale_dims(w, h, px, &nw, &nh, &pn);
+    const bool rescaled = (1.2f / px) > 1;
+    CKS(spectra_alloc(ctx, n));
+    if (rescaled) CK(ctx->rescaled.ensure((size_t)nw * nh * n));
+    CK(ctx->images.ensure((size_t)w * h * n));
+    // chunks: the first package alone (its full search starts early), then
+    // 8 packages, shrinking towards the end so little work follows the last copy
+    std::vector<int> bounds{0};
+    for (int b = 1; b < n;) {
+        bounds.push_back(b);
+        int rem = n - b;
+        b += rem > 12 ? 8 : rem > 6 ? 4 : rem > 2 ? 2 : 1;
+    }
+    bounds.push_back(n);
+    const int nchunks = (int)bounds.size() - 1;
+    while ((int)ctx->chunk_ev.size() < nchunks) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->chunk_ev.push_back(e);
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st_copy, ctx->ev[0], 0));
+    const size_t cnt = (size_t)w * h;
+    for (int c = 0; c < nchunks; ++c) {
+        for (int k = bounds[c]; k < bounds[c + 1]; ++k)
+            CK(cudaMemcpyAsync(ctx->images.p + cnt * k, imgs[k], cnt * sizeof(float), cudaMemcpyHostToDevice,
+                               ctx->st_copy));
+        CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st_copy));
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->st_copy));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    for (int c = 0; c < nchunks; ++c) {
+        const int k0 = bounds[c], k1 = bounds[c + 1];
+        CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
+        for (int k = k0; k < k1; ++k) {
+            size_t used = 0;
+            float* dst = rescaled ? ctx->rescaled.p + (size_t)nw * nh * k : nullptr;
+            CKS(stage_image(ctx, ctx->images.p + cnt * k, w, h, px, dst, mics[k], &used));
+        }
+        CKS(spectra_chunk(ctx, mics, k0, k1 - k0));
+        CKS(spectra_post(ctx, k1 - k0, k0));
+        CKS(loop.run(k0, k1));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    return GCF_OK;
+}
+
+}  // namespace
+
+gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w, int h,
+                          int on_device, const gcf_optics* optics, const int* order, int is_tomo,
+                          gcf_result* results, float* full_out)
+{
+    if (!ctx || !images || n <= 0 || w <= 0 || h <= 0 || !valid_optics(optics) || !order ||
+        !results)
+        return GCF_ERR_INVALID_ARG;
+    std::vector<int> seen(n, 0), pos(n);
+    for (int k = 0; k < n; ++k) {
+        if (order[k] < 0 || order[k] >= n || seen[order[k]]) return GCF_ERR_INVALID_ARG;
+        seen[order[k]] = 1;
+        pos[order[k]] = k;
+    }
+    for (int i = 0; i < n; ++i)
+        if (!images[i]) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    for (float& t : ctx->stage_ms) t = 0.0f;
+    ctx->kev_used = 0;
+    ctx->launches = 0;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, ctx->st));
+    // slot k holds package k of the processing order (image order[k])
+    std::vector<const float*> imgs(n);
+    for (int k = 0; k < n; ++k) imgs[k] = images[order[k]];
+    int nw, nh;
+    float pxn;
+    gcf_rescale_dims(w, h, optics->pixel_size, &nw, &nh, &pxn);
+    SeriesLoop loop{ctx, *optics, pxn, is_tomo, std::vector<gcf_result>(n), std::vector<int>(n, -1)};
+    std::vector<MicImage> mics;
+    gcf_status st;
+    if (on_device) {
+        std::vector<int> ws(n, w), hs(n, h);
+        std::vector<float> pxs(n, optics->pixel_size);
+        st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, 1, mics);
+        if (st == GCF_OK) st = loop.run(0, n);
+    } else {
+        st = series_streamed(ctx, imgs, w, h, optics->pixel_size, mics, loop);
+    }
+    if (st == GCF_OK && full_out) {
         std::vector<int> mi(n);
+        std::vector<gcf_result> ri(n);
         std::vector<float> pv(n, pxn);
-        for (int i = 0; i < n; ++i) mi[i] = i;
-        st = full_spectra(ctx, mi, res, pv, op, full_out);
-        if (st != GCF_OK) goto done;
+        for (int i = 0; i < n; ++i) {
+            mi[i] = pos[i];
+            ri[i] = loop.res[pos[i]];
+        }
+        st = full_spectra(ctx, mi, ri, pv, *optics, full_out);
     }
-    for (int i = 0; i < n; ++i) results[i] = res[i];
-done:
+    if (st == GCF_OK)
+        for (int i = 0; i < n; ++i) results[i] = loop.res[pos[i]];
     cudaEventRecord(t1, ctx->st);
     cudaEventSynchronize(t1);
     accumulate_stage_times(ctx);

@@ -92,11 +92,18 @@ CASES = [
     (1024, 896, 1.5, (20000.0, 20500.0), 75.0, 103, 0.0, 256, 1, 0.0, 0.0, None),
     (1024, 1024, 1.35, (18000.0, 18400.0), 10.0, 104, 0.0, 512, 0, 0.0, 0.0,
      [18300.0, 9000.0, 0.011, 0.04, 12.0, 30.0, 0.0, 0.0]),
+    # tile 1024 (batched-cuFFT spectrum), rescaled from 1.0 A/px
+    (3072, 3072, 1.0, (30000.0, 30600.0), -35.0, 108, 0.0, 1024, 0, 0.0, 0.0, None),
+    # odd raw sizes, rescale by 1.5 (0.8 A/px), tile 256, log spectrum
+    (1501, 1101, 0.8, (12000.0, 12300.0), 5.0, 109, 0.0, 256, 1, 0.0, 0.0, None),
+    # odd raw width without rescale: the last column is dropped (new size even)
+    (1023, 777, 1.5, (26000.0, 26600.0), 60.0, 110, 0.0, 256, 0, 0.0, 0.0, None),
 ]
 
 
 @pytest.mark.parametrize("case", CASES, ids=["px1.0_t512", "px1.35_t512", "phase_t512", "log_t256",
-                                             "refine_t512"])
+                                             "refine_t512", "px1.0_t1024", "odd_rescale_log_t256",
+                                             "odd_width_t256"])
 def test_single_micrograph_matches_reference(gpu_lib, ref, case):
     w, h, px, df, az, seed, phase_truth, tile, log, ph0, phr, refine = case
     img = _img(w, h, px, df, az, seed, phase=phase_truth)
@@ -117,9 +124,15 @@ def test_single_micrograph_matches_reference(gpu_lib, ref, case):
     fm[:9, :] = fm[-8:, :] = False
     fm[:, :9] = fm[:, -8:] = False
     fm[:, tile // 2 - 8: tile // 2 + 9] = False
+    ref_res = [float(x) for x in R["result"]]
+    if max(abs(a - b) for a, b in zip(res, ref_res)) > 0.01:
+        # a neighbouring candidate won a CC tie (float vs FP64 sums): the
+        # fitted CTF drawn into the left half differs, so compare the
+        # spectrum half only
+        fm[:, : tile // 2 + 9] = False
     F = R["full"].astype(np.float64)
     assert np.abs(full - F)[fm].max() <= 5e-3 * np.sqrt((F * F).mean())
-    _close(res, [float(x) for x in R["result"]])
+    _close(res, ref_res)
 
 
 @pytest.mark.parametrize("phase", [(0.0, 0.0), (30.0, 60.0)], ids=["no_phase", "phase_search"])
@@ -226,3 +239,20 @@ def test_background1d_matches_reference(gpu_lib, ref):
             m2 = ctx.remove_background2d(half, bg, st)
             assert np.allclose(m2, rhalf, rtol=1e-6, atol=1e-6 * np.abs(half).max())
     ctx.close()
+
+
+def test_flat_spectrum_skips_lowpass_like_reference(gpu_lib, ref):
+    """CFindCtfBase::mRemoveBackground skips the lowpass when the background-
+    removed spectrum's variance is below 1 (FindCTF/CFindCtfBase.cpp:170-175):
+    a faint image (x 1e-4) goes down that branch in both implementations."""
+    G = gpu_lib
+    img = _img(1024, 1024, 1.35, (16000.0, 16500.0), 20.0, 111) * np.float32(1e-4)
+    R = ref.single(img, 1.35, tile=512)
+    resc, raw, ctf, full, res = _mine_single(G, img, 1.35, 512)
+    C = R["ctf_half"].astype(np.float64)
+    assert np.abs(ctf - C).max() <= 1e-4 * np.sqrt((C * C).mean())
+    ctx = G.Context(0, 512, 0)
+    r = ctx.run_series([img], G.make_optics(pixel_size=1.35), [0], is_tomo=False)[0]
+    ctx.close()
+    assert r.lowpassed == 0
+    _close(res, [float(x) for x in R["result"]])
