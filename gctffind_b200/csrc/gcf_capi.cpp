@@ -103,6 +103,7 @@ struct gcf_ctx {
     DBuf<float4> cand;
     DBuf<float2> cval;
     DBuf<double2> part;
+    DBuf<int> arrive;
     DBuf<gcf_result> d_res;
     DBuf<PixOptics> d_optics;
 
@@ -705,6 +706,8 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     CK(ctx->part.ensure((size_t)nj * kMaxCand * max_chunks));
     CK(ctx->cc_res.ensure((size_t)nj * cx));
     CK(ctx->d_res.ensure(nj));
+    CK(ctx->arrive.ensure(nj));
+    CK(cudaMemsetAsync(ctx->arrive.p, 0, nj * sizeof(int), ctx->st));
     CK(cudaMemcpyAsync(ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), cudaMemcpyHostToDevice,
                        ctx->st));
     CK(cudaMemcpyAsync(ctx->spec_off.p, soff.data(), nj * sizeof(int), cudaMemcpyHostToDevice,
@@ -722,6 +725,7 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     a.cand = ctx->cand.p;
     a.cval = ctx->cval.p;
     a.part = ctx->part.p;
+    a.arrive = ctx->arrive.p;
     a.max_chunks = max_chunks;
     a.njobs = nj;
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
@@ -742,9 +746,7 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         int cb = (k == 0) ? 1 : (k == 1 && any_grid) ? (kMaxCand / kEvalCB + 3) / 4 : 4;
         launch_eval2d(a, cb, max_band, ctx->st);
         CKL();
-        launch_update2d(a, ctx->st);
-        CKL();
-        ctx->launches += 2;
+        ctx->launches += 1;
     }
     if (any_2d) {
         // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)

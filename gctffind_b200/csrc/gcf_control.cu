@@ -5,18 +5,21 @@
 // Here the whole control flow lives on the GPU:
 //   k_search1d : radial average -> 1D brute force -> 1D refine -> 2D init,
 //                one CTA per Do2D job (CFindCtf1D::Do1D, FindCTF/CFindCtf1D.cpp:49-111);
-//   k_update2d : reduce the candidate partial sums of the pending line
-//                search, take the first strict maximum, advance the
+//   k_eval2d   : one step of every job's line search: all pending candidates
+//                against all band pixels, then (last block of each job)
+//                reduce, take the first strict maximum, advance the
 //                CFindDefocus2D::mIterate state machine and write the next
-//                candidate set, one CTA per job.
-// The host only enqueues (eval, update) pairs; no value comes back until
-// the search is over.
+//                candidate set.
+// The host only enqueues k_eval2d launches; no value comes back until the
+// search is over.
 //
 // Compiled with -fmad=false: every float step/range expression is rounded
 // operation by operation like the reference's host code, so candidate grids
 // coincide with the reference and with the oracle.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 
 #include "gcf_internal.h"
 
@@ -317,34 +320,22 @@ __device__ void write_candidates(const SearchJob& J, int n, float4* cand, float2
 }
 
 // ---------------------------------------------------------------------------
-__global__ void k_update2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands,
+// One block finishes job j's pending line search: reduce the candidates'
+// partial sums in chunk order, take the first strict maximum, advance the
+// CFindDefocus2D::mIterate state machine and write the next candidates.
+__device__ void update_job(int j, SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands,
                            const double* __restrict__ sum_ss, float4* __restrict__ cand,
-                           float2* __restrict__ cval, const double2* __restrict__ part,
-                           int max_chunks, int init)
+                           float2* __restrict__ cval, const double2* __restrict__ part, int max_chunks)
 {
     __shared__ SearchJob sJ;
     __shared__ ArgMax shm[32];
     __shared__ float s_cc0;
     __shared__ int s_n;
-    const int j = blockIdx.x;
     if (threadIdx.x == 0) sJ = jobs[j];
     __syncthreads();
+    if (sJ.step == STEP_DONE) return;
     float4* cj = cand + (size_t)j * kMaxCand;
     float2* vj = cval + (size_t)j * kMaxCand;
-    if (init) {
-        if (sJ.mode >= 2) return;   // 1D-only job, finished by k_search1d
-        // fresh job: pending step is CC0 with one candidate
-        if (threadIdx.x == 0) {
-            sJ.step = STEP_CC0;
-            s_n = advance(sJ, vj);
-            sJ.ncand = s_n;
-            jobs[j] = sJ;
-        }
-        __syncthreads();
-        write_candidates(sJ, s_n, cj, vj);
-        return;
-    }
-    if (sJ.step == STEP_DONE) return;
     const int n = sJ.ncand;
     const BandDev b = bands[sJ.band];
     const int nch = (b.n + kEvalChunk - 1) / kEvalChunk;
@@ -373,6 +364,156 @@ __global__ void k_update2d(SearchJob* __restrict__ jobs, const BandDev* __restri
     }
     __syncthreads();
     write_candidates(sJ, s_n, cj, vj);
+}
+
+// Fresh jobs: the pending step is CC0 with one candidate (Do2D jobs were
+// set up by k_search1d; 1D-only jobs have nothing to search).
+__global__ void k_init_jobs(SearchJob* __restrict__ jobs, float4* __restrict__ cand, float2* __restrict__ cval)
+{
+    __shared__ SearchJob sJ;
+    __shared__ int s_n;
+    const int j = blockIdx.x;
+    if (threadIdx.x == 0) sJ = jobs[j];
+    __syncthreads();
+    if (sJ.mode >= 2) return;
+    float4* cj = cand + (size_t)j * kMaxCand;
+    float2* vj = cval + (size_t)j * kMaxCand;
+    if (threadIdx.x == 0) {
+        sJ.step = STEP_CC0;
+        s_n = advance(sJ, vj);
+        sJ.ncand = s_n;
+        jobs[j] = sJ;
+    }
+    __syncthreads();
+    write_candidates(sJ, s_n, cj, vj);
+}
+
+// ---------------------------------------------------------------------------
+// Candidate x band-pixel correlation (GCalcCTF2D + GCC2D fused,
+// FindCTF/GCalcCTF2D.cu:15-38, FindCTF/GCC2D.cu:13-170).
+//
+// For every job the pending line search holds up to kMaxCand candidates,
+// each reduced to four numbers
+//   q = (mean defocus [px], sigma*cos(2 alpha), sigma*sin(2 alpha), phase/pi)
+// and every in-band pixel to five
+//   a = wl*s^2, d = -0.5*wl^3*s^4*Cs, env = exp(-16 s^2), cos(2 theta), sin(2 theta)
+// so that the model at one (candidate, pixel) pair is
+//   t   = a * (mean + sigma*cos(2(theta - alpha))) + d + phase/pi   (= chi/pi)
+//   C   = (|sin(pi * (t - rint(t)))| - 1/2) * env
+// and the kernel accumulates sum(C*S) and sum(C*C); sum(S*S) is per job.
+// The argument of the fast sine stays within [-pi/2, pi/2].
+//
+// Grid: x = band chunk (kEvalChunk pixels), y = candidate block (kEvalCB
+// candidates, strided), z = job.  Pixel data stay in registers; candidate
+// parameters come from shared memory; partial sums leave as FP64, one slot
+// per (candidate, chunk).  The last block of a job to finish (an arrival
+// counter, no waiting) runs update_job for it, so one launch is one step of
+// every job's search.  No expression here is contracted differently by
+// -fmad=false: every multiply-add is an explicit fmaf.
+__global__ void __launch_bounds__(kEvalThreads)
+k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const float* __restrict__ band_spec,
+         const int* __restrict__ spec_off, const double* __restrict__ sum_ss, float4* __restrict__ cand,
+         float2* __restrict__ cval, double2* __restrict__ part, int max_chunks, int* __restrict__ arrive)
+{
+    __shared__ float4 sq[kEvalCB];
+    __shared__ float red[kEvalThreads / 32][2 * kEvalCB];
+    __shared__ int s_last;
+    const int j = blockIdx.z;
+    const int ncand = jobs[j].ncand;
+    const int cand_blocks = (ncand + kEvalCB - 1) / kEvalCB;
+    if ((int)blockIdx.y >= cand_blocks) return;
+    const BandDev b = bands[jobs[j].band];
+    const int nchunk = (b.n + kEvalChunk - 1) / kEvalChunk;
+    const int p0 = blockIdx.x * kEvalChunk;
+    if ((int)blockIdx.x >= max(nchunk, 1)) return;
+    const float* S = band_spec + spec_off[j];
+    float pa[kEvalPPT], pd[kEvalPPT], pe[kEvalPPT], pc[kEvalPPT], ps[kEvalPPT], pv[kEvalPPT];
+#pragma unroll
+    for (int k = 0; k < kEvalPPT; ++k) {
+        int p = p0 + k * kEvalThreads + threadIdx.x;
+        if (p < b.n) {
+            pa[k] = __ldg(b.a + p);
+            pd[k] = __ldg(b.d + p);
+            pe[k] = __ldg(b.env + p);
+            pc[k] = __ldg(b.c2t + p);
+            ps[k] = __ldg(b.s2t + p);
+            pv[k] = __ldg(S + p);
+        } else {
+            pa[k] = 0.f;
+            pd[k] = 0.f;
+            pe[k] = 0.f;
+            pc[k] = 0.f;
+            ps[k] = 0.f;
+            pv[k] = 0.f;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // candidate blocks y, y + gridDim.y, ... so any candidate count is covered
+    for (int c0 = blockIdx.y * kEvalCB; c0 < ncand && nchunk > 0; c0 += gridDim.y * kEvalCB) {
+        __syncthreads();
+        if (threadIdx.x < kEvalCB) {
+            int c = c0 + threadIdx.x;
+            sq[threadIdx.x] =
+                c < ncand ? cand[(size_t)j * kMaxCand + c] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+        float acs[kEvalCB], acc[kEvalCB];
+#pragma unroll
+        for (int c = 0; c < kEvalCB; ++c) {
+            const float4 q = sq[c];
+            float s_cs = 0.f, s_cc = 0.f;
+#pragma unroll
+            for (int k = 0; k < kEvalPPT; ++k) {
+                float df = fmaf(ps[k], q.z, fmaf(pc[k], q.y, q.x));
+                float t = fmaf(pa[k], df, pd[k]) + q.w;
+                float r = t - rintf(t);
+                float sv = __sinf(r * 3.14159265358979f);
+                float C = (fabsf(sv) - 0.5f) * pe[k];
+                s_cs = fmaf(C, pv[k], s_cs);
+                s_cc = fmaf(C, C, s_cc);
+            }
+            acs[c] = s_cs;
+            acc[c] = s_cc;
+        }
+#pragma unroll
+        for (int c = 0; c < kEvalCB; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                acs[c] += __shfl_xor_sync(0xffffffffu, acs[c], o);
+                acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+            }
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < kEvalCB; ++c) {
+                red[warp][2 * c] = acs[c];
+                red[warp][2 * c + 1] = acc[c];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < kEvalCB) {
+            int c = c0 + threadIdx.x;
+            if (c < ncand) {
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int w = 0; w < kEvalThreads / 32; ++w) {
+                    s1 += (double)red[w][2 * threadIdx.x];
+                    s2 += (double)red[w][2 * threadIdx.x + 1];
+                }
+                part[((size_t)j * kMaxCand + c) * max_chunks + blockIdx.x] = make_double2(s1, s2);
+            }
+        }
+    }
+    // arrival: the last working block of job j finishes its step
+    const int expected = max(nchunk, 1) * min((int)gridDim.y, cand_blocks);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(arrive + j, 1) == expected - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) arrive[j] = 0;
+    update_job(j, jobs, bands, sum_ss, cand, cval, part, max_chunks);
 }
 
 // ---------------------------------------------------------------------------
@@ -620,18 +761,18 @@ __global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const i
 
 }  // namespace
 
-void launch_update2d(const EvalArgs& a, cudaStream_t st)
+void launch_eval2d(const EvalArgs& a, int cand_blocks, int max_band_n, cudaStream_t st)
 {
-    if (a.njobs <= 0) return;
-    k_update2d<<<a.njobs, 256, 0, st>>>(a.jobs, a.bands, a.sum_ss, a.cand, a.cval, a.part,
-                                        a.max_chunks, 0);
+    if (a.njobs <= 0 || cand_blocks <= 0 || max_band_n < 0) return;
+    dim3 grid(std::max(1, (max_band_n + kEvalChunk - 1) / kEvalChunk), cand_blocks, a.njobs);
+    k_eval2d<<<grid, kEvalThreads, 0, st>>>(a.jobs, a.bands, a.band_spec, a.spec_off, a.sum_ss, a.cand,
+                                            a.cval, a.part, a.max_chunks, a.arrive);
 }
 
 void launch_init_jobs(const EvalArgs& a, cudaStream_t st)
 {
     if (a.njobs <= 0) return;
-    k_update2d<<<a.njobs, 256, 0, st>>>(a.jobs, a.bands, a.sum_ss, a.cand, a.cval, a.part,
-                                        a.max_chunks, 1);
+    k_init_jobs<<<a.njobs, 256, 0, st>>>(a.jobs, a.cand, a.cval);
 }
 
 void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, float4* cand,

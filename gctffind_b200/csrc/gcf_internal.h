@@ -107,6 +107,7 @@ struct EvalArgs {
     float4* cand;               // [job][kMaxCand] (mean_px, sig*cos2a, sig*sin2a, phase/pi)
     float2* cval;               // [job][kMaxCand] searched parameter values
     double2* part;              // [job][kMaxCand][max_chunks] (sum CS, sum CC)
+    int* arrive;                // [job] blocks of the current step done (0 between steps)
     int max_chunks;
     int njobs;
 };
@@ -165,9 +166,8 @@ void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_o
 void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, const int* ring_off,
                     const int* ring_pix, double* ring_sums, float* cc, cudaStream_t st);
 
-// gcf_search.cu (candidate kernel) and gcf_control.cu (state machine)
+// gcf_control.cu: candidate kernel with the state machine in its last blocks
 void launch_eval2d(const EvalArgs& a, int cand_blocks, int max_band_n, cudaStream_t st);
-void launch_update2d(const EvalArgs& a, cudaStream_t st);
 void launch_init_jobs(const EvalArgs& a, cudaStream_t st);
 void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, float4* cand,
                      float2* cval, cudaStream_t st);
