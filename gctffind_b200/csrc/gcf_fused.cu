@@ -82,6 +82,15 @@ __device__ __forceinline__ float2 w16(int m)
 // halves of the (m + 16 k + 256 p) stores hit distinct banks.
 __device__ __forceinline__ int sslot(int K) { return K + ((K >> 8) << 3); }
 
+// |z| with the fast square root (relative error within 2^-22): the
+// amplitudes only enter averages compared at 1e-4.
+__device__ __forceinline__ float amp(float x, float y)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x * x + y * y));
+    return r;
+}
+
 // Position of output k of dft16 in its register array.
 __host__ __device__ constexpr int P16(int k) { return (k & 3) * 4 + (k >> 2); }
 
@@ -102,7 +111,7 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 // 512-point forward FFT held by one warp.  In: lane l holds x[32 j + l] in
 // v[j].  Out: lane 2m+p holds X[m + 16 k + 256 p] in v[P16(k)].
 // scr: FSCR float2 of warp-private shared memory; twl[k1 * 32 + l] =
-// exp(-2 pi i l k1 / 512); tw32[k] = exp(-2 pi i k / 32).
+// exp(-2 pi i l k1 / 512); tw32[16 p + k] = p ? exp(-2 pi i k / 32) : 1.
 __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* twl,
                                             const float2* tw32, int lane)
 {
@@ -117,18 +126,18 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = scr[m * FROW + 2 * q + p];
     dft16(v);
+    // radix-2 across the lane pair: lane p = 1 multiplies its odd half by
+    // the twiddle before the exchange (lane 0 by 1, exactly), then lane 0
+    // forms E0 + W E1 and lane 1 forms E0 - W E1
     const float sg = p ? -1.0f : 1.0f;
+    const float2* twp = tw32 + 16 * p;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        float2 mine = v[P16(k)];
+        float2 u = cmul(twp[k], v[P16(k)]);
         float2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, mine.x, 1);
-        o.y = __shfl_xor_sync(0xffffffffu, mine.y, 1);
-        // lane p = 0: E0 + W E1 with E0 = mine, E1 = o;  p = 1: E0 - W E1 with E0 = o, E1 = mine
-        float2 e0 = p ? o : mine;
-        float2 e1 = p ? mine : o;
-        float2 t = cmul(tw32[k], e1);
-        v[P16(k)] = make_float2(fmaf(sg, t.x, e0.x), fmaf(sg, t.y, e0.y));
+        o.x = __shfl_xor_sync(0xffffffffu, u.x, 1);
+        o.y = __shfl_xor_sync(0xffffffffu, u.y, 1);
+        v[P16(k)] = make_float2(fmaf(sg, u.x, o.x), fmaf(sg, u.y, o.y));
     }
     __syncwarp();
 }
@@ -208,7 +217,7 @@ struct FusedShape {
     static constexpr size_t BUF = (size_t)C * YS * sizeof(float2);   // this CTA's C columns x 512 rows
     static constexpr size_t SCR = (size_t)NW * FSCR * sizeof(float2);
     static constexpr size_t TWL = 16 * 32 * sizeof(float2);
-    static constexpr size_t TW32 = 16 * sizeof(float2);
+    static constexpr size_t TW32 = 32 * sizeof(float2);
     static constexpr size_t ACCN = FT * sizeof(float);
     static constexpr size_t SMEM = (DB ? 2 : 1) * BUF + SCR + TWL + TW32 + ACCN;
     static_assert(R % 32 == 0 && PW >= 1 && NR >= 1 && R / 2 == PW * NW && C == NR * NW && C <= 32, "shape");
@@ -229,7 +238,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     float2* scr_all = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF);
     float2* twl = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF + S::SCR);
     float2* tw32 = twl + 16 * 32;
-    float* accN = reinterpret_cast<float*>(tw32 + 16);
+    float* accN = reinterpret_cast<float*>(tw32 + 32);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int r = (int)cluster.block_rank();
@@ -241,7 +250,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
 
     // per-lane twiddles exp(-2 pi i l k1 / 512) and the 32-point ones
     for (int i = tid; i < 16 * 32; i += S::THR) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
-    if (tid < 16) tw32[tid] = twg[16 * tid];
+    if (tid < 32) tw32[tid] = tid < 16 ? make_float2(1.0f, 0.0f) : twg[16 * (tid - 16)];
     __syncthreads();
 
     int par = 0;   // column-buffer parity (double buffering)
@@ -321,11 +330,12 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                 for (int i = 0; i < 8; ++i) {
                     const int K = lane + 32 * i;
                     float2 zk = scr[sslot(K)], zn = scr[sslot((FT - K) & (FT - 1))];
-                    float4 AB = make_float4(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y),
-                                            0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+                    // twice the two rows' bins (the 1/2 of the split is applied
+                    // once, exactly, to the averaged spectrum in k_item_reduce)
+                    float4 AB = make_float4(zk.x + zn.x, zk.y - zn.y, zk.y + zn.y, zn.x - zk.x);
                     if (K == 0) {   // pack the real DC and Nyquist bins of both rows
                         float2 zh = scr[sslot(FT / 2)];
-                        AB = make_float4(zk.x, zh.x, zk.y, zh.y);
+                        AB = make_float4(2.0f * zk.x, 2.0f * zh.x, 2.0f * zk.y, 2.0f * zh.y);
                     }
                     float2* dst = cluster.map_shared_rank(colbuf, K / C) + (size_t)(K % C) * YS + Y0;
                     *reinterpret_cast<float4*>(dst) = AB;
@@ -360,7 +370,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         float2 z = v[P16(k)];
-                        acc[rho][k] += sqrtf(z.x * z.x + z.y * z.y);
+                        acc[rho][k] += amp(z.x, z.y);
                     }
                 } else {
 #pragma unroll
@@ -372,8 +382,8 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                         float2 zk = v[P16(k)], zn = scr[sslot((FT - Kk) & (FT - 1))];
                         float ax = 0.5f * (zk.x + zn.x), ay = 0.5f * (zk.y - zn.y);
                         float bx = 0.5f * (zk.y + zn.y), by = -0.5f * (zk.x - zn.x);
-                        acc[rho][k] += sqrtf(ax * ax + ay * ay);
-                        accN[Kk] += sqrtf(bx * bx + by * by);
+                        acc[rho][k] += amp(ax, ay);
+                        accN[Kk] += amp(bx, by);
                     }
                     __syncwarp();
                 }
@@ -406,7 +416,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     cluster.sync();   // keep shared memory alive until every peer is done
 }
 
-// raw[img] = sum of the img's item partials (in item order) / ntiles.
+// raw[img] = sum of the img's item partials (in item order) / ntiles / 2.
 __global__ void k_item_reduce(const float* __restrict__ partial, const int* __restrict__ first,
                               const float* __restrict__ inv, float* __restrict__ raw)
 {
@@ -416,7 +426,7 @@ __global__ void k_item_reduce(const float* __restrict__ partial, const int* __re
     if (i >= n) return;
     double s = 0.0;
     for (int k = first[img]; k < first[img + 1]; ++k) s += partial[(size_t)k * n + i];
-    raw[(size_t)img * n + i] = (float)(s * (double)inv[img]);
+    raw[(size_t)img * n + i] = (float)(s * (double)inv[img] * 0.5);   // rows were split without the 1/2
 }
 
 template <class S>
