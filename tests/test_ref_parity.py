@@ -256,3 +256,24 @@ def test_flat_spectrum_skips_lowpass_like_reference(gpu_lib, ref):
     ctx.close()
     assert r.lowpassed == 0
     _close(res, [float(x) for x in R["result"]])
+
+
+def test_uneven_batch_matches_reference_single_file_mode(gpu_lib, ref):
+    """gcf_run_batch (independent full searches of micrographs of different
+    sizes and pixel sizes in one call) against the reference run once per
+    micrograph, as its single-file mode does (CInputFolder::mReadSingle)."""
+    G = gpu_lib
+    rng = np.random.default_rng(12)
+    specs = [(2048, 2048, 0.8), (1536, 1152, 1.5), (2000, 1400, 1.0), (1024, 1024, 1.35),
+             (1777, 1333, 1.2)]
+    imgs, truth = [], []
+    for k, (w, h, px) in enumerate(specs):
+        df = float(rng.uniform(8000.0, 30000.0))
+        ast = float(rng.uniform(0.0, 600.0))
+        imgs.append(_img(w, h, px, (df - ast / 2, df + ast / 2), float(rng.uniform(-90, 90)), 900 + k))
+    ctx = G.Context(0, 512, 0)
+    mine = ctx.run_batch(imgs, [s[2] for s in specs], G.make_optics())
+    ctx.close()
+    for img, (w, h, px), r in zip(imgs, specs, mine):
+        R, _, _ = ref.run_series([img], px, [0], is_tomo=False, tile=512)
+        _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], [float(x) for x in R[0]])
