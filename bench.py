@@ -108,7 +108,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -306,12 +306,14 @@ def main():
     op = G.make_optics(pixel_size=PX)
 
     # ---- device-resident inputs -------------------------------------------------
+    # clocks are sampled from the warm-up on through the end-to-end steps, so
+    # the short device-resident region gets samples on both sides as well
+    clk = ClockSampler(local)
+    clk.start()
     for _ in range(args.warmup):
         ctx.run_series(imgs, op, order, is_tomo=True)
     barrier(world)
     torch.cuda.synchronize()
-    clk = ClockSampler(local)
-    clk.start()
     dev_ms, stage = 0.0, {}
     launches = 0
     results = None
@@ -325,7 +327,6 @@ def main():
         launches += ctx.launch_count()
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    clocks = clk.stop()
     barrier(world)
     t_step = max_over_ranks(dev_ms / args.steps, world)
     value = world * args.n_tilts / (t_step / 1000.0)
@@ -341,6 +342,7 @@ def main():
         ctx.run_series(host, op, order, is_tomo=True)
         e2e_ms += ctx.stage_times()["total"]
     torch.cuda.nvtx.range_pop()
+    clocks = clk.stop()
     barrier(world)
     t_e2e = max_over_ranks(e2e_ms / args.steps, world)
     e2e = world * args.n_tilts / (t_e2e / 1000.0)

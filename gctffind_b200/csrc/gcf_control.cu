@@ -427,7 +427,8 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
     const int p0 = blockIdx.x * kEvalChunk;
     if ((int)blockIdx.x >= max(nchunk, 1)) return;
     const float* S = band_spec + spec_off[j];
-    float pa[kEvalPPT], pd[kEvalPPT], pe[kEvalPPT], pc[kEvalPPT], ps[kEvalPPT], pv[kEvalPPT];
+    // per pixel: a, d, envelope and -envelope/2, cos 2theta, sin 2theta, spectrum
+    float pa[kEvalPPT], pd[kEvalPPT], pe[kEvalPPT], ph[kEvalPPT], pc[kEvalPPT], ps[kEvalPPT], pv[kEvalPPT];
 #pragma unroll
     for (int k = 0; k < kEvalPPT; ++k) {
         int p = p0 + k * kEvalThreads + threadIdx.x;
@@ -446,6 +447,7 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
             ps[k] = 0.f;
             pv[k] = 0.f;
         }
+        ph[k] = -0.5f * pe[k];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // candidate blocks y, y + gridDim.y, ... so any candidate count is covered
@@ -468,7 +470,7 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
                 float t = fmaf(pa[k], df, pd[k]) + q.w;
                 float r = t - rintf(t);
                 float sv = __sinf(r * 3.14159265358979f);
-                float C = (fabsf(sv) - 0.5f) * pe[k];
+                float C = fmaf(fabsf(sv), pe[k], ph[k]);   // (|sin| - 1/2) * env
                 s_cs = fmaf(C, pv[k], s_cs);
                 s_cc = fmaf(C, C, s_cc);
             }

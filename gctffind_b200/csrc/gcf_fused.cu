@@ -103,7 +103,10 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 #pragma unroll
     for (int k1 = 1; k1 < 4; ++k1)
 #pragma unroll
-        for (int n2 = 1; n2 < 4; ++n2) v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w16(n2 * k1));
+        for (int n2 = 1; n2 < 4; ++n2) {
+            if (n2 * k1 == 4) v[4 * k1 + n2] = make_float2(v[4 * k1 + n2].y, -v[4 * k1 + n2].x);   // * (-i)
+            else v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w16(n2 * k1));
+        }
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) dft4(v[4 * k1 + 0], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
 }
