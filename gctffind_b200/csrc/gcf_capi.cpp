@@ -72,6 +72,11 @@ struct gcf_ctx {
     int impl = GCF_SPECT_CUFFT;
     cudaStream_t st = nullptr;
     cudaStream_t st_copy = nullptr;   // host -> device uploads
+    // Compute work goes to `st`.  A series in device memory runs its tile
+    // spectra on the high-priority stream while post-processing and searches
+    // of finished chunks run on `st_search` (low priority) in the SMs the
+    // cluster kernel leaves free; `st` is swapped with it for those calls.
+    cudaStream_t st_search = nullptr;
     std::vector<cudaEvent_t> chunk_ev;
     std::string err;
     long long launches = 0;
@@ -586,6 +591,8 @@ gcf_status spectra_post(gcf_ctx* ctx, int nm, int first = 0)
     cufftHandle pf, pi;
     CKS(get_plan(ctx, 3, T, nm, &pf));
     CKS(get_plan(ctx, 4, T, nm, &pi));
+    if (cufftSetStream(pf, ctx->st) != CUFFT_SUCCESS || cufftSetStream(pi, ctx->st) != CUFFT_SUCCESS)
+        return fail(ctx, GCF_ERR_CUFFT, "cufftSetStream (lowpass) failed");
     if (cufftExecR2C(pf, ctx->lpfull.p, (cufftComplex*)ctx->lpcmp.p) != CUFFT_SUCCESS)
         return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (lowpass) failed");
     launch_lp_filter(ctx->lpcmp.p, T, nm, 10.0, ctx->st);
@@ -994,8 +1001,11 @@ gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
     ctx->tile = tile_size;
     ctx->log_spect = log_spect ? 1 : 0;
     ctx->impl = fused_tile_supported(tile_size) ? GCF_SPECT_FUSED : GCF_SPECT_CUFFT;
+    int prio_lo = 0, prio_hi = 0;
     if (cudaSetDevice(gpu) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->st_search, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->st_copy, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return GCF_ERR_CUDA;
@@ -1016,6 +1026,7 @@ void gcf_destroy(gcf_ctx* ctx)
     cudaSetDevice(ctx->dev);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->st_copy) cudaStreamSynchronize(ctx->st_copy);
+    if (ctx->st_search) cudaStreamSynchronize(ctx->st_search);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
     for (auto* b : ctx->bands) {
         b->idx.release();
@@ -1075,6 +1086,7 @@ void gcf_destroy(gcf_ctx* ctx)
     for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
     for (auto& ev : ctx->kev) cudaEventDestroy(ev);
     if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
+    if (ctx->st_search) cudaStreamDestroy(ctx->st_search);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -1541,6 +1553,61 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     return GCF_OK;
 }
 
+// Device images: the tile spectra are enqueued at once on the high-priority
+// stream, the first package alone and then all others in one launch; the
+// first package's post-processing and full search run on the search stream
+// while the big launch proceeds (in the SMs its 8-CTA clusters leave free),
+// and the refinements follow once every spectrum is done.
+gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs, int w, int h,
+                             float px, std::vector<MicImage>& mics, SeriesLoop& loop)
+{
+    const int n = (int)imgs.size();
+    mics.assign(n, MicImage{});
+    int nw, nh;
+    float pn;
+    gcf_rescale_dims(w, h, px, &nw, &nh, &pn);
+    const bool rescaled = (1.2f / px) > 1;
+    CKS(spectra_alloc(ctx, n));
+    if (rescaled) CK(ctx->rescaled.ensure((size_t)nw * nh * n));
+    std::vector<int> bounds{0, 1};
+    if (n > 1) bounds.push_back(n);
+    const int nchunks = (int)bounds.size() - 1;
+    while ((int)ctx->chunk_ev.size() < nchunks + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->chunk_ev.push_back(e);
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    for (int c = 0; c < nchunks; ++c) {
+        for (int k = bounds[c]; k < bounds[c + 1]; ++k) {
+            size_t used = 0;
+            float* dst = rescaled ? ctx->rescaled.p + (size_t)nw * nh * k : nullptr;
+            CKS(stage_image(ctx, imgs[k], w, h, px, dst, mics[k], &used));
+        }
+        CKS(spectra_chunk(ctx, mics, bounds[c], bounds[c + 1] - bounds[c]));
+        CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    auto search_phase = [&]() -> gcf_status {
+        for (int c = 0; c < nchunks; ++c) {
+            CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
+            CKS(spectra_post(ctx, bounds[c + 1] - bounds[c], bounds[c]));
+            CKS(loop.run(bounds[c], bounds[c + 1]));
+        }
+        return GCF_OK;
+    };
+    std::swap(ctx->st, ctx->st_search);
+    gcf_status st = search_phase();
+    cudaError_t e = cudaEventRecord(ctx->chunk_ev[nchunks], ctx->st);
+    std::swap(ctx->st, ctx->st_search);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[nchunks], 0);
+    if (st == GCF_OK && e != cudaSuccess) st = fail(ctx, GCF_ERR_CUDA, cudaGetErrorString(e));
+    return st;
+}
+
 }  // namespace
 
 gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w, int h,
@@ -1576,10 +1643,7 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
     std::vector<MicImage> mics;
     gcf_status st;
     if (on_device) {
-        std::vector<int> ws(n, w), hs(n, h);
-        std::vector<float> pxs(n, optics->pixel_size);
-        st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, 1, mics);
-        if (st == GCF_OK) st = loop.run(0, n);
+        st = series_overlapped(ctx, imgs, w, h, optics->pixel_size, mics, loop);
     } else {
         st = series_streamed(ctx, imgs, w, h, optics->pixel_size, mics, loop);
     }
