@@ -277,3 +277,44 @@ def test_uneven_batch_matches_reference_single_file_mode(gpu_lib, ref):
     for img, (w, h, px), r in zip(imgs, specs, mine):
         R, _, _ = ref.run_series([img], px, [0], is_tomo=False, tile=512)
         _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], [float(x) for x in R[0]])
+
+
+def test_config0_single_micrograph_matches_reference(gpu_lib, ref):
+    """The single-micrograph configuration: 4096 x 4096 at 1.0 A/px (rescaled
+    to 3412 x 3412 at 1.2 A/px), 300 kV, Cs 2.7 mm, Ac 0.07, defocus
+    15000 A with 300 A of astigmatism at 20 degrees, 1 e/A^2, tile 512,
+    1D then 2D search."""
+    G = gpu_lib
+    spec = synth.MicrographSpec(width=4096, height=4096, pixel_size=1.0, df_min=14850.0,
+                                df_max=15150.0, azimuth_deg=20.0, dose=1.0, seed=2024)
+    img = synth.make_micrograph(spec, device="cpu").numpy().astype(np.float32)
+    R, _, _ = ref.run_series([img], 1.0, [0], is_tomo=False, tile=512)
+    ctx = G.Context(0, 512, 0)
+    r = ctx.run_series([img], G.make_optics(pixel_size=1.0), [0], is_tomo=False)[0]
+    ctx.close()
+    _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], [float(x) for x in R[0]])
+    assert abs(0.5 * (r.df_min + r.df_max) - 15000.0) < 150.0
+
+
+def test_config2_uneven_sizes_match_reference(gpu_lib, ref):
+    """The uneven batch's sizes (4096 x 4096, 5760 x 4092, 3838 x 3710) at
+    pixel sizes from 0.8 to 1.5 A/px through one gcf_run_batch call, against
+    the reference once per micrograph."""
+    G = gpu_lib
+    rng = np.random.default_rng(256)
+    sizes = [(4096, 4096, 0.8), (5760, 4092, 1.5), (3838, 3710, 1.1), (5760, 4092, 0.9),
+             (3838, 3710, 1.5), (4096, 4096, 1.3)]
+    imgs = []
+    for k, (w, h, px) in enumerate(sizes):
+        df = float(rng.uniform(9000.0, 38000.0))
+        ast = float(rng.uniform(0.0, 1000.0))
+        spec = synth.MicrographSpec(width=w, height=h, pixel_size=px, df_min=df - ast / 2,
+                                    df_max=df + ast / 2, azimuth_deg=float(rng.uniform(-90, 90)),
+                                    dose=float(rng.uniform(0.5, 2.0)), seed=3000 + k)
+        imgs.append(synth.make_micrograph(spec, device="cpu").numpy().astype(np.float32))
+    ctx = G.Context(0, 512, 0)
+    mine = ctx.run_batch(imgs, [s[2] for s in sizes], G.make_optics())
+    ctx.close()
+    for img, (w, h, px), r in zip(imgs, sizes, mine):
+        R, _, _ = ref.run_series([img], px, [0], is_tomo=False, tile=512)
+        _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], [float(x) for x in R[0]])
