@@ -98,12 +98,14 @@ CASES = [
     (1501, 1101, 0.8, (12000.0, 12300.0), 5.0, 109, 0.0, 256, 1, 0.0, 0.0, None),
     # odd raw width without rescale: the last column is dropped (new size even)
     (1023, 777, 1.5, (26000.0, 26600.0), 60.0, 110, 0.0, 256, 0, 0.0, 0.0, None),
+    # a tile size that is not a power of two (batched cuFFT with mixed radices)
+    (1536, 1536, 1.35, (19000.0, 19500.0), -50.0, 112, 0.0, 384, 0, 0.0, 0.0, None),
 ]
 
 
 @pytest.mark.parametrize("case", CASES, ids=["px1.0_t512", "px1.35_t512", "phase_t512", "log_t256",
                                              "refine_t512", "px1.0_t1024", "odd_rescale_log_t256",
-                                             "odd_width_t256"])
+                                             "odd_width_t256", "px1.35_t384"])
 def test_single_micrograph_matches_reference(gpu_lib, ref, case):
     w, h, px, df, az, seed, phase_truth, tile, log, ph0, phr, refine = case
     img = _img(w, h, px, df, az, seed, phase=phase_truth)
