@@ -40,6 +40,10 @@ namespace gcf {
 namespace {
 
 constexpr int FT = 512;          // tile edge
+
+// exp(-2 pi i k / 32), k < 16, rounded to float from double like the host
+// twiddle tables; written once per device before the first launch.
+__constant__ float2 c_tw32[16];
 constexpr int FCX = FT / 2 + 1;  // 257 half-spectrum columns
 constexpr int FSCR = 16 * 34;    // per-warp scratch, float2 units
 constexpr int FROW = 34;         // transpose row stride: 64-bit accesses of either side hit distinct banks
@@ -114,9 +118,8 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 // 512-point forward FFT held by one warp.  In: lane l holds x[32 j + l] in
 // v[j].  Out: lane 2m+p holds X[m + 16 k + 256 p] in v[P16(k)].
 // scr: FSCR float2 of warp-private shared memory; twl[k1 * 32 + l] =
-// exp(-2 pi i l k1 / 512); tw32[16 p + k] = p ? exp(-2 pi i k / 32) : 1.
-__device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* twl,
-                                            const float2* tw32, int lane)
+// exp(-2 pi i l k1 / 512); the 32-point twiddles are c_tw32.
+__device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const float2* twl, int lane)
 {
     dft16(v);
 #pragma unroll
@@ -130,13 +133,13 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
     for (int q = 0; q < 16; ++q) v[q] = scr[m * FROW + 2 * q + p];
     dft16(v);
     // radix-2 across the lane pair: lane p = 1 multiplies its odd half by
-    // the twiddle before the exchange (lane 0 by 1, exactly), then lane 0
-    // forms E0 + W E1 and lane 1 forms E0 - W E1
+    // the twiddle before the exchange, then lane 0 forms E0 + W E1 and
+    // lane 1 forms E0 - W E1
     const float sg = p ? -1.0f : 1.0f;
-    const float2* twp = tw32 + 16 * p;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        float2 u = cmul(twp[k], v[P16(k)]);
+        float2 u = cmul(c_tw32[k], v[P16(k)]);
+        if (!p) u = v[P16(k)];
         float2 o;
         o.x = __shfl_xor_sync(0xffffffffu, u.x, 1);
         o.y = __shfl_xor_sync(0xffffffffu, u.y, 1);
@@ -220,9 +223,8 @@ struct FusedShape {
     static constexpr size_t BUF = (size_t)C * YS * sizeof(float2);   // this CTA's C columns x 512 rows
     static constexpr size_t SCR = (size_t)NW * FSCR * sizeof(float2);
     static constexpr size_t TWL = 16 * 32 * sizeof(float2);
-    static constexpr size_t TW32 = 32 * sizeof(float2);
     static constexpr size_t ACCN = FT * sizeof(float);
-    static constexpr size_t SMEM = (DB ? 2 : 1) * BUF + SCR + TWL + TW32 + ACCN;
+    static constexpr size_t SMEM = (DB ? 2 : 1) * BUF + SCR + TWL + ACCN;
     static_assert(R % 32 == 0 && PW >= 1 && NR >= 1 && R / 2 == PW * NW && C == NR * NW && C <= 32, "shape");
 };
 using Shape16 = FusedShape<16, 16, true>;         // 16-CTA clusters, 512 threads
@@ -240,8 +242,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     float2* colbuf0 = reinterpret_cast<float2*>(smem);
     float2* scr_all = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF);
     float2* twl = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF + S::SCR);
-    float2* tw32 = twl + 16 * 32;
-    float* accN = reinterpret_cast<float*>(tw32 + 32);
+    float* accN = reinterpret_cast<float*>(twl + 16 * 32);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int r = (int)cluster.block_rank();
@@ -251,9 +252,8 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     const int m = lane >> 1, p = lane & 1;
     float2* scr = scr_all + warp * FSCR;
 
-    // per-lane twiddles exp(-2 pi i l k1 / 512) and the 32-point ones
+    // per-lane twiddles exp(-2 pi i l k1 / 512)
     for (int i = tid; i < 16 * 32; i += S::THR) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
-    if (tid < 32) tw32[tid] = tid < 16 ? make_float2(1.0f, 0.0f) : twg[16 * (tid - 16)];
     __syncthreads();
 
     int par = 0;   // column-buffer parity (double buffering)
@@ -323,7 +323,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                     int X = 32 * j + lane;
                     v[j] = make_float2((ca[j] - mean) * __ldg(ta + X), (cb[j] - mean) * __ldg(ta + FT + X));
                 }
-                fft512_warp(v, scr, twl, tw32, lane);
+                fft512_warp(v, scr, twl, lane);
 #pragma unroll
                 for (int k = 0; k < 16; ++k) scr[sslot(m + 16 * k + 256 * p)] = v[P16(k)];
                 __syncwarp();
@@ -368,7 +368,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
                 const float2* col = colbuf + (size_t)cl * YS;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) v[j] = col[32 * j + lane];
-                fft512_warp(v, scr, twl, tw32, lane);
+                fft512_warp(v, scr, twl, lane);
                 if (K != 0) {
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
@@ -449,9 +449,32 @@ cudaLaunchConfig_t fused_cfg(int nclusters, cudaStream_t st, cudaLaunchAttribute
     return cfg;
 }
 
+// c_tw32 of the current device, once.
+cudaError_t init_constants()
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return cudaSuccess;
+    float2 w[16];
+    for (int k = 0; k < 16; ++k) {
+        double a = -2.0 * M_PI * (double)(16 * k) / FT;
+        w[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    e = cudaMemcpyToSymbol(c_tw32, w, sizeof(w));
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+}
+
 template <class S>
 cudaError_t prepare_kernel()
 {
+    cudaError_t ec = init_constants();
+    if (ec != cudaSuccess) return ec;
     cudaError_t e = cudaFuncSetAttribute(k_fused_spectrum<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::SMEM);
     if (e != cudaSuccess) return e;
