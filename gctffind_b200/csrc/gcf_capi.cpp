@@ -77,6 +77,10 @@ struct gcf_ctx {
     // of finished chunks run on `st_search` (low priority) in the SMs the
     // cluster kernel leaves free; `st` is swapped with it for those calls.
     cudaStream_t st_search = nullptr;
+    // Second high-priority stream: consecutive tile-spectrum chunks of a
+    // device series alternate between `st` and `st_tile`, so a chunk's
+    // clusters start while the previous chunk's last items finish.
+    cudaStream_t st_tile = nullptr;
     std::vector<cudaEvent_t> chunk_ev;
     std::string err;
     long long launches = 0;
@@ -120,8 +124,11 @@ struct gcf_ctx {
     DBuf<int4> f_items;
     DBuf<int> f_first;
     DBuf<float> f_inv, f_partial;
+    DBuf<int> f_next;   // item counters of the tile kernel launches
     DBuf<double> f_bsum;
     DBuf<double*> f_bsum_ptr;
+    std::vector<int> f_first_h;    // host copy of f_first for the current plan
+    std::vector<int> f_blocks_h;   // block-sum blocks of each planned micrograph
     int fused_clusters = 0;
     int fused_shape = 0;
     int fused_shape_req = 0;   // 0: pick by SM coverage
@@ -453,9 +460,12 @@ gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
     return GCF_OK;
 }
 
-// CGenAvgSpectrum::DoIt for all micrographs in one launch of the fused
-// tile-spectrum kernel (tile 512).
-gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float* raw_out)
+// Work plan of the fused tile-spectrum kernel (tile 512) for mics: image
+// descriptors, block-sum slots and work items, uploaded on ctx->st.  Each
+// micrograph's tiles form runs of at most 32 (an item's |F| sums live in
+// registers until it ends); the split depends on the micrograph alone, so
+// its spectrum does not depend on the batch or chunk it is in.
+gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
 {
     const int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
     if (ctx->fused_clusters <= 0) {
@@ -466,17 +476,15 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
         ctx->fused_clusters = n;
         ctx->fused_shape = shape;
     }
-    // Work items: each micrograph's tiles in runs of at most 32 (every item's
-    // |F| sums live in registers until it ends).  The split depends on the
-    // micrograph alone, so its spectrum does not depend on the batch it is in.
     const int kItemTiles = 32;
     std::vector<FusedImageDesc> d(nm);
     std::vector<int4> items;
-    std::vector<int> first(nm + 1);
+    std::vector<int>& first = ctx->f_first_h;
+    first.assign(nm + 1, 0);
+    ctx->f_blocks_h.assign(nm, 0);
     std::vector<float> inv(nm);
     std::vector<size_t> boff(nm);
     size_t nblk = 0;
-    int max_blocks = 0;
     for (int i = 0; i < nm; ++i) {
         const MicImage& m = mics[i];
         Layout L = tile_layout(m.w, m.h, T);
@@ -494,8 +502,8 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
                     ((uintptr_t)m.img % 8) == 0) ? 2 : 1;
         d[i].nbx = L.ntx + 1;
         boff[i] = nblk;
-        nblk += (size_t)(L.ntx + 1) * (L.nty + 1);
-        max_blocks = std::max(max_blocks, (L.ntx + 1) * (L.nty + 1));
+        ctx->f_blocks_h[i] = (L.ntx + 1) * (L.nty + 1);
+        nblk += (size_t)ctx->f_blocks_h[i];
         inv[i] = 1.0f / nt;
         first[i] = (int)items.size();
         int nch = (nt + kItemTiles - 1) / kItemTiles;
@@ -518,10 +526,25 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     CK(ctx->f_first.ensure(nm + 1));
     CK(ctx->f_inv.ensure(nm));
     CK(ctx->f_partial.ensure((size_t)ni * cx * T));
+    CK(ctx->f_next.ensure(nm));
     CK(cudaMemcpyAsync(ctx->f_desc.p, d.data(), nm * sizeof(FusedImageDesc), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->f_items.p, items.data(), ni * sizeof(int4), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->f_inv.p, inv.data(), nm * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    return GCF_OK;
+}
+
+// Spectra of planned micrographs m0 .. m1-1 into raw_out (the spectrum of
+// m0) on stream st.  Launches of disjoint ranges share the plan's buffers
+// (each range owns its items, partial spectra and item counter), so they
+// may run concurrently once the plan's uploads are done.
+gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream_t st)
+{
+    const std::vector<int>& first = ctx->f_first_h;
+    if (m0 < 0 || m1 > (int)first.size() - 1 || m0 >= m1) return fail(ctx, GCF_ERR_STATE, "tile-spectrum range outside the plan");
+    const int ni = first[m1] - first[m0];
+    int max_blocks = 0;
+    for (int i = m0; i < m1; ++i) max_blocks = std::max(max_blocks, ctx->f_blocks_h[i]);
     int ncl = std::min(ctx->fused_clusters, ni);
     if (ctx->kev_used > 256) ctx->kev_used = 0;   // calls that never read their stage times
     while ((int)ctx->kev.size() < ctx->kev_used + 2) {
@@ -531,11 +554,19 @@ gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float
     }
     cudaEvent_t e0 = ctx->kev[ctx->kev_used], e1 = ctx->kev[ctx->kev_used + 1];
     ctx->kev_used += 2;
-    CK(launch_fused(ctx->f_desc.p, ctx->f_bsum_ptr.p, max_blocks, ctx->f_items.p, ni, ctx->f_first.p,
-                    ctx->f_inv.p, nm, ctx->taper.p, ctx->tw512.p, ctx->f_partial.p, raw_out, ncl,
-                    ctx->fused_shape, ctx->st, e0, e1));
+    CK(launch_fused(ctx->f_desc.p, ctx->f_bsum_ptr.p, max_blocks, ctx->f_items.p + first[m0], ni, ctx->f_first.p,
+                    ctx->f_inv.p, m0, m1 - m0, ctx->taper.p, ctx->tw512.p, ctx->f_partial.p, raw_out,
+                    ctx->f_next.p + m0, ncl, ctx->fused_shape, st, e0, e1));
     ctx->launches += 3;
     return GCF_OK;
+}
+
+// CGenAvgSpectrum::DoIt for all micrographs in one launch of the fused
+// tile-spectrum kernel (tile 512).
+gcf_status spectrum_fused(gcf_ctx* ctx, const std::vector<MicImage>& mics, float* raw_out)
+{
+    CKS(fused_plan(ctx, mics));
+    return fused_launch(ctx, 0, (int)mics.size(), raw_out, ctx->st);
 }
 
 // Buffers of the spectrum stage for nm micrographs.
@@ -916,11 +947,36 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
     return GCF_OK;
 }
 
+// Stage times of the last call.  The tile-kernel time is the union of the
+// launches' [begin, end] intervals (launches on two streams may overlap),
+// measured from ev[0]; where ev[0] was not recorded, the sum of durations.
 void accumulate_stage_times(gcf_ctx* ctx)
 {
     float t;
-    for (int i = 0; i + 1 < ctx->kev_used; i += 2)
-        if (cudaEventElapsedTime(&t, ctx->kev[i], ctx->kev[i + 1]) == cudaSuccess) ctx->stage_ms[1] += t;
+    std::vector<std::pair<float, float>> iv;
+    bool rel = true;
+    for (int i = 0; i + 1 < ctx->kev_used; i += 2) {
+        float a = 0.0f, b = 0.0f;
+        if (rel && cudaEventElapsedTime(&a, ctx->ev[0], ctx->kev[i]) == cudaSuccess &&
+            cudaEventElapsedTime(&b, ctx->ev[0], ctx->kev[i + 1]) == cudaSuccess) {
+            iv.emplace_back(a, b);
+        } else {
+            rel = false;
+        }
+    }
+    if (rel) {
+        std::sort(iv.begin(), iv.end());
+        float end = -1e30f;
+        for (auto& x : iv) {
+            float a = std::max(x.first, end);
+            if (x.second > a) ctx->stage_ms[1] += x.second - a;
+            end = std::max(end, x.second);
+        }
+    } else {
+        for (int i = 0; i + 1 < ctx->kev_used; i += 2)
+            if (cudaEventElapsedTime(&t, ctx->kev[i], ctx->kev[i + 1]) == cudaSuccess) ctx->stage_ms[1] += t;
+    }
+    cudaGetLastError();   // a failed elapsed-time query leaves no sticky error
     ctx->kev_used = 0;
     if (cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]) == cudaSuccess) ctx->stage_ms[0] += t;
     if (cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev[3]) == cudaSuccess) ctx->stage_ms[2] += t;
@@ -1006,6 +1062,7 @@ gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
         cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->st_search, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->st_tile, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->st_copy, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return GCF_ERR_CUDA;
@@ -1027,6 +1084,7 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->st_copy) cudaStreamSynchronize(ctx->st_copy);
     if (ctx->st_search) cudaStreamSynchronize(ctx->st_search);
+    if (ctx->st_tile) cudaStreamSynchronize(ctx->st_tile);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
     for (auto* b : ctx->bands) {
         b->idx.release();
@@ -1079,6 +1137,7 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->f_first.release();
     ctx->f_inv.release();
     ctx->f_partial.release();
+    ctx->f_next.release();
     ctx->f_bsum.release();
     ctx->f_bsum_ptr.release();
     for (auto& ev : ctx->ev)
@@ -1087,6 +1146,7 @@ void gcf_destroy(gcf_ctx* ctx)
     for (auto& ev : ctx->kev) cudaEventDestroy(ev);
     if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
     if (ctx->st_search) cudaStreamDestroy(ctx->st_search);
+    if (ctx->st_tile) cudaStreamDestroy(ctx->st_tile);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -1494,6 +1554,21 @@ struct SeriesLoop {
     }
 };
 
+// Chunk bounds of a series of n packages in processing order: the first
+// package alone (its full search starts early), then 8 packages, shrinking
+// towards the end so that little work follows the last chunk.
+std::vector<int> series_chunks(int n)
+{
+    std::vector<int> bounds{0};
+    for (int b = 1; b < n;) {
+        bounds.push_back(b);
+        int rem = n - b;
+        b += rem > 12 ? 8 : rem > 6 ? 4 : rem > 2 ? 2 : 1;
+    }
+    bounds.push_back(n);
+    return bounds;
+}
+
 // Host images: uploads in processing order on the copy stream (the first
 // package alone, then chunks of 8), and after each chunk its spectra,
 // post-processing and package searches, so only the last chunk's work
@@ -1510,15 +1585,7 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     CKS(spectra_alloc(ctx, n));
     if (rescaled) CK(ctx->rescaled.ensure((size_t)nw * nh * n));
     CK(ctx->images.ensure((size_t)w * h * n));
-    // chunks: the first package alone (its full search starts early), then
-    // 8 packages, shrinking towards the end so little work follows the last copy
-    std::vector<int> bounds{0};
-    for (int b = 1; b < n;) {
-        bounds.push_back(b);
-        int rem = n - b;
-        b += rem > 12 ? 8 : rem > 6 ? 4 : rem > 2 ? 2 : 1;
-    }
-    bounds.push_back(n);
+    std::vector<int> bounds = series_chunks(n);
     const int nchunks = (int)bounds.size() - 1;
     while ((int)ctx->chunk_ev.size() < nchunks) {
         cudaEvent_t e;
@@ -1553,15 +1620,18 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     return GCF_OK;
 }
 
-// Device images: the tile spectra are enqueued at once on the high-priority
-// stream, the first package alone and then all others in one launch; the
-// first package's post-processing and full search run on the search stream
-// while the big launch proceeds (in the SMs its 8-CTA clusters leave free),
-// and the refinements follow once every spectrum is done.
+// Device images: every chunk's tile spectra are enqueued at once, the
+// chunks alternating between the two high-priority streams (one plan, one
+// upload of the work items); post-processing and the package searches of
+// each finished chunk run on the search stream in the SMs the 8-CTA
+// clusters leave free, so only the last chunk's searches follow the last
+// tile-spectrum launch.
 gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs, int w, int h,
                              float px, std::vector<MicImage>& mics, SeriesLoop& loop)
 {
     const int n = (int)imgs.size();
+    const int T = ctx->tile;
+    const size_t cmp_n = (size_t)(T / 2 + 1) * T;
     mics.assign(n, MicImage{});
     int nw, nh;
     float pn;
@@ -1569,10 +1639,16 @@ gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs
     const bool rescaled = (1.2f / px) > 1;
     CKS(spectra_alloc(ctx, n));
     if (rescaled) CK(ctx->rescaled.ensure((size_t)nw * nh * n));
+    const bool fused = ctx->impl == GCF_SPECT_FUSED;
+    // the first package alone, then the rest in two halves: the searches of
+    // the first half overlap the tile spectra of the second (finer chunks
+    // measured slower: searches running beside the cluster kernel take SMs
+    // its 8-CTA clusters need)
     std::vector<int> bounds{0, 1};
+    if (fused && n > 2) bounds.push_back(1 + n / 2);
     if (n > 1) bounds.push_back(n);
     const int nchunks = (int)bounds.size() - 1;
-    while ((int)ctx->chunk_ev.size() < nchunks + 1) {
+    while ((int)ctx->chunk_ev.size() < nchunks + 2) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->chunk_ev.push_back(e);
@@ -1580,14 +1656,29 @@ gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
-    for (int c = 0; c < nchunks; ++c) {
-        for (int k = bounds[c]; k < bounds[c + 1]; ++k) {
-            size_t used = 0;
-            float* dst = rescaled ? ctx->rescaled.p + (size_t)nw * nh * k : nullptr;
-            CKS(stage_image(ctx, imgs[k], w, h, px, dst, mics[k], &used));
+    for (int k = 0; k < n; ++k) {
+        size_t used = 0;
+        float* dst = rescaled ? ctx->rescaled.p + (size_t)nw * nh * k : nullptr;
+        CKS(stage_image(ctx, imgs[k], w, h, px, dst, mics[k], &used));
+    }
+    if (fused) {
+        CKS(fused_plan(ctx, mics));
+        cudaEvent_t planned = ctx->chunk_ev[nchunks + 1];
+        CK(cudaEventRecord(planned, ctx->st));
+        CK(cudaStreamWaitEvent(ctx->st_tile, planned, 0));
+        for (int c = 0; c < nchunks; ++c) {
+            cudaStream_t s = (c & 1) ? ctx->st_tile : ctx->st;
+            CKS(fused_launch(ctx, bounds[c], bounds[c + 1], ctx->raw.p + cmp_n * bounds[c], s));
+            CK(cudaEventRecord(ctx->chunk_ev[c], s));
         }
-        CKS(spectra_chunk(ctx, mics, bounds[c], bounds[c + 1] - bounds[c]));
-        CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st));
+        // st joins st_tile (its last chunk) before anything else runs on it
+        CK(cudaEventRecord(planned, ctx->st_tile));
+        CK(cudaStreamWaitEvent(ctx->st, planned, 0));
+    } else {
+        for (int c = 0; c < nchunks; ++c) {
+            CKS(spectra_chunk(ctx, mics, bounds[c], bounds[c + 1] - bounds[c]));
+            CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st));
+        }
     }
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
     CK(cudaEventRecord(ctx->ev[4], ctx->st));

@@ -20,8 +20,9 @@
 //           all tiles of a work item and are written once.
 // With CL = 16 the column buffer is double-buffered, so one cluster barrier
 // per tile separates writers from readers.  Work items are (image, tile
-// range) pairs; their partial spectra are summed in item order by
-// k_item_reduce, so the result is deterministic.
+// range) pairs, handed out in order through a counter; their partial
+// spectra are summed in item order by k_item_reduce, so the result does not
+// depend on which cluster took which item.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -235,7 +236,7 @@ template <class S>
 __global__ void __launch_bounds__(S::THR, 1)
 k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ items, int nitems,
                  const float* __restrict__ taper, const float2* __restrict__ twg,
-                 float* __restrict__ partial)
+                 float* __restrict__ partial, int* __restrict__ next_item)
 {
     constexpr int CL = S::CL, NW = S::NW, R = S::R, C = S::C, PW = S::PW, NR = S::NR, YS = S::YS;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -244,10 +245,9 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     float2* twl = reinterpret_cast<float2*>(smem + (S::DB ? 2 : 1) * S::BUF + S::SCR);
     float* accN = reinterpret_cast<float*>(twl + 16 * 32);
 
+    __shared__ int s_item[2];   // the item rank 0 fetched, by item parity
     cg::cluster_group cluster = cg::this_cluster();
     const int r = (int)cluster.block_rank();
-    const int cid = blockIdx.x / CL;
-    const int ncl = gridDim.x / CL;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m = lane >> 1, p = lane & 1;
     float2* scr = scr_all + warp * FSCR;
@@ -256,8 +256,18 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     for (int i = tid; i < 16 * 32; i += S::THR) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
     __syncthreads();
 
-    int par = 0;   // column-buffer parity (double buffering)
-    for (int it = cid; it < nitems; it += ncl) {
+    int par = 0;    // column-buffer parity (double buffering)
+    int ipar = 0;   // s_item parity
+    for (;;) {
+        // Items are taken in order from one counter, so clusters that become
+        // resident late (SMs held by concurrent kernels) simply take fewer.
+        // Each s_item slot is rewritten two items later, after a cluster
+        // barrier that every peer reaches only once it has read the slot.
+        if (r == 0 && tid == 0) s_item[ipar] = atomicAdd(next_item, 1);
+        cluster.sync();
+        const int it = *cluster.map_shared_rank(&s_item[ipar], 0);
+        ipar ^= 1;
+        if (it >= nitems) break;
         const int4 item = items[it];   // (image, first tile, end tile, item index)
         const FusedTab im = imgs[item.x];
         float acc[NR][16];
@@ -533,36 +543,38 @@ cudaError_t fused_clusters_of(int shape, int* n)
 
 // Host launcher.  descs/items/first/inv are device arrays prepared by the caller.
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
-                         int nitems, const int* first, const float* inv, int nimg, const float* taper,
-                         const float2* tw, float* partial, float* raw, int nclusters, int shape,
-                         cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
+                         int nitems, const int* first, const float* inv, int img0, int nimg,
+                         const float* taper, const float2* tw, float* partial, float* raw, int* next_item,
+                         int nclusters, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
 {
     if (nclusters < 1) nclusters = 1;
-    k_block_sums<<<dim3(max_blocks, nimg), 256, 0, st>>>(reinterpret_cast<const FusedTab*>(descs), bsum_out);
+    k_block_sums<<<dim3(max_blocks, nimg), 256, 0, st>>>(reinterpret_cast<const FusedTab*>(descs) + img0,
+                                                          bsum_out + img0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(next_item, 0, sizeof(int), st)) != cudaSuccess) return e;
     if (ev0 && (e = cudaEventRecord(ev0, st)) != cudaSuccess) return e;
     cudaLaunchAttribute attr[1];
     if (shape == 16) {
         if ((e = prepare_kernel<Shape16>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape16>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16>, reinterpret_cast<const FusedTab*>(descs), items,
-                               nitems, taper, tw, partial);
+                               nitems, taper, tw, partial, next_item);
     } else if (shape == 816) {
         if ((e = prepare_kernel<Shape8W16>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape8W16>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape8W16>, reinterpret_cast<const FusedTab*>(descs),
-                               items, nitems, taper, tw, partial);
+                               items, nitems, taper, tw, partial, next_item);
     } else {
         if ((e = prepare_kernel<Shape8>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape8>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape8>, reinterpret_cast<const FusedTab*>(descs), items,
-                               nitems, taper, tw, partial);
+                               nitems, taper, tw, partial, next_item);
     }
     if (e != cudaSuccess) return e;
     if (ev1 && (e = cudaEventRecord(ev1, st)) != cudaSuccess) return e;
     dim3 g((FCX * FT + 255) / 256, nimg);
-    k_item_reduce<<<g, 256, 0, st>>>(partial, first, inv, raw);
+    k_item_reduce<<<g, 256, 0, st>>>(partial, first + img0, inv + img0, raw);
     return cudaGetLastError();
 }
 
@@ -596,6 +608,7 @@ struct NaMeta {
     int4 items[kNaMaxItems];
     int first[2];
     float inv[1];
+    int next_item;
 };
 constexpr size_t kNaBytes = kNaMetaOff + ((sizeof(NaMeta) + 255) / 256) * 256;
 
@@ -706,11 +719,11 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
         return GCF_ERR_CUDA;
     int ncl = clusters < nitems ? clusters : nitems;
     cudaError_t e = launch_fused(&dmeta->desc, dmeta->bsum_ptr, (ntx + 1) * (nty + 1), dmeta->items,
-                                 nitems, dmeta->first, dmeta->inv, 1,
+                                 nitems, dmeta->first, dmeta->inv, 0, 1,
                                  reinterpret_cast<const float*>(base + kNaTaperOff),
                                  reinterpret_cast<const float2*>(base + kNaTwOff),
-                                 reinterpret_cast<float*>(base), dev_raw_out, ncl, g_na_shape[dev], st,
-                                 nullptr, nullptr);
+                                 reinterpret_cast<float*>(base), dev_raw_out, &dmeta->next_item, ncl,
+                                 g_na_shape[dev], st, nullptr, nullptr);
     if (e != cudaSuccess) return GCF_ERR_CUDA;
     // a copy from pageable memory has consumed `meta` when cudaMemcpyAsync returns
     return GCF_OK;

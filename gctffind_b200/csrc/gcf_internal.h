@@ -137,12 +137,16 @@ struct FusedImageDesc {          // layout must match FusedTab in gcf_fused.cu
 int fused_tile_supported(int tile);
 cudaError_t fused_max_clusters(int* n, int* shape);
 cudaError_t fused_clusters_of(int shape, int* n);   // shape 8, 816 or 16
-// items: (image, first tile, end tile, item index); first[img]..first[img+1]
-// are the items of image img; inv[img] = 1 / tiles of img.
+// Spectra of images img0 .. img0 + nimg - 1 of descs/bsum_out/first/inv.
+// items: the nitems work items of those images, (image, first tile, end
+// tile, item index into partial); first[img]..first[img+1] are the items of
+// image img; inv[img] = 1 / tiles of img; raw: the spectrum of image img0;
+// next_item: one device int, the launch's item counter (zeroed on st).
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
-                         int nitems, const int* first, const float* inv, int nimg, const float* taper,
-                         const float2* tw, float* partial, float* raw, int nclusters, int shape,
-                         cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
+                         int nitems, const int* first, const float* inv, int img0, int nimg,
+                         const float* taper, const float2* tw, float* partial, float* raw, int* next_item,
+                         int nclusters, int shape, cudaStream_t st, cudaEvent_t ev0 = nullptr,
+                         cudaEvent_t ev1 = nullptr);
 
 // gcf_post.cu
 void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,
