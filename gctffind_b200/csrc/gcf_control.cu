@@ -477,21 +477,28 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
             acs[c] = s_cs;
             acc[c] = s_cc;
         }
+        // warp sums of the 2 * kEvalCB values by recursive halving: at each
+        // stage a lane keeps the half of its values selected by one lane bit
+        // and adds the partner's copy of that half, so lane l ends with the
+        // warp total of value l (31 shuffles instead of 5 per value)
+        static_assert(2 * kEvalCB == 32, "one value per lane");
+        float v[32];
 #pragma unroll
         for (int c = 0; c < kEvalCB; ++c) {
+            v[2 * c] = acs[c];
+            v[2 * c + 1] = acc[c];
+        }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                acs[c] += __shfl_xor_sync(0xffffffffu, acs[c], o);
-                acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+        for (int h = 16; h > 0; h >>= 1) {
+            const bool up = (lane & h) != 0;
+#pragma unroll
+            for (int i = 0; i < h; ++i) {
+                float send = up ? v[i] : v[i + h];
+                float keep = up ? v[i + h] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
             }
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int c = 0; c < kEvalCB; ++c) {
-                red[warp][2 * c] = acs[c];
-                red[warp][2 * c + 1] = acc[c];
-            }
-        }
+        red[warp][lane] = v[0];
         __syncthreads();
         if (threadIdx.x < kEvalCB) {
             int c = c0 + threadIdx.x;

@@ -115,13 +115,27 @@ __global__ void k_bg_vertical(const float* __restrict__ raw, const double* __res
 }
 
 // Mean and second moment of each half spectrum (Util/GCalcMoment2D.cu:10-58).
-__global__ void k_moments(const float* __restrict__ spect, int n, double* __restrict__ out2)
+// One block per spectrum; each thread keeps eight loads in flight.
+__global__ void __launch_bounds__(1024) k_moments(const float* __restrict__ spect, int n,
+                                                  double* __restrict__ out2)
 {
     __shared__ double sh[64];
     int m = blockIdx.x;
     const float* p = spect + (size_t)m * n;
+    const int S = blockDim.x;
     double v[2] = {0.0, 0.0};
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int i = threadIdx.x;
+    for (; i + 7 * S < n; i += 8 * S) {
+        double a[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = p[i + k * S];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            v[0] += a[k];
+            v[1] += a[k] * a[k];
+        }
+    }
+    for (; i < n; i += S) {
         double a = p[i];
         v[0] += a;
         v[1] += a * a;
@@ -202,18 +216,20 @@ __global__ void k_lp_extract(const float* __restrict__ ctf0, const float* __rest
 
 // GRadialAvg (FindCTF/GRadialAvg.cu:11-33) with the nearest-pixel sample
 // table precomputed on the host.
+// One warp per radius: the lanes stride over the ring's samples.
 __global__ void k_radial(const float* __restrict__ spect, int cmp_n, int cx,
                          const int* __restrict__ off, const int* __restrict__ pix,
                          float* __restrict__ radial)
 {
-    int m = blockIdx.x;
+    int m = blockIdx.y;
+    int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= cx) return;
     const float* p = spect + (size_t)m * cmp_n;
-    for (int r = threadIdx.x; r < cx; r += blockDim.x) {
-        double s = 0.0;
-        int a = off[r], b = off[r + 1];
-        for (int k = a; k < b; ++k) s += p[pix[k]];
-        radial[(size_t)m * cx + r] = (float)(s / (b - a));
-    }
+    double s = 0.0;
+    int a = off[r], b = off[r + 1];
+    for (int k = a + lane; k < b; k += 32) s += p[pix[k]];
+    s = warp_sum(s);
+    if (lane == 0) radial[(size_t)m * cx + r] = (float)(s / (b - a));
 }
 
 // Spectrum of each job gathered in band order, and its sum of squares.
@@ -229,7 +245,22 @@ __global__ void k_band_gather(const float* __restrict__ ctf, int cmp_n,
     const float* src = ctf + (size_t)jb.mic * cmp_n;
     float* dst = band_spec + spec_off[j];
     double v[1] = {0.0};
-    for (int k = threadIdx.x; k < b.n; k += blockDim.x) {
+    const int S = blockDim.x;
+    int k = threadIdx.x;
+    for (; k + 3 * S < b.n; k += 4 * S) {   // four gathers in flight per thread
+        int q[4];
+        float s[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = b.idx[k + u * S];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u] = src[q[u]];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            dst[k + u * S] = s[u];
+            v[0] += (double)s[u] * (double)s[u];
+        }
+    }
+    for (; k < b.n; k += S) {
         float s = src[b.idx[k]];
         dst[k] = s;
         v[0] += (double)s * (double)s;
@@ -390,7 +421,7 @@ void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic
 
 void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st)
 {
-    k_moments<<<nmic, 512, 0, st>>>(spect, n, out2);
+    k_moments<<<nmic, 1024, 0, st>>>(spect, n, out2);
 }
 
 void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStream_t st)
@@ -418,7 +449,8 @@ void launch_radial(const float* spect, int tile, int nmic, const int* off, const
                    float* radial, cudaStream_t st)
 {
     int cx = tile / 2 + 1;
-    k_radial<<<nmic, 256, 0, st>>>(spect, cx * tile, cx, off, pix, radial);
+    dim3 grid((cx + 7) / 8, nmic);
+    k_radial<<<grid, 256, 0, st>>>(spect, cx * tile, cx, off, pix, radial);
 }
 
 void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, const BandDev* bands,
@@ -426,7 +458,7 @@ void launch_band_gather(const float* ctf, int cmp_n, const SearchJob* jobs, cons
                         cudaStream_t st)
 {
     if (njobs <= 0) return;
-    k_band_gather<<<njobs, 512, 0, st>>>(ctf, cmp_n, jobs, bands, spec_off, band_spec, sum_ss);
+    k_band_gather<<<njobs, 1024, 0, st>>>(ctf, cmp_n, jobs, bands, spec_off, band_spec, sum_ss);
 }
 
 void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_of,
