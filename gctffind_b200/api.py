@@ -33,7 +33,7 @@ EXPORTS = [
     "gcf_get_spect_size", "gcf_get_half_spectrum", "gcf_gen_full_spectrum",
     "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
-    "gcf_get_stage_times", "gcf_get_launch_count", "gcf_avg_spectrum_noalloc",
+    "gcf_get_stage_times", "gcf_get_launch_count", "gcf_get_search_counts", "gcf_avg_spectrum_noalloc",
     "gcf_write_ctf_file",
     "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_mrc_write.argtypes = [C.c_char_p, vp, i, i, i, f]
     L.gcf_get_stage_times.argtypes = [vp, C.POINTER(f)]
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.gcf_get_search_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
     L.gcf_background1d.argtypes = [vp, vp, i, i, vp, C.POINTER(i)]
@@ -348,6 +349,12 @@ class Context:
         _check(self.L.gcf_get_stage_times(self._h, t), self._h)
         keys = ["upload", "tile_kernel", "spectrum", "post", "search1d", "search2d", "total"]
         return dict(zip(keys, list(t)))
+
+    def search_counts(self):
+        """Search work of the last batched call (gcf_get_search_counts)."""
+        c = (C.c_longlong * 4)()
+        _check(self.L.gcf_get_search_counts(self._h, c), self._h)
+        return dict(zip(["cand2d", "pairs2d", "cand1d", "pairs1d"], list(c)))
 
     def launch_count(self) -> int:
         v = C.c_longlong()

@@ -85,6 +85,10 @@ struct gcf_ctx {
     std::string err;
     long long launches = 0;
     float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    // candidates evaluated: 2D candidates, 2D (candidate, band pixel) pairs,
+    // 1D grid points, 1D (grid point, bin) pairs; reset like stage_ms
+    long long search_counts[4] = {0, 0, 0, 0};
+    DBuf<int> d_counts;
     cudaEvent_t ev[8] = {};
     std::vector<cudaEvent_t> kev;   // begin/end pairs around fused tile-kernel launches
     int kev_used = 0;
@@ -796,13 +800,24 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
         CKL();
         ctx->launches += 3;
     }
-    launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->st);
+    CK(ctx->d_counts.ensure(3 * (size_t)nj));
+    launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->d_counts.p, ctx->st);
     CKL();
     ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[7], ctx->st));
     CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost,
                        ctx->st));
+    std::vector<int> cnt(3 * (size_t)nj);
+    CK(cudaMemcpyAsync(cnt.data(), ctx->d_counts.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    for (int j = 0; j < nj; ++j) {
+        const long long n2 = cnt[3 * j], n1 = cnt[3 * j + 1], p1 = cnt[3 * j + 2];
+        ctx->search_counts[0] += n2;
+        ctx->search_counts[1] += n2 * (long long)ctx->bands[jh[j].band]->n;
+        ctx->search_counts[2] += n1;
+        ctx->search_counts[3] += p1;
+    }
     float t1 = 0, t2 = 0;
     cudaEventElapsedTime(&t1, ctx->ev[5], ctx->ev[6]);
     cudaEventElapsedTime(&t2, ctx->ev[6], ctx->ev[7]);
@@ -1131,6 +1146,7 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->part.release();
     ctx->d_res.release();
     ctx->d_optics.release();
+    ctx->d_counts.release();
     ctx->tw512.release();
     ctx->f_desc.release();
     ctx->f_items.release();
@@ -1718,6 +1734,7 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
         if (!images[i]) return GCF_ERR_INVALID_ARG;
     CKS(set_device(ctx));
     for (float& t : ctx->stage_ms) t = 0.0f;
+    for (long long& c : ctx->search_counts) c = 0;
     ctx->kev_used = 0;
     ctx->launches = 0;
     cudaEvent_t t0, t1;
@@ -1779,6 +1796,7 @@ gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_devi
     }
     CKS(set_device(ctx));
     for (float& t : ctx->stage_ms) t = 0.0f;
+    for (long long& c : ctx->search_counts) c = 0;
     ctx->kev_used = 0;
     ctx->launches = 0;
     cudaEvent_t t0, t1;
@@ -1819,6 +1837,13 @@ gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7])
 {
     if (!ctx || !times_ms) return GCF_ERR_INVALID_ARG;
     for (int i = 0; i < 7; ++i) times_ms[i] = ctx->stage_ms[i];
+    return GCF_OK;
+}
+
+gcf_status gcf_get_search_counts(gcf_ctx* ctx, long long counts[4])
+{
+    if (!ctx || !counts) return GCF_ERR_INVALID_ARG;
+    for (int i = 0; i < 4; ++i) counts[i] = ctx->search_counts[i];
     return GCF_OK;
 }
 

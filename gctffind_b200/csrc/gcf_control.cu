@@ -357,6 +357,7 @@ __device__ void update_job(int j, SearchJob* __restrict__ jobs, const BandDev* _
     __syncthreads();
     m = block_argmax(m, shm);
     if (threadIdx.x == 0) {
+        sJ.n_cand2d += n;
         finish_step(sJ, m.i >= 0 ? m.v : (float)-1e20, m.i, s_cc0, vj);
         s_n = advance(sJ, vj);
         sJ.ncand = s_n;
@@ -534,6 +535,7 @@ struct Bins1D {
 
 struct Brute {
     float df, ph, cc;
+    int n;   // grid points evaluated
 };
 
 __device__ Brute brute_1d(const Bins1D& B, int lo_bin, int hi_bin, double ss, const PixOptics& o,
@@ -581,7 +583,7 @@ __device__ Brute brute_1d(const Bins1D& B, int lo_bin, int hi_bin, double ss, co
     }
     __syncthreads();
     m = block_argmax(m, shm);
-    Brute r{0.0f, 0.0f, (float)-1e20};
+    Brute r{0.0f, 0.0f, (float)-1e20, npts};
     if (m.i >= 0) {
         int f = m.i % ndf, p = m.i / ndf;
         float ph = phr[0] + p * pss;
@@ -646,7 +648,7 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     if (sJ.mode == 3) {
         // CFindCtf1D::Refine1D (FindCTF/CFindCtf1D.cpp:58-67): refine pass only,
         // around the given defocus and the current extra phase
-        b1 = Brute{sJ.r1d_df, ext, 0.0f};
+        b1 = Brute{sJ.r1d_df, ext, 0.0f, 0};
         range = sJ.r1d_range;
     } else {
         float dfr[2] = {3000.0f * px2, 30000.0f * px2};
@@ -666,6 +668,10 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     phr2[0] = fmaxf(b1.ph - pr / 2, 0.0f);
     phr2[1] = fminf(0.0f + pr, 150.0f);   // the reference reads the zero-initialised bound
     Brute b2 = brute_1d(B, lo_bin, hi_bin, ss, o, dfr2, phr2, shm);
+    if (threadIdx.x == 0) {
+        sJ.n_cand1d += b1.n + b2.n;
+        sJ.n_pairs1d += (b1.n + b2.n) * max(hi_bin - lo_bin, 0);
+    }
     if (sJ.mode >= 2) {   // Do1D / Refine1D alone: no 2D search follows
         if (threadIdx.x == 0) {
             sJ.df_1d = b2.df;
@@ -735,11 +741,16 @@ __global__ void k_shell_select(SearchJob* __restrict__ jobs, int njobs, const fl
 // CFindCtf2D::mGetResults (FindCTF/CFindCtf2D.cpp:68-76) and the getters
 // of CFindDefocus2D (FindCTF/CFindDefocus2D.cpp:38-68).
 __global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const int* __restrict__ lowpassed,
-                          gcf_result* __restrict__ out)
+                          gcf_result* __restrict__ out, int* __restrict__ counts)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     const SearchJob& J = jobs[j];
+    if (counts) {
+        counts[3 * j] = J.n_cand2d;
+        counts[3 * j + 1] = J.n_cand1d;
+        counts[3 * j + 2] = J.n_pairs1d;
+    }
     gcf_result r;
     if (J.mode >= 2) {   // CFindCtf1D results: m_fDfMin = m_fDfMax = 1D defocus
         r.df_min = J.df_1d;
@@ -799,11 +810,11 @@ void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, in
     k_shell_select<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, cc, cx, cy);
 }
 
-void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out,
+void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out, int* counts,
                     cudaStream_t st)
 {
     if (njobs <= 0) return;
-    k_results<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, lowpassed, out);
+    k_results<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, lowpassed, out, counts);
 }
 
 }  // namespace gcf

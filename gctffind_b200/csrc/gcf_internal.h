@@ -81,7 +81,9 @@ struct SearchJob {
     float df_1d, phase_1d, score_1d;
     float ctf_res;
     int lowpassed;
-    int pad1[3];
+    // work done: 2D candidates evaluated (each over the whole band), 1D grid
+    // points evaluated, and 1D (grid point, bin) pairs
+    int n_cand2d, n_cand1d, n_pairs1d;
 };
 
 // Per-band device pointers (structure of arrays).
@@ -177,7 +179,8 @@ void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, fl
                      float2* cval, cudaStream_t st);
 void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, int cy,
                          cudaStream_t st);
-void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out,
+// counts (nullable): per job n_cand2d, n_cand1d, n_pairs1d
+void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out, int* counts,
                     cudaStream_t st);
 
 // gcf_background.cu: GBackground1D

@@ -284,13 +284,23 @@ gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height,
                                     float* dev_raw_out, void* cuda_stream);
 
 /* Device time (ms, CUDA events on the context streams) of the stages of the
- * last batched call: [0] upload of host inputs (it overlaps [2]), [1] the
- * fused tile-spectrum kernel launches alone (inside [2]; 0 for the cuFFT
- * variant), [2] rescale + tile spectra, [3] background + lowpass + radial,
- * [4] 1D search, [5] 2D search, [6] total. */
+ * last batched call: [0] upload of host inputs (it overlaps [2]), [1] time
+ * in which fused tile-spectrum launches ran (the union of their intervals,
+ * inside [2]; 0 for the cuFFT variant), [2] rescale + tile spectra,
+ * [3] background + lowpass + radial, [4] 1D search, [5] 2D search,
+ * [6] total. */
 gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7]);
 /* Number of kernels this library launched in the last batched call. */
 gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);
+/* Search work counted on the device since the last gcf_run_series /
+ * gcf_run_batch began (single-micrograph calls add to it): [0] 2D candidates
+ * evaluated (each is one GCalcCTF2D + GCC2D evaluation of the reference,
+ * FindCTF/CFindDefocus2D.cpp:363-380), [1] 2D (candidate, in-band pixel)
+ * pairs, [2] 1D grid points (CFindDefocus1D::mBrutalForceSearch,
+ * FindCTF/CFindDefocus1D.cpp:76-119), [3] 1D (grid point, bin) pairs.
+ * The pair counts are the multiply-adds of model x spectrum: twice them is
+ * the candidate contraction's algorithmic flop count. */
+gcf_status gcf_get_search_counts(gcf_ctx* ctx, long long counts[4]);
 
 #ifdef __cplusplus
 }

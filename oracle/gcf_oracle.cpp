@@ -32,6 +32,7 @@
 #include "gcf_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -50,6 +51,10 @@ typedef std::complex<double> cd;
 /* ------------------------------------------------------------------------ */
 /* FFT: iterative radix-2 for powers of two, Bluestein chirp-z otherwise.   */
 /* ------------------------------------------------------------------------ */
+// Work counters (test instrumentation): 2D candidates and 1D grid points
+// evaluated since the last orc_counts(..., reset = 1).
+static std::atomic<long long> g_cand2d{0}, g_cand1d{0};
+
 namespace {
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
@@ -686,6 +691,7 @@ struct Search2D {
     /* Evaluate a line of candidates in parallel, return CCs in order. */
     std::vector<float> eval(const std::vector<Cand>& c)
     {
+        g_cand2d += (long long)c.size();
         std::vector<float> out(c.size());
 #pragma omp parallel for schedule(dynamic, 1)
         for (int i = 0; i < (int)c.size(); ++i) out[i] = corr(c[i].dfmean, c[i].ast, c[i].ang, c[i].phase);
@@ -843,6 +849,7 @@ struct Search2D {
     void iterate()  // mIterate, :153-183
     {
         cc_max = corr(df_mean, ast_ratio, ast_angle, ext_phase);
+        g_cand2d += 1;
         float old = cc_max;
         find_astig();
         if (old > cc_max) return;
@@ -944,6 +951,7 @@ void brute_1d(const double* radial, int cx, const PixOptics& o, const float res_
     if (pss == 0) nps = 1;
     else nps = (int)(psr / pss) / 2 * 2 + 1;
     int npts = ndf * nps;
+    g_cand1d += npts;
     float res1 = ((cx - 1) * 2) * o.px;
     float lo = res1 / res_range[0], hi = res1 / res_range[1];
     std::vector<float> cc(npts), dfv(npts), phv(npts);
@@ -1308,5 +1316,15 @@ extern "C" void orc_remove_bg2d(float* spec, int tile, const float* bg, int bg_n
             int ir = (int)r;
             *v -= bg[ir] * (ir + 1 - r) + bg[ir + 1] * (r - ir);
         }
+    }
+}
+
+extern "C" void orc_counts(long long out[2], int reset)
+{
+    out[0] = g_cand2d.load();
+    out[1] = g_cand1d.load();
+    if (reset) {
+        g_cand2d = 0;
+        g_cand1d = 0;
     }
 }

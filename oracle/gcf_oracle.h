@@ -127,6 +127,10 @@ int  orc_background1d(const float* spec, int n, float* bg, int* start);
 void orc_remove_bg1d(float* spec, int n, const float* bg, int bg_n, int start);
 void orc_remove_bg2d(float* spec, int tile, const float* bg, int bg_n, int start);
 
+/* Work counters: out[0] = 2D candidates (GCC2D evaluations), out[1] = 1D
+ * grid points evaluated since the last reset; reset != 0 zeroes them. */
+void orc_counts(long long out[2], int reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,8 @@ def lib():
                              C.POINTER(OrcParams), C.POINTER(C.c_int), C.c_int,
                              C.POINTER(OrcResult)]
     L.orc_series.restype = C.c_int
+    L.orc_counts.argtypes = [C.POINTER(C.c_longlong), C.c_int]
+    L.orc_counts.restype = None
     _lib = L
     return L
 
@@ -275,3 +277,10 @@ def remove_bg2d(half, bg, start):
     sp = np.array(half, np.float32)
     lib().orc_remove_bg2d(sp, sp.shape[0], np.ascontiguousarray(bg, np.float32), len(bg), int(start))
     return sp
+
+
+def counts(reset: bool = True):
+    """(2D candidates, 1D grid points) evaluated since the last reset."""
+    c = (C.c_longlong * 2)()
+    lib().orc_counts(c, 1 if reset else 0)
+    return int(c[0]), int(c[1])

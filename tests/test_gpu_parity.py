@@ -112,6 +112,31 @@ def test_do2d_search_on_oracle_spectrum(case, oracle):
     _assert_result_close(r, s, df_tol=25.0, ang_tol=1.0, cc_tol=2e-4)
 
 
+def test_search_counts_match_oracle(case, oracle):
+    """gcf_get_search_counts: the 1D grid points and 2D candidates a Do2D
+    evaluates on the device equal the oracle's count of GCC1D / GCC2D
+    evaluations on the same spectrum (exactly when both searches end on the
+    same grid point; the line-search windows follow the running best)."""
+    ctx = case["ctx"]
+    ctx.set_phase(0.0, 0.0)
+    c0 = ctx.search_counts()
+    r = ctx.do2d()
+    c1 = ctx.search_counts()
+    d = {k: c1[k] - c0[k] for k in c0}
+    oracle.counts(reset=True)
+    s = oracle.search(ctx.half_spectrum(raw=False).astype(np.float64), PX, case["p"])
+    o2d, o1d = oracle.counts(reset=True)
+    assert d["cand1d"] == o1d > 0
+    assert d["pairs1d"] > d["cand1d"]
+    assert d["cand2d"] > 2601                          # the 51 x 51 astigmatism grid and more
+    assert d["pairs2d"] % d["cand2d"] == 0             # every candidate covers the whole band
+    same = (r.df_min, r.df_max, r.azimuth, r.ext_phase) == (s.df_min, s.df_max, s.azimuth, s.ext_phase)
+    if same:
+        assert d["cand2d"] == o2d
+    else:
+        assert abs(d["cand2d"] - o2d) <= 0.02 * o2d
+
+
 def test_refine_matches_oracle(case, oracle):
     ctx = case["ctx"]
     rin = [15100.0, 7550.0, 0.01, 0.04, 10.0, 30.0, 0.0, 0.0]

@@ -239,3 +239,18 @@ def test_background1d_known_answers(oracle):
     assert np.all(bg[:st] == 0)
     r = oracle.remove_bg1d(sp, bg, st)
     assert np.all(r[:st] == 0) and np.allclose(r[st:], sp[st:] - bg[st:])
+
+
+def test_work_counters():
+    """orc_counts: the 1D grid points of Do1D (coarse and refine passes) are
+    counted, and a reset zeroes the counters."""
+    import numpy as np
+    from oracle import oracle as O
+    rng = np.random.default_rng(5)
+    ctf = rng.random((256, 129)) - 0.5
+    p = O.params(pixel_size=1.35, tile_size=256)
+    O.counts(reset=True)
+    O.search1d(ctf, 1.35, p)
+    c2, c1 = O.counts(reset=True)
+    assert c2 == 0 and c1 > 501           # two brute-force passes of up to 501 points
+    assert O.counts(reset=False) == (0, 0)
