@@ -55,6 +55,17 @@ __device__ float4 cand_params(const Cand& c, const PixOptics& o)
     return q;
 }
 
+// rintf(t) for |t| < 2^22 with two FP32 additions, which run on the FMA
+// pipe rather than the transcendental unit that the sine needs: t + 1.5*2^23
+// lies in [2^23, 2^24), where floats are the integers, so the addition
+// rounds t to the nearest integer (ties to even, as rintf) and the
+// subtraction is exact.  The CTF phase in turns stays within a few hundred.
+__device__ __forceinline__ float rint_small(float t)
+{
+    const float M = 12582912.0f;   // 1.5 * 2^23
+    return __fsub_rn(__fadd_rn(t, M), M);
+}
+
 // Candidate i of the pending step of job J.
 __device__ Cand cand_of(const SearchJob& J, int i, const float2* cval)
 {
@@ -469,7 +480,7 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
             for (int k = 0; k < kEvalPPT; ++k) {
                 float df = fmaf(ps[k], q.z, fmaf(pc[k], q.y, q.x));
                 float t = fmaf(pa[k], df, pd[k]) + q.w;
-                float r = t - rintf(t);
+                float r = t - rint_small(t);
                 float sv = __sinf(r * 3.14159265358979f);
                 float C = fmaf(fabsf(sv), pe[k], ph[k]);   // (|sin| - 1/2) * env
                 s_cs = fmaf(C, pv[k], s_cs);
@@ -567,7 +578,7 @@ __device__ Brute brute_1d(const Bins1D& B, int lo_bin, int hi_bin, double ss, co
         float cs = 0.f, cc = 0.f;
         for (int x = lo_bin + lane; x < hi_bin; x += 32) {
             float t = B.a[x] * pdf + B.d[x] + tw;
-            float r = t - rintf(t);
+            float r = t - rint_small(t);
             float sv = __sinf(r * 3.14159265358979f);
             float C = (fabsf(sv) - 0.5f) * B.env[x];
             cs += C * B.s[x];
