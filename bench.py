@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--n-tilts", type=int, default=N_TILTS)
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trace", default=None,
+                    help="after the timed steps, record one device-resident step with the CUDA "
+                         "activity tracer (torch.profiler) and write a Chrome trace here")
     return ap.parse_args()
 
 
@@ -350,6 +353,15 @@ def main():
     e2e = world * args.n_tilts / (t_e2e / 1000.0)
     h2d = sum(int(im.numel()) * 4 for im in imgs)
     d2h = args.n_tilts * 40
+
+    if args.trace and rank == 0:
+        # kernel start/end times on every stream, recorded without serialising
+        # the launches (unlike ncu): shows how the searches overlap the tiles
+        from torch.profiler import profile, ProfilerActivity
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            ctx.run_series(imgs, op, order, is_tomo=True)
+            torch.cuda.synchronize()
+        prof.export_chrome_trace(args.trace)
 
     # ---- roofline of the dominant kernel: the fused tile-spectrum kernel.
     # In a series step its launches share the GPU with the searches, so it is
