@@ -21,7 +21,7 @@ namespace gcf {
 
 constexpr int kMaxCand = 2624;        // >= 51 * 51 astigmatism grid
 constexpr int kEvalThreads = 256;     // threads of the candidate kernel
-constexpr int kEvalPPT = 8;           // band pixels per thread per chunk
+constexpr int kEvalPPT = 6;           // band pixels per thread per chunk
 constexpr int kEvalChunk = kEvalThreads * kEvalPPT;
 constexpr int kEvalCB = 16;           // candidates per CTA
 constexpr int kMax1DBins = 1025;      // tile <= 2048
