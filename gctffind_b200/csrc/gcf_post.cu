@@ -57,61 +57,94 @@ __device__ __forceinline__ float bg_val(const float* row, const float* mrow, int
     return (u >= 0) ? row[u] : mrow[-u];
 }
 
+// Rows per block of the horizontal box sums (powers of two, so that the
+// 256 threads split evenly over the rows).
+__host__ __device__ constexpr int bg_rows_per_block(int tile)
+{
+    return tile <= 512 ? 8 : tile <= 1024 ? 4 : tile <= 2048 ? 2 : 1;
+}
+
 // Horizontal box sums of sqrt(raw) (or raw if log_spect) for every row and
-// every output column x in [0, cx).
-__global__ void k_bg_horizontal(const float* __restrict__ raw, int tile, int log_spect, int box,
-                                double* __restrict__ hsum)
+// every output column x in [0, cx).  A block holds bg_rows_per_block rows
+// and their mirror rows; each thread sums the box at the first column of
+// its run of consecutive columns and slides it over the rest (add the
+// entering, subtract the leaving value), in FP64.
+__global__ void __launch_bounds__(256) k_bg_horizontal(const float* __restrict__ raw, int tile, int log_spect,
+                                                       int box, double* __restrict__ hsum)
 {
     extern __shared__ float sh[];
-    int cx = tile / 2 + 1, half_x = cx - 1;
-    int R = blockIdx.x, m = blockIdx.y;
-    int mr = (tile - R) % tile;   // half_y - (R - half_y) modulo tile
+    const int cx = tile / 2 + 1, half_x = cx - 1;
+    const int RB = bg_rows_per_block(tile), tpr = blockDim.x / RB;
+    const int r0 = blockIdx.x * RB, m = blockIdx.y;
     const float* src = raw + (size_t)m * cx * tile;
-    float* row = sh;
-    float* mrow = sh + cx;
-    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
+    for (int i = threadIdx.x; i < RB * cx; i += blockDim.x) {
+        const int rr = i / cx, x = i - rr * cx, R = r0 + rr;
+        if (R >= tile) continue;
+        const int mr = (tile - R) % tile;   // half_y - (R - half_y) modulo tile
         float a = src[(size_t)R * cx + x], b = src[(size_t)mr * cx + x];
-        row[x] = log_spect ? a : sqrtf(a);
-        mrow[x] = log_spect ? b : sqrtf(b);
+        sh[rr * 2 * cx + x] = log_spect ? a : sqrtf(a);
+        sh[rr * 2 * cx + cx + x] = log_spect ? b : sqrtf(b);
     }
     __syncthreads();
-    int hb = box / 2;
-    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
-        double s = 0.0;
-        for (int j = -hb; j <= hb; ++j) s += (double)bg_val(row, mrow, x + j, half_x, tile);
-        hsum[((size_t)m * tile + R) * cx + x] = s;
+    const int rr = threadIdx.x / tpr, t = threadIdx.x - rr * tpr, R = r0 + rr;
+    if (rr >= RB || R >= tile) return;
+    const float* row = sh + rr * 2 * cx;
+    const float* mrow = row + cx;
+    const int seg = (cx + tpr - 1) / tpr;
+    const int x0 = t * seg, x1 = min(cx, x0 + seg);
+    if (x0 >= x1) return;
+    const int hb = box / 2;
+    double* out = hsum + ((size_t)m * tile + R) * cx;
+    double sum = 0.0;
+    for (int j = -hb; j <= hb; ++j) sum += (double)bg_val(row, mrow, x0 + j, half_x, tile);
+    out[x0] = sum;
+    for (int x = x0 + 1; x < x1; ++x) {
+        sum += (double)bg_val(row, mrow, x + hb, half_x, tile) - (double)bg_val(row, mrow, x - 1 - hb, half_x, tile);
+        out[x] = sum;
     }
 }
 
 // Vertical box sums, DC mask (fR < 0.04) and subtraction
-// (FindCTF/GRmBackground2D.cu:18-31, :67-69).
-__global__ void k_bg_vertical(const float* __restrict__ raw, const double* __restrict__ hsum,
-                              int tile, int log_spect, int box, float* __restrict__ ctf)
+// (FindCTF/GRmBackground2D.cu:18-31, :67-69).  A block covers kBgSegY rows
+// of every column; each thread slides the vertical box down its column.
+constexpr int kBgSegY = 16;
+__global__ void __launch_bounds__(256) k_bg_vertical(const float* __restrict__ raw, const double* __restrict__ hsum,
+                                                     int tile, int log_spect, int box, float* __restrict__ ctf)
 {
-    int cx = tile / 2 + 1, cy = tile;
-    int m = blockIdx.y;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= cx * cy) return;
-    int y = i / cx, x = i - y * cx;
-    int yr = y - cy / 2;
-    size_t base = (size_t)m * cx * cy;
-    float fr = x * 0.5f / (cx - 1);
-    fr = sqrtf(fr * fr + yr * yr / (float)(cy * cy));
-    if ((double)fr < 0.04) {
-        ctf[base + i] = 0.0f;
-        return;
+    const int cx = tile / 2 + 1, cy = tile;
+    const int m = blockIdx.y;
+    const int y0 = blockIdx.x * kBgSegY, y1 = min(cy, y0 + kBgSegY);
+    const size_t base = (size_t)m * cx * cy;
+    const int hb = box / 2;
+    const double norm = (double)box * (double)box;
+    for (int x = threadIdx.x; x < cx; x += blockDim.x) {
+        double sum = 0.0;
+        for (int k = -hb; k <= hb; ++k) {
+            int yy = y0 + k;
+            if (yy < 0) yy += cy;
+            else if (yy >= cy) yy -= cy;
+            sum += hsum[base + (size_t)yy * cx + x];
+        }
+        for (int y = y0; y < y1; ++y) {
+            if (y > y0) {
+                int yin = y + hb, yout = y - 1 - hb;
+                if (yin >= cy) yin -= cy;
+                if (yout < 0) yout += cy;
+                sum += hsum[base + (size_t)yin * cx + x] - hsum[base + (size_t)yout * cx + x];
+            }
+            const int i = y * cx + x;
+            const int yr = y - cy / 2;
+            float fr = x * 0.5f / (cx - 1);
+            fr = sqrtf(fr * fr + yr * yr / (float)(cy * cy));
+            if ((double)fr < 0.04) {
+                ctf[base + i] = 0.0f;
+                continue;
+            }
+            double b = sum / norm;
+            if (!log_spect) b *= b;
+            ctf[base + i] = (float)((double)raw[base + i] - b);
+        }
     }
-    int hb = box / 2;
-    double s = 0.0;
-    for (int k = -hb; k <= hb; ++k) {
-        int yy = y + k;
-        if (yy < 0) yy += cy;
-        else if (yy >= cy) yy -= cy;
-        s += hsum[base + (size_t)yy * cx + x];
-    }
-    s /= (double)box * (double)box;
-    if (!log_spect) s *= s;
-    ctf[base + i] = (float)((double)raw[base + i] - s);
 }
 
 // Mean and second moment of each half spectrum (Util/GCalcMoment2D.cu:10-58).
@@ -400,10 +433,9 @@ void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, d
     if (box > (0.3f * tile)) box = (int)(0.3f * tile);
     box = box / 2 * 2 + 1;
     if (box < 7) box = 7;
-    int cx = tile / 2 + 1;
-    int th = cx < 256 ? ((cx + 31) / 32) * 32 : 256;
-    dim3 grid(tile, nmic);
-    k_bg_horizontal<<<grid, th, 2 * cx * sizeof(float), st>>>(raw, tile, log_spect, box, hsum);
+    int cx = tile / 2 + 1, rb = bg_rows_per_block(tile);
+    dim3 grid((tile + rb - 1) / rb, nmic);
+    k_bg_horizontal<<<grid, 256, 2 * rb * cx * sizeof(float), st>>>(raw, tile, log_spect, box, hsum);
 }
 
 void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic, int log_spect,
@@ -414,9 +446,10 @@ void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic
     if (box > (0.3f * tile)) box = (int)(0.3f * tile);
     box = box / 2 * 2 + 1;
     if (box < 7) box = 7;
-    int n = (tile / 2 + 1) * tile;
-    dim3 grid((n + 255) / 256, nmic);
-    k_bg_vertical<<<grid, 256, 0, st>>>(raw, hsum, tile, log_spect, box, ctf);
+    int cx = tile / 2 + 1;
+    int th = cx < 256 ? ((cx + 31) / 32) * 32 : 256;
+    dim3 grid((tile + kBgSegY - 1) / kBgSegY, nmic);
+    k_bg_vertical<<<grid, th, 0, st>>>(raw, hsum, tile, log_spect, box, ctf);
 }
 
 void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st)
