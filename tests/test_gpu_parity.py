@@ -295,3 +295,25 @@ def test_series_host_and_device_inputs_agree(gpu_lib):
         assert [a.df_min, a.df_max, a.azimuth, a.ext_phase, a.score] == \
             [b.df_min, b.df_max, b.azimuth, b.ext_phase, b.score]
     assert np.array_equal(fh, fd)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_short_series_host_and_device_inputs_agree(gpu_lib, n):
+    """Series of 1 to 3 packages: the device path splits a series into the
+    first package and two halves (empty for n < 3) and the host path into
+    upload chunks; both must give the same rows."""
+    import torch
+    G = gpu_lib
+    tilts = [3.0 * (k - n // 2) for k in range(n)]
+    imgs = [_img(seed=70 + k, w=1024, h=1024, df=(15000.0 + 40 * k, 15400.0 + 40 * k), tilt=t)
+            for k, t in enumerate(tilts)]
+    so = G.series_order(tilts)
+    op = G.make_optics(pixel_size=PX)
+    ctx = G.Context(0, 512, 0)
+    rh = ctx.run_series(imgs, op, so.order, is_tomo=True)
+    rd = ctx.run_series([torch.from_numpy(a).cuda() for a in imgs], op, so.order, is_tomo=True)
+    ctx.close()
+    for a, b in zip(rh, rd):
+        assert [a.df_min, a.df_max, a.azimuth, a.ext_phase, a.score] == \
+            [b.df_min, b.df_max, b.azimuth, b.ext_phase, b.score]
+        assert abs(a.df_min - 15000.0) < 600.0
