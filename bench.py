@@ -395,7 +395,8 @@ def main():
     sec = kern_ms / 1000.0
     achieved = algo_bytes / sec / 1e9 if sec > 0 else 0.0
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # nominal FP32 FMA rate at max clock
-    roof = {"kernel": "k_fused_spectrum (one launch over all tiles of the series, timed alone)",
+    roof = {"kernel": "k_fused_spectrum (8-CTA clusters) + k_fused_spectrum_solo (the SMs the clusters leave "
+                      "free): one launch pair over all tiles of the series, timed alone",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": pk.get("hbm_gbs"),
             "unit": "GB/s", "frac": round(achieved / pk.get("hbm_gbs", 6650.0), 4),
             "traffic": TILE_KERNEL_TRAFFIC_PER_MICROGRAPH * args.n_tilts if TILE_KERNEL_TRAFFIC_PER_MICROGRAPH else None,

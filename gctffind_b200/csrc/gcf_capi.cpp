@@ -128,7 +128,14 @@ struct gcf_ctx {
     DBuf<int4> f_items;
     DBuf<int> f_first;
     DBuf<float> f_inv, f_partial;
-    DBuf<int> f_next;   // item counters of the tile kernel launches
+    DBuf<unsigned long long> f_next;   // item queues of the tile kernel launches
+    // cluster-less tile CTAs beside each cluster launch (SMs the clusters
+    // leave free) and their global scratch
+    int solo_n = -1;
+    cudaStream_t st_solo = nullptr;
+    cudaEvent_t solo_fork = nullptr, solo_join = nullptr;
+    DBuf<float2> solo_col;
+    DBuf<float> solo_acc;
     DBuf<double> f_bsum;
     DBuf<double*> f_bsum_ptr;
     std::vector<int> f_first_h;    // host copy of f_first for the current plan
@@ -542,7 +549,42 @@ gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
 // m0) on stream st.  Launches of disjoint ranges share the plan's buffers
 // (each range owns its items, partial spectra and item counter), so they
 // may run concurrently once the plan's uploads are done.
-gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream_t st)
+// The cluster-less CTAs beside a cluster launch: one per SM that the
+// clusters leave free, with their scratch (set up on first use; 1.5 MB of
+// global memory per CTA, L2-resident while it works).  Their launches all
+// go to st_solo, so launches of two chunks never share the scratch at once.
+gcf_status solo_setup(gcf_ctx* ctx, SoloLaunch* sl)
+{
+    if (ctx->solo_n < 0) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->dev));
+        const int per_cluster = ctx->fused_shape == 16 ? 16 : 8;
+        ctx->solo_n = std::max(0, sms - ctx->fused_clusters * per_cluster);
+        if (ctx->solo_n > 0 && !ctx->st_solo) {
+            int lo = 0, hi = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CK(cudaStreamCreateWithPriority(&ctx->st_solo, cudaStreamNonBlocking, hi));
+            CK(cudaEventCreateWithFlags(&ctx->solo_fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->solo_join, cudaEventDisableTiming));
+        }
+        if (ctx->solo_n > 0) {
+            CK(ctx->solo_col.ensure(solo_scratch_float2(ctx->solo_n)));
+            CK(ctx->solo_acc.ensure(solo_scratch_floats(ctx->solo_n)));
+        }
+    }
+    sl->n = ctx->solo_n;
+    // they stop taking items when <= 10 items per cluster remain (6 and 10
+    // measured alike on the 41-micrograph series, 14 slower)
+    sl->reserve_per_cluster = 10;
+    sl->st = ctx->st_solo;
+    sl->col = ctx->solo_col.p;
+    sl->acc = ctx->solo_acc.p;
+    sl->fork = ctx->solo_fork;
+    sl->join = ctx->solo_join;
+    return GCF_OK;
+}
+
+gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream_t st, bool solo = true)
 {
     const std::vector<int>& first = ctx->f_first_h;
     if (m0 < 0 || m1 > (int)first.size() - 1 || m0 >= m1) return fail(ctx, GCF_ERR_STATE, "tile-spectrum range outside the plan");
@@ -558,10 +600,12 @@ gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream
     }
     cudaEvent_t e0 = ctx->kev[ctx->kev_used], e1 = ctx->kev[ctx->kev_used + 1];
     ctx->kev_used += 2;
+    SoloLaunch sl{};
+    if (solo) CKS(solo_setup(ctx, &sl));
     CK(launch_fused(ctx->f_desc.p, ctx->f_bsum_ptr.p, max_blocks, ctx->f_items.p + first[m0], ni, ctx->f_first.p,
                     ctx->f_inv.p, m0, m1 - m0, ctx->taper.p, ctx->tw512.p, ctx->f_partial.p, raw_out,
-                    ctx->f_next.p + m0, ncl, ctx->fused_shape, st, e0, e1));
-    ctx->launches += 3;
+                    ctx->f_next.p + m0, ncl, ctx->fused_shape, st, e0, e1, solo ? &sl : nullptr));
+    ctx->launches += (solo && sl.n > 0 && ni > ncl) ? 4 : 3;
     return GCF_OK;
 }
 
@@ -1099,6 +1143,7 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->st_copy) cudaStreamSynchronize(ctx->st_copy);
     if (ctx->st_search) cudaStreamSynchronize(ctx->st_search);
+    if (ctx->st_solo) cudaStreamSynchronize(ctx->st_solo);
     if (ctx->st_tile) cudaStreamSynchronize(ctx->st_tile);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
     for (auto* b : ctx->bands) {
@@ -1154,6 +1199,8 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->f_inv.release();
     ctx->f_partial.release();
     ctx->f_next.release();
+    ctx->solo_col.release();
+    ctx->solo_acc.release();
     ctx->f_bsum.release();
     ctx->f_bsum_ptr.release();
     for (auto& ev : ctx->ev)
@@ -1162,6 +1209,9 @@ void gcf_destroy(gcf_ctx* ctx)
     for (auto& ev : ctx->kev) cudaEventDestroy(ev);
     if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
     if (ctx->st_search) cudaStreamDestroy(ctx->st_search);
+    if (ctx->st_solo) cudaStreamDestroy(ctx->st_solo);
+    if (ctx->solo_fork) cudaEventDestroy(ctx->solo_fork);
+    if (ctx->solo_join) cudaEventDestroy(ctx->solo_join);
     if (ctx->st_tile) cudaStreamDestroy(ctx->st_tile);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -1229,6 +1279,7 @@ gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape)
     if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16)) return GCF_ERR_INVALID_ARG;
     ctx->fused_shape_req = shape;
     ctx->fused_clusters = 0;   // recomputed at the next launch
+    ctx->solo_n = -1;
     return GCF_OK;
 }
 

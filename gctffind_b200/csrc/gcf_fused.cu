@@ -19,7 +19,10 @@
 //   |F|     amplitudes (DC moved to row 256) accumulate in registers across
 //           all tiles of a work item and are written once.
 // With CL = 16 the column buffer is double-buffered, so one cluster barrier
-// per tile separates writers from readers.  Work items are (image, tile
+// per tile separates writers from readers.  Beside the cluster launch,
+// k_fused_spectrum_solo runs one CTA on each SM that the clusters leave free
+// (8-CTA clusters fit twice per GPC) and takes items from the back of the
+// same queue.  Work items are (image, tile
 // range) pairs, handed out in order through a counter; their partial
 // spectra are summed in item order by k_item_reduce, so the result does not
 // depend on which cluster took which item.
@@ -208,6 +211,28 @@ __global__ void __launch_bounds__(256) k_block_sums(const FusedTab* __restrict__
     }
 }
 
+// The work-item queue of one launch: a 64-bit counter whose low half counts
+// items taken from the front (by clusters) and whose high half counts items
+// taken from the back (by the cluster-less CTAs).  An index >= nitems means
+// the queue is empty.
+__device__ __forceinline__ int take_front(unsigned long long* q, int nitems)
+{
+    const unsigned long long old = atomicAdd(q, 1ull);
+    const unsigned front = (unsigned)old, back = (unsigned)(old >> 32);
+    return front + back < (unsigned)nitems ? (int)front : nitems;
+}
+// From the back, while more than `reserve` items remain: a cluster-less CTA
+// takes about eight times as long per item as a cluster, so it must not
+// take one of the last items, or it would end the launch late.
+__device__ __forceinline__ int take_back(unsigned long long* q, int nitems, int reserve)
+{
+    const unsigned long long cur = atomicAdd(q, 0ull);
+    if ((long long)nitems - (long long)((unsigned)cur + (unsigned)(cur >> 32)) <= (long long)reserve) return nitems;
+    const unsigned long long old = atomicAdd(q, 1ull << 32);
+    const unsigned front = (unsigned)old, back = (unsigned)(old >> 32);
+    return front + back < (unsigned)nitems ? nitems - 1 - (int)back : nitems;
+}
+
 // Compile-time shape of one cluster configuration.
 template <int CL_, int NW_, bool DB_, bool PF_ = true>
 struct FusedShape {
@@ -236,7 +261,7 @@ template <class S>
 __global__ void __launch_bounds__(S::THR, 1)
 k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ items, int nitems,
                  const float* __restrict__ taper, const float2* __restrict__ twg,
-                 float* __restrict__ partial, int* __restrict__ next_item)
+                 float* __restrict__ partial, unsigned long long* __restrict__ next_item)
 {
     constexpr int CL = S::CL, NW = S::NW, R = S::R, C = S::C, PW = S::PW, NR = S::NR, YS = S::YS;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -263,7 +288,7 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
         // resident late (SMs held by concurrent kernels) simply take fewer.
         // Each s_item slot is rewritten two items later, after a cluster
         // barrier that every peer reaches only once it has read the slot.
-        if (r == 0 && tid == 0) s_item[ipar] = atomicAdd(next_item, 1);
+        if (r == 0 && tid == 0) s_item[ipar] = take_front(next_item, nitems);
         cluster.sync();
         const int it = *cluster.map_shared_rank(&s_item[ipar], 0);
         ipar ^= 1;
@@ -429,6 +454,157 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
     cluster.sync();   // keep shared memory alive until every peer is done
 }
 
+// ---- tiles on the SMs that the clusters leave free --------------------------
+// 8-CTA clusters fit twice per GPC, so some SMs stay idle beside the cluster
+// kernel.  One CTA of this kernel runs on each of them, takes work items
+// from the same counter and transforms whole tiles alone: the row spectra go
+// to the CTA's column buffer in global memory (L2-resident scratch), the
+// column transforms read them back, and the item's |F| sums live in a second
+// global buffer ([column][row]) until the item ends, when they are written
+// to the item's partial spectrum in the cluster kernel's layout.  The
+// transforms, the split and the order of every addition are those of
+// k_fused_spectrum, so an item's partial spectrum does not depend on which
+// kernel took it.
+constexpr int kSoloThreads = 256;
+constexpr int kSoloWarps = kSoloThreads / 32;
+constexpr int kSoloYS = FT + 2;                                      // column stride, float2
+constexpr size_t kSoloColFloat2 = (size_t)(FT / 2) * kSoloYS;        // columns 0..255 of one tile
+constexpr size_t kSoloAccFloats = (size_t)(FT / 2) * FT;             // |F| sums, [column][row]
+constexpr size_t kSoloSmem = (size_t)kSoloWarps * FSCR * sizeof(float2) + 16 * 32 * sizeof(float2) +
+                             FT * sizeof(float);
+
+__global__ void __launch_bounds__(kSoloThreads, 1)
+k_fused_spectrum_solo(const FusedTab* __restrict__ imgs, const int4* __restrict__ items, int nitems,
+                      const float* __restrict__ taper, const float2* __restrict__ twg,
+                      float* __restrict__ partial, unsigned long long* __restrict__ next_item, int reserve,
+                      float2* __restrict__ colg_all, float* __restrict__ accg_all)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* scr_all = reinterpret_cast<float2*>(smem);
+    float2* twl = scr_all + kSoloWarps * FSCR;
+    float* accN = reinterpret_cast<float*>(twl + 16 * 32);
+    __shared__ int s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m = lane >> 1, p = lane & 1;
+    float2* scr = scr_all + warp * FSCR;
+    float2* colg = colg_all + (size_t)blockIdx.x * kSoloColFloat2;
+    float* accg = accg_all + (size_t)blockIdx.x * kSoloAccFloats;
+    for (int i = tid; i < 16 * 32; i += kSoloThreads) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
+    for (;;) {
+        __syncthreads();   // the previous item is written; every thread has read s_item
+        if (tid == 0) s_item = take_back(next_item, nitems, reserve);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 item = items[it];   // (image, first tile, end tile, item index)
+        const FusedTab im = imgs[item.x];
+        for (int i = tid; i < FT; i += kSoloThreads) accN[i] = 0.0f;   // read after the row phase's barrier
+        for (int t = item.y; t < item.z; ++t) {
+            const bool first = t == item.y;
+            const int tx = t % im.ntx, ty = t / im.ntx;
+            const float* src = im.img + (size_t)(im.offy + ty * im.stride) * im.pitch + im.offx + tx * im.stride;
+            const double* bs = im.bsum + (size_t)ty * im.nbx + tx;
+            const float mean = (float)((bs[0] + bs[1] + bs[im.nbx] + bs[im.nbx + 1]) / ((double)FT * FT));
+
+            // ---- row transforms: 256 row pairs, the next pair prefetched --------
+            float na[16], nb[16];
+            {
+                const float* ga = src + (size_t)(2 * warp) * im.pitch;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    na[j] = __ldg(ga + 32 * j + lane);
+                    nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                }
+            }
+            for (int q = 0; q < FT / 2 / kSoloWarps; ++q) {
+                const int Y0 = 2 * (warp + kSoloWarps * q);
+                float ca[16], cb[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    ca[j] = na[j];
+                    cb[j] = nb[j];
+                }
+                if (q + 1 < FT / 2 / kSoloWarps) {
+                    const float* ga = src + (size_t)(Y0 + 2 * kSoloWarps) * im.pitch;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        na[j] = __ldg(ga + 32 * j + lane);
+                        nb[j] = __ldg(ga + im.pitch + 32 * j + lane);
+                    }
+                }
+                float2 v[16];
+                const float* ta = taper + (size_t)Y0 * FT;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    int X = 32 * j + lane;
+                    v[j] = make_float2((ca[j] - mean) * __ldg(ta + X), (cb[j] - mean) * __ldg(ta + FT + X));
+                }
+                fft512_warp(v, scr, twl, lane);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) scr[sslot(m + 16 * k + 256 * p)] = v[P16(k)];
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int K = lane + 32 * i;
+                    float2 zk = scr[sslot(K)], zn = scr[sslot((FT - K) & (FT - 1))];
+                    float4 AB = make_float4(zk.x + zn.x, zk.y - zn.y, zk.y + zn.y, zn.x - zk.x);
+                    if (K == 0) {
+                        float2 zh = scr[sslot(FT / 2)];
+                        AB = make_float4(2.0f * zk.x, 2.0f * zh.x, 2.0f * zk.y, 2.0f * zh.y);
+                    }
+                    *reinterpret_cast<float4*>(colg + (size_t)K * kSoloYS + Y0) = AB;
+                }
+                __syncwarp();
+            }
+            __syncthreads();   // the tile's column buffer is complete
+
+            // ---- column transforms from the global column buffer ----------------
+            for (int cc = 0; cc < FT / 2 / kSoloWarps; ++cc) {
+                const int K = warp + kSoloWarps * cc;   // 0 = packed (0, 256)
+                float2 v[16];
+                const float2* col = colg + (size_t)K * kSoloYS;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = col[32 * j + lane];
+                float* a = accg + (size_t)K * FT;
+                float av[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) av[k] = first ? 0.0f : a[m + 16 * k + 256 * p];
+                fft512_warp(v, scr, twl, lane);
+                if (K != 0) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        float2 z = v[P16(k)];
+                        a[m + 16 * k + 256 * p] = av[k] + amp(z.x, z.y);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) scr[sslot(m + 16 * k + 256 * p)] = v[P16(k)];
+                    __syncwarp();
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        int Kk = m + 16 * k + 256 * p;
+                        float2 zk = v[P16(k)], zn = scr[sslot((FT - Kk) & (FT - 1))];
+                        float ax = 0.5f * (zk.x + zn.x), ay = 0.5f * (zk.y - zn.y);
+                        float bx = 0.5f * (zk.y + zn.y), by = -0.5f * (zk.x - zn.x);
+                        a[Kk] = av[k] + amp(ax, ay);
+                        accN[Kk] += amp(bx, by);
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();   // the column buffer is free again; the sums are complete
+        }
+        // ---- the item's partial spectrum (DC moved to row 256) ------------------
+        float* out = partial + (size_t)item.w * FCX * FT;
+        for (int i = tid; i < (FT / 2) * FT; i += kSoloThreads) {
+            const int kx = i / FT, ky = i - kx * FT;
+            out[(size_t)((ky + FT / 2) & (FT - 1)) * FCX + kx] = accg[i];
+        }
+        for (int ky = tid; ky < FT; ky += kSoloThreads)
+            out[(size_t)((ky + FT / 2) & (FT - 1)) * FCX + FT / 2] = accN[ky];
+    }
+}
+
 // raw[img] = sum of the img's item partials (in item order) / ntiles / 2.
 __global__ void k_item_reduce(const float* __restrict__ partial, const int* __restrict__ first,
                               const float* __restrict__ inv, float* __restrict__ raw)
@@ -542,18 +718,27 @@ cudaError_t fused_clusters_of(int shape, int* n)
 }
 
 // Host launcher.  descs/items/first/inv are device arrays prepared by the caller.
+size_t solo_scratch_float2(int nsolo) { return (size_t)nsolo * kSoloColFloat2; }
+size_t solo_scratch_floats(int nsolo) { return (size_t)nsolo * kSoloAccFloats; }
+
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
                          int nitems, const int* first, const float* inv, int img0, int nimg,
-                         const float* taper, const float2* tw, float* partial, float* raw, int* next_item,
-                         int nclusters, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
+                         const float* taper, const float2* tw, float* partial, float* raw,
+                         unsigned long long* next_item, int nclusters, int shape, cudaStream_t st, cudaEvent_t ev0,
+                         cudaEvent_t ev1, const SoloLaunch* solo)
 {
     if (nclusters < 1) nclusters = 1;
     k_block_sums<<<dim3(max_blocks, nimg), 256, 0, st>>>(reinterpret_cast<const FusedTab*>(descs) + img0,
                                                           bsum_out + img0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(next_item, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(next_item, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
     if (ev0 && (e = cudaEventRecord(ev0, st)) != cudaSuccess) return e;
+    const bool use_solo = solo && solo->n > 0 && nitems > nclusters;
+    if (use_solo) {
+        if ((e = cudaEventRecord(solo->fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(solo->st, solo->fork, 0)) != cudaSuccess) return e;
+    }
     cudaLaunchAttribute attr[1];
     if (shape == 16) {
         if ((e = prepare_kernel<Shape16>()) != cudaSuccess) return e;
@@ -572,6 +757,16 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
                                nitems, taper, tw, partial, next_item);
     }
     if (e != cudaSuccess) return e;
+    if (use_solo) {
+        // after the cluster launch, so that its clusters are placed first and
+        // these CTAs land on the SMs they leave free
+        k_fused_spectrum_solo<<<solo->n, kSoloThreads, kSoloSmem, solo->st>>>(
+            reinterpret_cast<const FusedTab*>(descs), items, nitems, taper, tw, partial, next_item,
+            solo->reserve_per_cluster * nclusters, solo->col, solo->acc);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(solo->join, solo->st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, solo->join, 0)) != cudaSuccess) return e;
+    }
     if (ev1 && (e = cudaEventRecord(ev1, st)) != cudaSuccess) return e;
     dim3 g((FCX * FT + 255) / 256, nimg);
     k_item_reduce<<<g, 256, 0, st>>>(partial, first + img0, inv + img0, raw);
@@ -608,7 +803,7 @@ struct NaMeta {
     int4 items[kNaMaxItems];
     int first[2];
     float inv[1];
-    int next_item;
+    unsigned long long next_item;
 };
 constexpr size_t kNaBytes = kNaMetaOff + ((sizeof(NaMeta) + 255) / 256) * 256;
 

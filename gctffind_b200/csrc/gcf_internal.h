@@ -139,16 +139,30 @@ struct FusedImageDesc {          // layout must match FusedTab in gcf_fused.cu
 int fused_tile_supported(int tile);
 cudaError_t fused_max_clusters(int* n, int* shape);
 cudaError_t fused_clusters_of(int shape, int* n);   // shape 8, 816 or 16
+// CTAs of the cluster-less tile kernel beside a cluster launch (on the SMs
+// the clusters leave free), with their global scratch: col holds
+// solo_scratch_float2(n) float2, acc solo_scratch_floats(n) floats.  fork and
+// join order `st` around the launch on the solo stream.
+struct SoloLaunch {
+    int n;
+    int reserve_per_cluster;   // they stop taking items when <= this x clusters remain
+    cudaStream_t st;
+    float2* col;
+    float* acc;
+    cudaEvent_t fork, join;
+};
+size_t solo_scratch_float2(int nsolo);
+size_t solo_scratch_floats(int nsolo);
 // Spectra of images img0 .. img0 + nimg - 1 of descs/bsum_out/first/inv.
 // items: the nitems work items of those images, (image, first tile, end
 // tile, item index into partial); first[img]..first[img+1] are the items of
 // image img; inv[img] = 1 / tiles of img; raw: the spectrum of image img0;
-// next_item: one device int, the launch's item counter (zeroed on st).
+// next_item: the launch's 64-bit item queue counter (zeroed on st).
 cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blocks, const int4* items,
                          int nitems, const int* first, const float* inv, int img0, int nimg,
-                         const float* taper, const float2* tw, float* partial, float* raw, int* next_item,
-                         int nclusters, int shape, cudaStream_t st, cudaEvent_t ev0 = nullptr,
-                         cudaEvent_t ev1 = nullptr);
+                         const float* taper, const float2* tw, float* partial, float* raw,
+                         unsigned long long* next_item, int nclusters, int shape, cudaStream_t st,
+                         cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, const SoloLaunch* solo = nullptr);
 
 // gcf_post.cu
 void launch_bg_horizontal(const float* raw, int tile, int nmic, int log_spect, double* hsum,
