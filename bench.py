@@ -384,7 +384,7 @@ def main():
     T = 512
     ov = T // 2
     nt1 = ((args.size - ov) // (T - ov)) ** 2            # tiles per micrograph
-    nch = -(-nt1 // 32)                                   # work items per micrograph (32 tiles)
+    nch = -(-nt1 // 24)                                   # work items per micrograph (<= 24 tiles)
     img_bytes = args.n_tilts * 4 * args.size * args.size  # every pixel read once
     part_bytes = args.n_tilts * nch * (T // 2 + 1) * T * 4  # per-item partial spectra written
     algo_bytes = img_bytes + part_bytes

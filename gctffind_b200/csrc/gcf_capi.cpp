@@ -473,7 +473,7 @@ gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
 
 // Work plan of the fused tile-spectrum kernel (tile 512) for mics: image
 // descriptors, block-sum slots and work items, uploaded on ctx->st.  Each
-// micrograph's tiles form runs of at most 32 (an item's |F| sums live in
+// micrograph's tiles form runs of at most 24 (an item's |F| sums live in
 // registers until it ends); the split depends on the micrograph alone, so
 // its spectrum does not depend on the batch or chunk it is in.
 gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
@@ -487,7 +487,10 @@ gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
         ctx->fused_clusters = n;
         ctx->fused_shape = shape;
     }
-    const int kItemTiles = 32;
+    // 24 rather than 32: the cluster-less CTAs then finish their last items
+    // sooner and may keep taking items longer (a 41-tilt series step 12.43
+    // -> 12.21 ms; the spectra change only in the grouping of the sums)
+    const int kItemTiles = 24;
     std::vector<FusedImageDesc> d(nm);
     std::vector<int4> items;
     std::vector<int>& first = ctx->f_first_h;
@@ -573,9 +576,9 @@ gcf_status solo_setup(gcf_ctx* ctx, SoloLaunch* sl)
         }
     }
     sl->n = ctx->solo_n;
-    // they stop taking items when <= 10 items per cluster remain (6 and 10
-    // measured alike on the 41-micrograph series, 14 slower)
-    sl->reserve_per_cluster = 10;
+    // they stop taking items when <= 6 items per cluster remain (with items
+    // of <= 24 tiles; 10 and 14 measured slower)
+    sl->reserve_per_cluster = 6;
     sl->st = ctx->st_solo;
     sl->col = ctx->solo_col.p;
     sl->acc = ctx->solo_acc.p;
