@@ -739,10 +739,20 @@ void refine_init(SearchJob& J, const float* rin)
 
 // Runs the 1D + 2D searches of `specs` on the spectra already in their
 // slots; results in job order.
-gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vector<gcf_result>& out)
+// A search whose launches are enqueued on `st` and whose results have not
+// been read back yet.
+struct SearchPending {
+    int nj = 0;
+    std::vector<int> band;   // band slot of each job
+    cudaStream_t st = nullptr;
+};
+
+gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, SearchPending& pend)
 {
     int nj = (int)specs.size();
-    out.assign(nj, gcf_result{});
+    pend.nj = nj;
+    pend.st = ctx->st;
+    pend.band.assign(nj, 0);
     if (nj == 0) return GCF_OK;
     int T = ctx->tile, cx = T / 2 + 1;
     size_t cmp_n = (size_t)cx * T;
@@ -852,16 +862,24 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     CKL();
     ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[7], ctx->st));
-    CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost,
-                       ctx->st));
+    for (int j = 0; j < nj; ++j) pend.band[j] = jh[j].band;
+    return GCF_OK;
+}
+
+// Reads back the results of an enqueued search (waits for it on the host).
+gcf_status run_search_collect(gcf_ctx* ctx, const SearchPending& pend, std::vector<gcf_result>& out)
+{
+    const int nj = pend.nj;
+    out.assign(nj, gcf_result{});
+    if (nj == 0) return GCF_OK;
+    CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost, pend.st));
     std::vector<int> cnt(3 * (size_t)nj);
-    CK(cudaMemcpyAsync(cnt.data(), ctx->d_counts.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost,
-                       ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpyAsync(cnt.data(), ctx->d_counts.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, pend.st));
+    CK(cudaStreamSynchronize(pend.st));
     for (int j = 0; j < nj; ++j) {
         const long long n2 = cnt[3 * j], n1 = cnt[3 * j + 1], p1 = cnt[3 * j + 2];
         ctx->search_counts[0] += n2;
-        ctx->search_counts[1] += n2 * (long long)ctx->bands[jh[j].band]->n;
+        ctx->search_counts[1] += n2 * (long long)ctx->bands[pend.band[j]]->n;
         ctx->search_counts[2] += n1;
         ctx->search_counts[3] += p1;
     }
@@ -871,6 +889,13 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     ctx->stage_ms[4] += t1;
     ctx->stage_ms[5] += t2;
     return GCF_OK;
+}
+
+gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vector<gcf_result>& out)
+{
+    SearchPending pend;
+    CKS(run_search_enqueue(ctx, specs, pend));
+    return run_search_collect(ctx, pend, out);
 }
 
 gcf_status set_device(gcf_ctx* ctx)
@@ -1690,12 +1715,19 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     return GCF_OK;
 }
 
-// Device images: every chunk's tile spectra are enqueued at once, the
-// chunks alternating between the two high-priority streams (one plan, one
-// upload of the work items); post-processing and the package searches of
-// each finished chunk run on the search stream in the SMs the 8-CTA
-// clusters leave free, so only the last chunk's searches follow the last
-// tile-spectrum launch.
+// Device images: the first package alone, then all others.  With fused
+// spectra both tile launches are enqueued at once (one plan, one upload of
+// the work items) on the two high-priority streams, so the second launch's
+// clusters start while the first package's items finish, and each launch
+// brings its cluster-less CTAs onto the SMs the clusters leave free.  The
+// post-processing and searches of each chunk run on the low-priority search
+// stream when its spectra are done: the first package's full search mostly
+// in the last part of the big launch, when its cluster-less CTAs have
+// stopped, and the other packages' refinements as one batch at the end.
+// (Measured alternatives, all slower on a 41-tilt series: the other packages
+// in two launches with their searches in between; one launch for all; the
+// first package's search started before the big launch's cluster-less CTAs;
+// fewer cluster-less CTAs to leave SMs to that search.)
 gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs, int w, int h,
                              float px, std::vector<MicImage>& mics, SeriesLoop& loop)
 {
@@ -1710,12 +1742,7 @@ gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs
     CKS(spectra_alloc(ctx, n));
     if (rescaled) CK(ctx->rescaled.ensure((size_t)nw * nh * n));
     const bool fused = ctx->impl == GCF_SPECT_FUSED;
-    // the first package alone, then the rest in two halves: the searches of
-    // the first half overlap the tile spectra of the second (finer chunks
-    // measured slower: searches running beside the cluster kernel take SMs
-    // its 8-CTA clusters need)
     std::vector<int> bounds{0, 1};
-    if (fused && n > 2) bounds.push_back(1 + n / 2);
     if (n > 1) bounds.push_back(n);
     const int nchunks = (int)bounds.size() - 1;
     while ((int)ctx->chunk_ev.size() < nchunks + 2) {

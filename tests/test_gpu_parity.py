@@ -300,8 +300,8 @@ def test_series_host_and_device_inputs_agree(gpu_lib):
 @pytest.mark.parametrize("n", [1, 2, 3])
 def test_short_series_host_and_device_inputs_agree(gpu_lib, n):
     """Series of 1 to 3 packages: the device path splits a series into the
-    first package and two halves (empty for n < 3) and the host path into
-    upload chunks; both must give the same rows."""
+    first package and the rest (two tile launches with their cluster-less
+    CTAs) and the host path into upload chunks; both must give the same rows."""
     import torch
     G = gpu_lib
     tilts = [3.0 * (k - n // 2) for k in range(n)]
