@@ -1665,9 +1665,11 @@ std::vector<int> series_chunks(int n)
 }
 
 // Host images: uploads in processing order on the copy stream (the first
-// package alone, then chunks of 8), and after each chunk its spectra,
-// post-processing and package searches, so only the last chunk's work
-// follows the last copy.
+// package alone, then chunks of 8 shrinking towards the end); each chunk's
+// spectra on the high-priority stream as soon as it lands, and its
+// post-processing and package searches on the low-priority search stream
+// once its spectra are done, so only the last chunk's work follows the last
+// copy.
 gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, int w, int h,
                            float px, std::vector<MicImage>& mics, SeriesLoop& loop)
 {
@@ -1682,7 +1684,9 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     CK(ctx->images.ensure((size_t)w * h * n));
     std::vector<int> bounds = series_chunks(n);
     const int nchunks = (int)bounds.size() - 1;
-    while ((int)ctx->chunk_ev.size() < nchunks) {
+    // chunk_ev: [0, nchunks) copies done, [nchunks, 2 nchunks) spectra done,
+    // [2 nchunks] searches done
+    while ((int)ctx->chunk_ev.size() < 2 * nchunks + 1) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->chunk_ev.push_back(e);
@@ -1698,6 +1702,7 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st_copy));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    // every chunk's spectra on st as its copy lands ...
     for (int c = 0; c < nchunks; ++c) {
         const int k0 = bounds[c], k1 = bounds[c + 1];
         CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
@@ -1707,12 +1712,29 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
             CKS(stage_image(ctx, ctx->images.p + cnt * k, w, h, px, dst, mics[k], &used));
         }
         CKS(spectra_chunk(ctx, mics, k0, k1 - k0));
-        CKS(spectra_post(ctx, k1 - k0, k0));
-        CKS(loop.run(k0, k1));
+        CK(cudaEventRecord(ctx->chunk_ev[nchunks + c], ctx->st));
     }
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    return GCF_OK;
+    // ... and its post-processing and package searches on the low-priority
+    // search stream once they are done, so that no chunk's spectra wait for
+    // the searches of the chunks before it
+    auto search_phase = [&]() -> gcf_status {
+        for (int c = 0; c < nchunks; ++c) {
+            const int k0 = bounds[c], k1 = bounds[c + 1];
+            CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[nchunks + c], 0));
+            CKS(spectra_post(ctx, k1 - k0, k0));
+            CKS(loop.run(k0, k1));
+        }
+        return GCF_OK;
+    };
+    std::swap(ctx->st, ctx->st_search);
+    gcf_status st = search_phase();
+    cudaError_t e = cudaEventRecord(ctx->chunk_ev[2 * nchunks], ctx->st);
+    std::swap(ctx->st, ctx->st_search);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[2 * nchunks], 0);
+    if (st == GCF_OK && e != cudaSuccess) st = fail(ctx, GCF_ERR_CUDA, cudaGetErrorString(e));
+    return st;
 }
 
 // Device images: the first package alone, then all others.  With fused
