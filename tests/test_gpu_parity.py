@@ -246,6 +246,31 @@ def test_fused_batch_deterministic(gpu_lib):
         assert x.as_dict() == y.as_dict()
 
 
+def test_cluster_less_ctas_do_not_change_spectra(gpu_lib):
+    """Twelve 4096 x 4096 micrographs (10 work items each) through one
+    gcf_run_batch call: with 120 items in one launch the cluster-less tile
+    CTAs take items from the back of the queue while the clusters take the
+    rest.  Each micrograph alone (10 items, clusters only) must give the same
+    result fields bit for bit, since an item's partial spectrum does not
+    depend on which kernel computed it."""
+    import torch
+    G = gpu_lib
+    n = 12
+    imgs = [torch.from_numpy(_img(seed=90 + i, w=4096, h=4096, df=(14600.0 + 150 * i, 15200.0 + 150 * i),
+                                  az=10.0 * i)).cuda() for i in range(n)]
+    ctx = G.Context(0, 512, 0)
+    op = G.make_optics(pixel_size=PX)
+    batch = ctx.run_batch(imgs, [PX] * n, op)
+    for img, rb in zip(imgs, batch):
+        ctx.setup(op, 4096, 4096)
+        ctx.gen_half_spectrum(img)
+        ctx.set_phase(0.0, 0.0)
+        rs = ctx.do2d()
+        assert [rs.df_min, rs.df_max, rs.azimuth, rs.score, rs.df_1d] == \
+            [rb.df_min, rb.df_max, rb.azimuth, rb.score, rb.df_1d]
+    ctx.close()
+
+
 def _bg_curves(case):
     x = np.arange(257, dtype=np.float64)
     yield (1000 * np.exp(-x / 40) + 50 * np.cos(x / 3) ** 2 + 20).astype(np.float32)
