@@ -42,7 +42,7 @@ METRIC = "4096^2 micrographs/s (tilt series, plain FP32 search)"
 # DRAM bytes (read + write) of one micrograph's share of k_fused_spectrum,
 # from ncu dram__bytes_read.sum + dram__bytes_write.sum on a 3-micrograph
 # launch of the same kernel divided by 3 (profiles/k_fused_spectrum_3x4096.md)
-TILE_KERNEL_TRAFFIC_PER_MICROGRAPH = (320_177_664 + 8_108_032) // 3
+TILE_KERNEL_TRAFFIC_PER_MICROGRAPH = (262_052_608 + 11_340_544) // 3
 
 
 def parse():
