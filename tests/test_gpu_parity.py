@@ -1,7 +1,8 @@
 """GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
 
-Tolerances (north star: averaged spectra within 1e-4 relative, defocus within
-one reference search step, astigmatism angle within 1 degree, CC within 1e-3):
+Tolerances (the path's accuracy bar: averaged spectra within 1e-4 relative,
+defocus within one reference search step, astigmatism angle within 1 degree,
+CC within 1e-3):
   raw averaged spectrum : |gpu - orc| <= 1e-4 * |orc| + 1e-5 * mean(orc) per pixel
   ctf spectrum          : |gpu - orc| <= 1e-4 * rms(orc) per pixel
   radial average        : |gpu - orc| <= 1e-4 * rms(orc) per bin

@@ -14,7 +14,7 @@ library with float32 spectra and FP64 sums, so the two agree to rounding:
                          padding of an in-place C2R, FindCTF/CFindCtfBase.cpp:
                          212-218) that its blur spreads a few pixels inward
   full spectrum        : max |d| <= 5e-3 x rms away from the same border
-  search results       : the north-star bound -- defocus within one search
+  search results       : the path's accuracy bar -- defocus within one search
                          step of the final iteration (max(20 A, range / 31))
                          -> 60 A here, azimuth 1 degree (mod 180) when the
                          astigmatism exceeds 50 A, extra phase 2 degrees,
