@@ -236,6 +236,29 @@ def test_fused_spectrum_matches_oracle_and_cufft(gpu_lib, oracle, w):
     _assert_result_close(r2, ores)
 
 
+def test_largest_frame_matches_oracle(gpu_lib, oracle):
+    """A K3 super-resolution sized frame, 11520 x 8184 at 1.2 A/px (no
+    rescale): 44 x 30 = 1320 tiles in 55 work items of one launch.  The
+    averaged spectrum within the per-pixel tolerance and the Do2D result
+    within one search step of the oracle's."""
+    G = gpu_lib
+    w, h, px = 11520, 8184, 1.2
+    img = _img(seed=61, w=w, h=h, px=px, df=(21800.0, 22300.0), az=35.0, dose=1.5)
+    ctx = G.Context(0, 512, 0)
+    op = G.make_optics(pixel_size=px)
+    ctx.setup(op, w, h)
+    ctx.gen_half_spectrum(img)
+    g = ctx.half_spectrum(raw=True).astype(np.float64)
+    o = oracle.avg_spectrum(img, 512)
+    tol = 1e-4 * np.abs(o) + 1e-5 * o.mean()
+    assert np.all(np.abs(g - o) <= tol), float((np.abs(g - o) / np.abs(o)).max())
+    ctx.set_phase(0.0, 0.0)
+    r = ctx.do2d()
+    ores = oracle.find_ctf_image(img, px, oracle.params(pixel_size=px, tile_size=512))
+    _assert_result_close(r, ores)
+    ctx.close()
+
+
 def test_fused_batch_deterministic(gpu_lib):
     G = gpu_lib
     imgs = [_img(seed=30 + i, w=1024 + 512 * (i % 2), h=1024, df=(15000.0, 15100.0)) for i in range(3)]
