@@ -132,6 +132,7 @@ struct gcf_ctx {
     // cluster-less tile CTAs beside each cluster launch (SMs the clusters
     // leave free) and their global scratch
     int solo_n = -1;
+    int n_sms = 0;   // multiprocessors of the device (0 until first asked)
     cudaStream_t st_solo = nullptr;
     cudaEvent_t solo_fork = nullptr, solo_join = nullptr;
     DBuf<float2> solo_col;
@@ -841,8 +842,16 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     bool any_2d = false;
     for (const JobSpec& s : specs) any_2d = any_2d || s.mode <= 1;
     int pairs = any_2d ? 2 + 19 * ((any_grid ? 2 : 0) + 1 + (any_phase ? 1 : 0)) : 0;
+    // Candidate blocks per (chunk, job) of the line searches (<= 61
+    // candidates, 4 blocks of 16): one block loops over the candidate blocks
+    // it is given, reusing its pixels, so with many jobs fewer y-blocks
+    // (enough for about two waves of 3 CTAs per SM) do the same work without
+    // the blocks that find no candidates and exit.
+    if (ctx->n_sms == 0) CK(cudaDeviceGetAttribute(&ctx->n_sms, cudaDevAttrMultiProcessorCount, ctx->dev));
+    const long long per_y = (long long)nj * max_chunks;
+    const int line_cb = (int)std::min<long long>(4, std::max<long long>(1, (2LL * 3 * ctx->n_sms + per_y - 1) / per_y));
     for (int k = 0; k < pairs; ++k) {
-        int cb = (k == 0) ? 1 : (k == 1 && any_grid) ? (kMaxCand / kEvalCB + 3) / 4 : 4;
+        int cb = (k == 0) ? 1 : (k == 1 && any_grid) ? (kMaxCand / kEvalCB + 3) / 4 : line_cb;
         launch_eval2d(a, cb, max_band, ctx->st);
         CKL();
         ctx->launches += 1;

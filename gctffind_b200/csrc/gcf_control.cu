@@ -66,6 +66,47 @@ __device__ __forceinline__ float rint_small(float t)
     return __fsub_rn(__fadd_rn(t, M), M);
 }
 
+// sin(pi r) and cos(pi r) for |r| <= 1/2 from their Taylor series in r
+// (coefficients (-1)^k pi^n / n!), truncated after r^13 and r^14: the first
+// omitted terms are below (pi/2)^15/15! < 7e-10 and (pi/2)^16/16! < 7e-11,
+// so the Horner evaluation's own float rounding (a few ulp) dominates.  Runs
+// on the FMA pipe only.
+constexpr double kPiD = 3.14159265358979323846;
+constexpr double kPi2D = kPiD * kPiD;
+constexpr float kS1 = (float)kPiD;
+constexpr float kS3 = (float)(-kPiD * kPi2D / 6.0);
+constexpr float kS5 = (float)(kPiD * kPi2D * kPi2D / 120.0);
+constexpr float kS7 = (float)(-kPiD * kPi2D * kPi2D * kPi2D / 5040.0);
+constexpr float kS9 = (float)(kPiD * kPi2D * kPi2D * kPi2D * kPi2D / 362880.0);
+constexpr float kS11 = (float)(-kPiD * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 39916800.0);
+constexpr float kS13 = (float)(kPiD * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 6227020800.0);
+constexpr float kC2 = (float)(-kPi2D / 2.0);
+constexpr float kC4 = (float)(kPi2D * kPi2D / 24.0);
+constexpr float kC6 = (float)(-kPi2D * kPi2D * kPi2D / 720.0);
+constexpr float kC8 = (float)(kPi2D * kPi2D * kPi2D * kPi2D / 40320.0);
+constexpr float kC10 = (float)(-kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 3628800.0);
+constexpr float kC12 = (float)(kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 479001600.0);
+constexpr float kC14 = (float)(-kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 87178291200.0);
+
+__device__ __forceinline__ void sincos_pi_half(float r, float& s, float& c)
+{
+    const float r2 = r * r;
+    float p = fmaf(kS13, r2, kS11);
+    p = fmaf(p, r2, kS9);
+    p = fmaf(p, r2, kS7);
+    p = fmaf(p, r2, kS5);
+    p = fmaf(p, r2, kS3);
+    p = fmaf(p, r2, kS1);
+    s = p * r;
+    float q = fmaf(kC14, r2, kC12);
+    q = fmaf(q, r2, kC10);
+    q = fmaf(q, r2, kC8);
+    q = fmaf(q, r2, kC6);
+    q = fmaf(q, r2, kC4);
+    q = fmaf(q, r2, kC2);
+    c = fmaf(q, r2, 1.0f);
+}
+
 // Candidate i of the pending step of job J.
 __device__ Cand cand_of(const SearchJob& J, int i, const float2* cval)
 {
@@ -437,6 +478,11 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
     const int ncand = jobs[j].ncand;
     const int cand_blocks = (ncand + kEvalCB - 1) / kEvalCB;
     if ((int)blockIdx.y >= cand_blocks) return;
+    // steps whose candidates move one parameter by a fixed step: the mean
+    // defocus, the astigmatism magnitude or the phase (in candidate order),
+    // and the single candidate of CC0
+    const int kind = jobs[j].step;
+    const bool linear = kind == STEP_CC0 || kind == STEP_ASTMAG || kind == STEP_DFMEAN || kind == STEP_PHASE;
     const BandDev b = bands[jobs[j].band];
     const int nchunk = (b.n + kEvalChunk - 1) / kEvalChunk;
     const int p0 = blockIdx.x * kEvalChunk;
@@ -475,6 +521,47 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
         }
         __syncthreads();
         float acs[kEvalCB], acc[kEvalCB];
+        if (linear) {
+            // The block's candidates step one parameter evenly, so t is
+            // t0 + i * dt at every pixel (dt from the block's end points) and
+            // sin(pi t_i) follows from sin and cos of pi t0 and pi dt by
+            // rotation: 4 FMA-pipe operations per pair instead of a sine.
+            // Both angles are reduced to [-pi/2, pi/2] first; shifting dt by
+            // an integer m flips the sign of sin(pi t_i) for odd i * m only,
+            // which |sin| ignores.
+            const int nb = min(kEvalCB, ncand - c0);
+            const float4 q0 = sq[0];
+            float4 dq = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (nb > 1) {
+                const float4 q1 = sq[nb - 1];
+                const float inv = 1.0f / (float)(nb - 1);
+                dq = make_float4((q1.x - q0.x) * inv, (q1.y - q0.y) * inv, (q1.z - q0.z) * inv,
+                                 (q1.w - q0.w) * inv);
+            }
+#pragma unroll
+            for (int c = 0; c < kEvalCB; ++c) {
+                acs[c] = 0.f;
+                acc[c] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kEvalPPT; ++k) {
+                float df = fmaf(ps[k], q0.z, fmaf(pc[k], q0.y, q0.x));
+                float t = fmaf(pa[k], df, pd[k]) + q0.w;
+                float dt = fmaf(pa[k], fmaf(ps[k], dq.z, fmaf(pc[k], dq.y, dq.x)), dq.w);
+                float s, co, sd, cd;
+                sincos_pi_half(t - rint_small(t), s, co);
+                sincos_pi_half(dt - rint_small(dt), sd, cd);
+#pragma unroll
+                for (int c = 0; c < kEvalCB; ++c) {
+                    float C = fmaf(fabsf(s), pe[k], ph[k]);
+                    acs[c] = fmaf(C, pv[k], acs[c]);
+                    acc[c] = fmaf(C, C, acc[c]);
+                    float sn = fmaf(s, cd, co * sd);
+                    co = fmaf(co, cd, -(s * sd));
+                    s = sn;
+                }
+            }
+        } else {
 #pragma unroll
         for (int c = 0; c < kEvalCB; ++c) {
             const float4 q = sq[c];
@@ -491,6 +578,7 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
             }
             acs[c] = s_cs;
             acc[c] = s_cc;
+        }
         }
         // warp sums of the 2 * kEvalCB values by recursive halving: at each
         // stage a lane keeps the half of its values selected by one lane bit

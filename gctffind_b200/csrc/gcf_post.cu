@@ -106,9 +106,12 @@ __global__ void __launch_bounds__(256) k_bg_horizontal(const float* __restrict__
 
 // Vertical box sums, DC mask (fR < 0.04) and subtraction
 // (FindCTF/GRmBackground2D.cu:18-31, :67-69).  A block covers kBgSegY rows
-// of every column; each thread slides the vertical box down its column.
+// of every column; each thread slides the vertical box down its column (one
+// column per thread up to tile 1024: the block has cx threads rounded up to
+// whole warps, at most kBgVertThreads).
 constexpr int kBgSegY = 16;
-__global__ void __launch_bounds__(256) k_bg_vertical(const float* __restrict__ raw, const double* __restrict__ hsum,
+constexpr int kBgVertThreads = 544;
+__global__ void k_bg_vertical(const float* __restrict__ raw, const double* __restrict__ hsum,
                                                      int tile, int log_spect, int box, float* __restrict__ ctf)
 {
     const int cx = tile / 2 + 1, cy = tile;
@@ -447,7 +450,7 @@ void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic
     box = box / 2 * 2 + 1;
     if (box < 7) box = 7;
     int cx = tile / 2 + 1;
-    int th = cx < 256 ? ((cx + 31) / 32) * 32 : 256;
+    int th = std::min(kBgVertThreads, ((cx + 31) / 32) * 32);
     dim3 grid((tile + kBgSegY - 1) / kBgSegY, nmic);
     k_bg_vertical<<<grid, th, 0, st>>>(raw, hsum, tile, log_spect, box, ctf);
 }
