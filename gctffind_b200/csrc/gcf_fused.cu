@@ -52,12 +52,18 @@ constexpr int FCX = FT / 2 + 1;  // 257 half-spectrum columns
 constexpr int FSCR = 16 * 34;    // per-warp scratch, float2 units
 constexpr int FROW = 34;         // transpose row stride: 64-bit accesses of either side hit distinct banks
 
+// Complex products stay scalar: a packed form needs one factor's halves
+// swapped or broadcast into a register pair, and those moves measured
+// slower than the four scalar operations.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex additions as packed two-float operations (one f32x2 instruction
+// each; exact IEEE round-to-nearest like the scalar pair): halves the issue
+// slots of the butterflies.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 
 // Forward 4-point DFT in place (W4 = -i).
 __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3)
@@ -66,8 +72,9 @@ __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2&
     float2 s13 = cadd(a1, a3), d13 = csub(a1, a3);
     a0 = cadd(s02, s13);
     a2 = csub(s02, s13);
-    a1 = make_float2(d02.x + d13.y, d02.y - d13.x);   // d02 - i d13
-    a3 = make_float2(d02.x - d13.y, d02.y + d13.x);   // d02 + i d13
+    const float2 sw = make_float2(d13.y, d13.x);
+    a1 = __ffma2_rn(sw, make_float2(1.0f, -1.0f), d02);   // d02 - i d13
+    a3 = __ffma2_rn(sw, make_float2(-1.0f, 1.0f), d02);   // d02 + i d13
 }
 
 // exp(-2 pi i m / 16) for the compile-time products m = n2 * k1 <= 9
@@ -147,7 +154,7 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
         float2 o;
         o.x = __shfl_xor_sync(0xffffffffu, u.x, 1);
         o.y = __shfl_xor_sync(0xffffffffu, u.y, 1);
-        v[P16(k)] = make_float2(fmaf(sg, u.x, o.x), fmaf(sg, u.y, o.y));
+        v[P16(k)] = __ffma2_rn(make_float2(sg, sg), u, o);
     }
     __syncwarp();
 }
