@@ -88,6 +88,28 @@ constexpr float kC10 = (float)(-kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 3628800.
 constexpr float kC12 = (float)(kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 479001600.0);
 constexpr float kC14 = (float)(-kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D * kPi2D / 87178291200.0);
 
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// sincos_pi_half on a packed pair of arguments
+__device__ __forceinline__ void sincos_pi_half2(float2 r, float2& s, float2& c)
+{
+    const float2 r2 = __fmul2_rn(r, r);
+    float2 p = __ffma2_rn(f2(kS13), r2, f2(kS11));
+    p = __ffma2_rn(p, r2, f2(kS9));
+    p = __ffma2_rn(p, r2, f2(kS7));
+    p = __ffma2_rn(p, r2, f2(kS5));
+    p = __ffma2_rn(p, r2, f2(kS3));
+    p = __ffma2_rn(p, r2, f2(kS1));
+    s = __fmul2_rn(p, r);
+    float2 q = __ffma2_rn(f2(kC14), r2, f2(kC12));
+    q = __ffma2_rn(q, r2, f2(kC10));
+    q = __ffma2_rn(q, r2, f2(kC8));
+    q = __ffma2_rn(q, r2, f2(kC6));
+    q = __ffma2_rn(q, r2, f2(kC4));
+    q = __ffma2_rn(q, r2, f2(kC2));
+    c = __ffma2_rn(q, r2, f2(1.0f));
+}
+
 __device__ __forceinline__ void sincos_pi_half(float r, float& s, float& c)
 {
     const float r2 = r * r;
@@ -526,8 +548,10 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
             // t0 + i * dt at every pixel (dt from the block's end points) and
             // sin(pi t_i) follows from sin and cos of pi t0 and pi dt by
             // rotation: 4 FMA-pipe operations per pair instead of a sine.
-            // Both angles are reduced to [-pi/2, pi/2] first; shifting dt by
-            // an integer m flips the sign of sin(pi t_i) for odd i * m only,
+            // Two chains, seeded at candidates 0 and 8, advance as one
+            // packed f32x2 pair (7 rotations each instead of 15).  All
+            // angles are reduced to [-pi/2, pi/2] first; shifting dt by an
+            // integer m flips the sign of sin(pi t_i) for odd i * m only,
             // which |sin| ignores.
             const int nb = min(kEvalCB, ncand - c0);
             const float4 q0 = sq[0];
@@ -538,28 +562,41 @@ k_eval2d(SearchJob* __restrict__ jobs, const BandDev* __restrict__ bands, const 
                 dq = make_float4((q1.x - q0.x) * inv, (q1.y - q0.y) * inv, (q1.z - q0.z) * inv,
                                  (q1.w - q0.w) * inv);
             }
+            constexpr int H = kEvalCB / 2;
+            float2 as2[H], ac2[H];
 #pragma unroll
-            for (int c = 0; c < kEvalCB; ++c) {
-                acs[c] = 0.f;
-                acc[c] = 0.f;
+            for (int c = 0; c < H; ++c) {
+                as2[c] = f2(0.f);
+                ac2[c] = f2(0.f);
             }
 #pragma unroll
             for (int k = 0; k < kEvalPPT; ++k) {
                 float df = fmaf(ps[k], q0.z, fmaf(pc[k], q0.y, q0.x));
                 float t = fmaf(pa[k], df, pd[k]) + q0.w;
                 float dt = fmaf(pa[k], fmaf(ps[k], dq.z, fmaf(pc[k], dq.y, dq.x)), dq.w);
-                float s, co, sd, cd;
-                sincos_pi_half(t - rint_small(t), s, co);
+                float t8 = fmaf((float)H, dt, t);
+                float2 s2, c2;
+                sincos_pi_half2(make_float2(t - rint_small(t), t8 - rint_small(t8)), s2, c2);
+                float sd, cd;
                 sincos_pi_half(dt - rint_small(dt), sd, cd);
+                const float2 cd2 = f2(cd), sd2 = f2(sd), nsd2 = f2(-sd);
+                const float2 e2 = f2(pe[k]), h2 = f2(ph[k]), v2 = f2(pv[k]);
 #pragma unroll
-                for (int c = 0; c < kEvalCB; ++c) {
-                    float C = fmaf(fabsf(s), pe[k], ph[k]);
-                    acs[c] = fmaf(C, pv[k], acs[c]);
-                    acc[c] = fmaf(C, C, acc[c]);
-                    float sn = fmaf(s, cd, co * sd);
-                    co = fmaf(co, cd, -(s * sd));
-                    s = sn;
+                for (int c = 0; c < H; ++c) {
+                    float2 C = __ffma2_rn(make_float2(fabsf(s2.x), fabsf(s2.y)), e2, h2);
+                    as2[c] = __ffma2_rn(C, v2, as2[c]);
+                    ac2[c] = __ffma2_rn(C, C, ac2[c]);
+                    float2 sn = __ffma2_rn(s2, cd2, __fmul2_rn(c2, sd2));
+                    c2 = __ffma2_rn(c2, cd2, __fmul2_rn(s2, nsd2));
+                    s2 = sn;
                 }
+            }
+#pragma unroll
+            for (int c = 0; c < H; ++c) {
+                acs[c] = as2[c].x;
+                acs[c + H] = as2[c].y;
+                acc[c] = ac2[c].x;
+                acc[c + H] = ac2[c].y;
             }
         } else {
 #pragma unroll
