@@ -52,12 +52,20 @@ constexpr int FCX = FT / 2 + 1;  // 257 half-spectrum columns
 constexpr int FSCR = 16 * 34;    // per-warp scratch, float2 units
 constexpr int FROW = 34;         // transpose row stride: 64-bit accesses of either side hit distinct banks
 
-// Complex products stay scalar: a packed form needs one factor's halves
-// swapped or broadcast into a register pair, and those moves measured
-// slower than the four scalar operations.
+// Complex product, scalar.  The per-lane twiddles (read from shared
+// memory) use it: a packed form with the twiddle stored pre-arranged
+// (wx, wx, -wy, wy) measured slower, with twice the shared-memory reads.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// Complex product by a compile-time or constant-bank twiddle w as two packed
+// operations: a * w = (a.x, a.y) (wx, wx) + (a.y, a.x) (-wy, wy).  (The form
+// with a's halves broadcast, (a.x, a.x) w + (a.y, a.y) (-wy, wx), measured
+// slower.)
+__device__ __forceinline__ float2 cmul_k(float2 a, float2 w)
+{
+    return __ffma2_rn(make_float2(a.y, a.x), make_float2(-w.y, w.y), __fmul2_rn(a, make_float2(w.x, w.x)));
 }
 // Complex additions as packed two-float operations (one f32x2 instruction
 // each; exact IEEE round-to-nearest like the scalar pair): halves the issue
@@ -120,7 +128,7 @@ __device__ __forceinline__ void dft16(float2 (&v)[16])
 #pragma unroll
         for (int n2 = 1; n2 < 4; ++n2) {
             if (n2 * k1 == 4) v[4 * k1 + n2] = make_float2(v[4 * k1 + n2].y, -v[4 * k1 + n2].x);   // * (-i)
-            else v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w16(n2 * k1));
+            else v[4 * k1 + n2] = cmul_k(v[4 * k1 + n2], w16(n2 * k1));
         }
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) dft4(v[4 * k1 + 0], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
@@ -149,7 +157,7 @@ __device__ __forceinline__ void fft512_warp(float2 (&v)[16], float2* scr, const 
     const float sg = p ? -1.0f : 1.0f;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        float2 u = cmul(c_tw32[k], v[P16(k)]);
+        float2 u = cmul_k(v[P16(k)], c_tw32[k]);
         if (!p) u = v[P16(k)];
         float2 o;
         o.x = __shfl_xor_sync(0xffffffffu, u.x, 1);
