@@ -131,6 +131,8 @@ struct gcf_ctx {
     DBuf<unsigned long long> f_next;   // item queues of the tile kernel launches
     // cluster-less tile CTAs beside each cluster launch (SMs the clusters
     // leave free) and their global scratch
+    DBuf<double> lp_g;   // lowpass filter per half-spectrum bin, for tile lp_g_tile
+    int lp_g_tile = 0;
     int solo_n = -1;
     int n_sms = 0;   // multiprocessors of the device (0 until first asked)
     cudaStream_t st_solo = nullptr;
@@ -678,7 +680,13 @@ gcf_status spectra_post(gcf_ctx* ctx, int nm, int first = 0)
         return fail(ctx, GCF_ERR_CUFFT, "cufftSetStream (lowpass) failed");
     if (cufftExecR2C(pf, ctx->lpfull.p, (cufftComplex*)ctx->lpcmp.p) != CUFFT_SUCCESS)
         return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (lowpass) failed");
-    launch_lp_filter(ctx->lpcmp.p, T, nm, 10.0, ctx->st);
+    if (ctx->lp_g_tile != T) {   // filter table of this tile size (B-factor 10)
+        CK(ctx->lp_g.ensure((size_t)cx * T));
+        launch_lp_table(ctx->lp_g.p, T, 10.0, ctx->st);
+        CKL();
+        ctx->lp_g_tile = T;
+    }
+    launch_lp_filter(ctx->lpcmp.p, T, nm, ctx->lp_g.p, ctx->st);
     CKL();
     if (cufftExecC2R(pi, (cufftComplex*)ctx->lpcmp.p, ctx->lpfull.p) != CUFFT_SUCCESS)
         return fail(ctx, GCF_ERR_CUFFT, "cufftExecC2R (lowpass) failed");

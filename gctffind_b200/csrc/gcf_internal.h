@@ -172,7 +172,8 @@ void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic
 void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st);
 // lowpass of CFindCtfBase::mLowpass around a batched R2C / C2R pair
 void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStream_t st);
-void launch_lp_filter(float2* cmp, int tile, int nmic, double bfactor, cudaStream_t st);
+void launch_lp_table(double* g, int tile, double bfactor, cudaStream_t st);
+void launch_lp_filter(float2* cmp, int tile, int nmic, const double* g, cudaStream_t st);
 void launch_lp_extract(const float* ctf0, const float* full, int tile, int nmic, const double* moments,
                        float* out, int* lowpassed, cudaStream_t st);
 void launch_radial(const float* spect, int tile, int nmic, const int* off, const int* pix,

@@ -211,16 +211,26 @@ __global__ void k_lp_full(const float* __restrict__ ctf0, int tile, float* __res
     full[(size_t)m * tile * tile + i] = full_val(ctf0 + (size_t)m * cx * tile, tile, y, X);
 }
 
-__global__ void k_lp_filter(float2* __restrict__ cmp, int tile, double bfactor)
+// The filter depends on the tile size and B-factor only: one table per
+// context, shared by every micrograph (the same double expression per bin).
+__global__ void k_lp_table(double* __restrict__ g, int tile, double bfactor)
 {
-    int m = blockIdx.y;
     int cx = tile / 2 + 1;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cx * tile) return;
     int y = i / cx, x = i - y * cx;
     int ky = (y > tile / 2) ? y - tile : y;
     double scale = -bfactor / ((double)tile * tile + (double)tile * tile);
-    double g = exp(scale * ((double)x * x + (double)ky * ky)) / ((double)tile * tile);
+    g[i] = exp(scale * ((double)x * x + (double)ky * ky)) / ((double)tile * tile);
+}
+
+__global__ void k_lp_filter(float2* __restrict__ cmp, int tile, const double* __restrict__ gtab)
+{
+    int m = blockIdx.y;
+    int cx = tile / 2 + 1;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cx * tile) return;
+    double g = gtab[i];
     float2 v = cmp[(size_t)m * cx * tile + i];
     cmp[(size_t)m * cx * tile + i] = make_float2((float)(v.x * g), (float)(v.y * g));
 }
@@ -466,11 +476,17 @@ void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStre
     k_lp_full<<<grid, 256, 0, st>>>(ctf0, tile, full);
 }
 
-void launch_lp_filter(float2* cmp, int tile, int nmic, double bfactor, cudaStream_t st)
+void launch_lp_table(double* g, int tile, double bfactor, cudaStream_t st)
+{
+    int n = (tile / 2 + 1) * tile;
+    k_lp_table<<<(n + 255) / 256, 256, 0, st>>>(g, tile, bfactor);
+}
+
+void launch_lp_filter(float2* cmp, int tile, int nmic, const double* g, cudaStream_t st)
 {
     int n = (tile / 2 + 1) * tile;
     dim3 grid((n + 255) / 256, nmic);
-    k_lp_filter<<<grid, 256, 0, st>>>(cmp, tile, bfactor);
+    k_lp_filter<<<grid, 256, 0, st>>>(cmp, tile, g);
 }
 
 void launch_lp_extract(const float* ctf0, const float* full, int tile, int nmic, const double* moments,
