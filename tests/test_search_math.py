@@ -7,11 +7,12 @@ so the kernel forms sin(pi t_i) by rotation instead of one hardware sine per
 Taylor series (coefficients (-1)^k pi^n / n!, truncated after r^13 and r^14),
 and each further candidate costs one complex rotation by pi dt; two chains,
 seeded at candidates 0 and 8 of a 16-candidate block, advance side by side.
-This test restates that arithmetic in float32, with each fused multiply-add
-rounded once (float64 product and sum, then one rounding: exact for these
-float32 operands), and checks it against float64 sines: the seed within a few
-float32 ulps, and |sin| along a block within 1.5e-6, the size of the error of
-the fast hardware sine the other path uses.
+This test restates that arithmetic in float32, each fused multiply-add as a
+float64 product (exact for float32 operands) and sum rounded to float32 (a
+true fused multiply-add but for rare double roundings), and checks it against
+float64 sines: the seed within a few float32 ulps, and |sin| along a block
+within 1.5e-6 beyond the rounding of t itself, the size of the error of the
+fast hardware sine the other path uses.
 """
 import math
 
