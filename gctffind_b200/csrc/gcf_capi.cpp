@@ -97,6 +97,7 @@ struct gcf_ctx {
     DBuf<float> taper;
     DBuf<int> rad_off, rad_pix;
     DBuf<int> ring_off, ring_pix;
+    DBuf<double2> ring_geo;   // (s^2, polar angle) of each ring pixel
 
     // bands
     std::vector<BandHost*> bands;
@@ -295,6 +296,18 @@ gcf_status build_tile_tables(gcf_ctx* ctx)
         CK(ctx->ring_pix.ensure(rpix.size()));
         CK(cudaMemcpy(ctx->ring_off.p, roff.data(), roff.size() * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->ring_pix.p, rpix.data(), rpix.size() * sizeof(int), cudaMemcpyHostToDevice));
+        // s^2 and the polar angle atan(fy / (fx + 1e-30)) of GCalcCTF2D
+        // (FindCTF/GCalcCTF2D.cu:20-27) per ring pixel, in double: they
+        // depend on the tile size only
+        std::vector<double2> geo(rpix.size());
+        for (size_t k = 0; k < rpix.size(); ++k) {
+            const int y = rpix[k] / cx, x = rpix[k] - y * cx;
+            const double fx = x * 0.5 / (cx - 1);
+            const double fy = (double)(y - cy / 2) / cy;
+            geo[k] = make_double2(fx * fx + fy * fy, std::atan(fy / (fx + 1e-30)));
+        }
+        CK(ctx->ring_geo.ensure(geo.size()));
+        CK(cudaMemcpy(ctx->ring_geo.p, geo.data(), geo.size() * sizeof(double2), cudaMemcpyHostToDevice));
     }
     // exp(-2 pi i t / T), t < T: twiddles of the fused tile FFT
     std::vector<float2> tw(T);
@@ -867,7 +880,7 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     if (any_2d) {
         // GSpectralCC2D resolution (FindCTF/CFindDefocus2D.cpp:382-400)
         CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
-        launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p,
+        launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p, ctx->ring_geo.p,
                        ctx->ring_sums.p, ctx->cc_res.p, ctx->st);
         CKL();
         launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
@@ -1205,6 +1218,7 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->rad_pix.release();
     ctx->ring_off.release();
     ctx->ring_pix.release();
+    ctx->ring_geo.release();
     ctx->d_bands.release();
     ctx->images.release();
     ctx->rescaled.release();

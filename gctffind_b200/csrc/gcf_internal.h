@@ -185,7 +185,8 @@ void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_o
                           const gcf_result* res, const PixOptics* o, const double* moments,
                           float res_lo_freq_dummy, float* full, cudaStream_t st);
 void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, const int* ring_off,
-                    const int* ring_pix, double* ring_sums, float* cc, cudaStream_t st);
+                    const int* ring_pix, const double2* ring_geo, double* ring_sums, float* cc,
+                    cudaStream_t st);
 
 // gcf_control.cu: candidate kernel with the state machine in its last blocks
 void launch_eval2d(const EvalArgs& a, int cand_blocks, int max_band_n, cudaStream_t st);

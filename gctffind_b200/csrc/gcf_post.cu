@@ -315,7 +315,17 @@ __global__ void k_band_gather(const float* __restrict__ ctf, int cmp_n,
     if (threadIdx.x == 0) sum_ss[j] = v[0];
 }
 
-// Signed CTF of GCalcCTF2D (FindCTF/GCalcCTF2D.cu:15-38) at one pixel, double.
+// Signed CTF of GCalcCTF2D (FindCTF/GCalcCTF2D.cu:15-38), double, from a
+// pixel's s^2 and polar angle.
+__device__ double ctf_geo(double s2, double th, const PixOptics& o, double add, double mean, double sigma,
+                          double az)
+{
+    double df = mean + sigma * cos(2.0 * (th - az));
+    double chi = add + M_PI * (double)o.wl * s2 * (df - 0.5 * s2 * (double)o.wl * o.wl * o.cs);
+    return -sin(chi);
+}
+
+// The same at one pixel (x, y) of the half spectrum.
 __device__ double ctf_at(int x, int y, int cx, int cy, const PixOptics& o, double add,
                          double mean, double sigma, double az)
 {
@@ -323,9 +333,7 @@ __device__ double ctf_at(int x, int y, int cx, int cy, const PixOptics& o, doubl
     double fy = (double)(y - cy / 2) / cy;
     double s2 = fx * fx + fy * fy;
     double th = atan(fy / (fx + 1e-30));
-    double df = mean + sigma * cos(2.0 * (th - az));
-    double chi = add + M_PI * (double)o.wl * s2 * (df - 0.5 * s2 * (double)o.wl * o.wl * o.cs);
-    return -sin(chi);
+    return ctf_geo(s2, th, o, add, mean, sigma, az);
 }
 
 // CSpectrumImage::mGenFullSpectrum + mEmbedCTF (FindCTF/CSpectrumImage.cpp:36-71,
@@ -373,7 +381,7 @@ __global__ void k_full_spectrum(const float* __restrict__ ctf, int tile, const i
 // the Pearson CC of each width-10 shell from its rings.
 __global__ void k_ring_sums(const float* __restrict__ ctf, int tile, const SearchJob* __restrict__ jobs,
                             const int* __restrict__ ring_off, const int* __restrict__ ring_pix,
-                            double* __restrict__ ring_sums)
+                            const double2* __restrict__ ring_geo, double* __restrict__ ring_sums)
 {
     __shared__ double sh[5 * 32];
     int ring = blockIdx.x, j = blockIdx.y;
@@ -389,8 +397,8 @@ __global__ void k_ring_sums(const float* __restrict__ ctf, int tile, const Searc
     double v[5] = {0, 0, 0, 0, 0};
     for (int k = ring_off[ring] + threadIdx.x; k < ring_off[ring + 1]; k += blockDim.x) {
         int pix = ring_pix[k];
-        int y = pix / cx, x = pix - y * cx;
-        double c = ctf_at(x, y, cx, cy, o, add, mn, sg, az);
+        const double2 g = ring_geo[k];   // (s^2, polar angle) of the pixel
+        double c = ctf_geo(g.x, g.y, o, add, mn, sg, az);
         double s = sp[pix];
         v[0] += c * s;
         v[1] += c;
@@ -524,11 +532,12 @@ void launch_full_spectrum(const float* ctf, int tile, int nmic, const int* mic_o
 }
 
 void launch_ctf_res(const float* ctf, int tile, const SearchJob* jobs, int njobs, const int* ring_off,
-                    const int* ring_pix, double* ring_sums, float* cc, cudaStream_t st)
+                    const int* ring_pix, const double2* ring_geo, double* ring_sums, float* cc,
+                    cudaStream_t st)
 {
     if (njobs <= 0) return;
     dim3 grid(tile / 2 + 1, njobs);
-    k_ring_sums<<<grid, 128, 0, st>>>(ctf, tile, jobs, ring_off, ring_pix, ring_sums);
+    k_ring_sums<<<grid, 128, 0, st>>>(ctf, tile, jobs, ring_off, ring_pix, ring_geo, ring_sums);
     k_shell_cc<<<njobs, 128, 0, st>>>(tile, ring_sums, cc);
 }
 
