@@ -1,24 +1,35 @@
 #!/usr/bin/env python
 """Benchmark of the CTF-estimation hot path on B200.
 
-Workload (one "step"): a synthetic tilt series of 41 micrographs, 4096 x 4096
-float32 at 1.35 A/px (-60..+60 degrees in 3-degree steps, 3 e/A^2 per tilt,
-defocus 30000 A at 0 degrees with a per-column gradient set by the tilt,
-astigmatism uniform in 0-800 A at a random angle), processed with the
-reference's series policy (CFindSeriesCtfs: zero tilt full search, every
-other tilt refined around the best-scoring earlier one) through the C ABI
-call gcf_run_series.
+Workload (one "step"): the uneven batch -- 256 independent synthetic
+micrographs, each a seeded pick of 4096 x 4096, 5760 x 4092 or 3838 x 3710
+float32 at 0.8-1.5 A/px (rescaled to >= 1.2 A/px like the reference),
+defocus 5000-40000 A, astigmatism 0-1000 A at a random angle, dose
+0.5-2 e/A^2 -- searched in one gcf_run_batch_mode call.
 
-  value : micrographs/s with the series already resident in HBM
-          (device pointers), device time from CUDA events on the library stream
-  e2e   : the same call with pinned HOST buffers; the host->device copy of
-          the 41 images and the device->host read of the results are inside
-          the timed region
+  value  : micrographs/s of the learned + batched + BF16 contraction path
+           (GCF_SEARCH_LEARNED when trained weights are present, else
+           GCF_SEARCH_BF16), micrographs resident in HBM, device time from
+           CUDA events on the library stream
+  plain  : the same batch through this project's plain FP32 exhaustive
+           search, batched (one GCF_SEARCH_PLAIN call) and in the
+           reference's single-file mode (one call per micrograph)
+  e2e    : the headline path with pinned HOST buffers, host clock around the
+           call: host->device copies of the 256 images and the result rows
+           are inside the timed region
+  defocus_error : the fast path against the plain path on the same batch
+           (median |d defocus|, fraction within one search step) and both
+           against the generator's truth
 
-Rank r of N processes its own series (seeded by r): weak scaling, replicas
+Secondary figures on the same line: the 41-tilt 4096^2 series at 1.35 A/px
+through the reference's series policy (plain search), and one 4096^2
+micrograph at 1.0 A/px (rescale path) in single-file mode.
+
+Rank r of N processes its own batch (seeded by r): weak scaling, replicas
 only, no data-path collective.  `--impl reference` times the reference's own
-CUDA implementation of the path, built from its sources, on the same GPU
-(the FP64 host oracle when that build is absent).
+CUDA implementation of the path, built from its sources, on a rotating
+sample of the same batch (single-file mode, as the reference runs
+independent micrographs).
 """
 from __future__ import annotations
 
@@ -29,20 +40,18 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_TILTS = 41
-SIZE = 4096
-PX = 1.35
-METRIC = "4096^2 micrographs/s (tilt series, plain FP32 search)"
-# DRAM bytes (read + write) of one micrograph's share of k_fused_spectrum,
-# from ncu dram__bytes_read.sum + dram__bytes_write.sum on a 3-micrograph
-# launch of the same kernel divided by 3 (profiles/k_fused_spectrum_3x4096.md)
-TILE_KERNEL_TRAFFIC_PER_MICROGRAPH = (262_052_608 + 11_340_544) // 3
+N_BATCH = 256
+METRIC = "4096^2 micrographs/s, learned+batched+BF16 vs plain GPU path; defocus error (A)"
+SERIES_PX = 1.35
+# DRAM bytes (read + write) of k_fused_spectrum per algorithmic byte (the
+# image read once), from ncu dram__bytes_read.sum + dram__bytes_write.sum on
+# a 3-micrograph capture of the same kernel
+TILE_KERNEL_TRAFFIC_RATIO = (262_052_608 + 11_340_544) / (3 * 67_108_864)
 
 
 def parse():
@@ -51,25 +60,25 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--spectrum", default="auto", choices=["auto", "fused", "cufft"])
-    ap.add_argument("--n-tilts", type=int, default=N_TILTS)
-    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--batch", type=int, default=N_BATCH)
+    ap.add_argument("--mode", default="auto", choices=["auto", "bf16", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--trace", default=None,
-                    help="after the timed steps, record one device-resident step with the CUDA "
-                         "activity tracer (torch.profiler) and write a Chrome trace here")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the tilt-series and 1.0 A/px single-micrograph figures")
+    ap.add_argument("--shrink", type=int, default=1,
+                    help="divide the micrograph sizes by this factor (quick checks only)")
     return ap.parse_args()
 
 
-def dist_setup(n):
+def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         import datetime
         import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         backend = "nccl" if torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
@@ -146,17 +155,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def make_series(rank, n_tilts, size, device):
-    import torch
-    from gctffind_b200 import synth
-    specs = synth.tilt_series_specs(n_tilts=n_tilts, step_deg=3.0, size=size, pixel_size=PX,
-                                    dose=3.0, df0=30000.0, seed=1 + rank)
-    imgs = [synth.make_micrograph(s, device=device) for s in specs]
-    if torch.cuda.is_available():
-        torch.cuda.synchronize()
-    return specs, imgs
-
-
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -164,289 +162,360 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "_fallback": True}
 
 
-def cpu_baseline(imgs_host, order, budget_s=25.0):
-    """FP64 OpenMP oracle on the host cores: the zero-tilt full search plus
-    refinements of the next tilts in processing order, as many as fit the
-    time budget (at least one)."""
+def batch_specs(n, seed, shrink=1):
+    from gctffind_b200 import synth
+    sizes = tuple((w // shrink // 2 * 2, h // shrink // 2 * 2) for w, h in synth.UNEVEN_SIZES)
+    return synth.uneven_batch_specs(n, seed=seed, sizes=sizes)
+
+
+def make_batch(rank, n, device, shrink=1):
+    import torch
+    from gctffind_b200 import synth
+    specs = batch_specs(n, 2 + rank, shrink)
+    imgs = [synth.make_micrograph(s, device=device) for s in specs]
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+    return specs, imgs
+
+
+def workload_name(n):
+    return (f"uneven batch of {n} independent micrographs (4096x4096 / 5760x4092 / 3838x3710 float32, "
+            "0.8-1.5 A/px rescaled to >= 1.2, df 5000-40000 A, astig 0-1000 A, dose 0.5-2 e/A^2), "
+            "one search per micrograph")
+
+
+def search_step(spec_mean):
+    """The plain search's last mean-defocus step (max(20 A, range / 31) with
+    range 0.525 * 0.2 * mean, FindCTF/CFindDefocus2D.cpp:166-182, 296-300)."""
+    return max(20.0, 0.105 * spec_mean / 31.0)
+
+
+def defocus_error(fast, plain, specs):
+    import numpy as np
+    from gctffind_b200 import synth
+    d_fp, within, d_ft, d_pt = [], [], [], []
+    for f, p, s in zip(fast, plain, specs):
+        mf, mp = 0.5 * (f.df_min + f.df_max), 0.5 * (p.df_min + p.df_max)
+        mt = 0.5 * (s.df_min + s.df_max)
+        step = search_step(mp)
+        d_fp.append(abs(mf - mp))
+        within.append(abs(f.df_min - p.df_min) <= step and abs(f.df_max - p.df_max) <= step)
+        if synth.inside_reference_envelope(s):
+            d_ft.append(abs(mf - mt))
+            d_pt.append(abs(mp - mt))
+    return {"median_abs_ddf_vs_plain_A": round(float(np.median(d_fp)), 2),
+            "p90_abs_ddf_vs_plain_A": round(float(np.percentile(d_fp, 90)), 2),
+            "frac_within_one_step_of_plain": round(float(np.mean(within)), 4),
+            "median_abs_ddf_vs_truth_A": {"fast": round(float(np.median(d_ft)), 2) if d_ft else None,
+                                          "plain": round(float(np.median(d_pt)), 2) if d_pt else None,
+                                          "micrographs": len(d_ft),
+                                          "note": "inside the reference's search envelope"},
+            "one_step": "max(20 A, 0.105 * mean / 31): the plain search's last mean-defocus step"}
+
+
+def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
+    import torch
+    for _ in range(warmup):
+        ctx.run_batch(imgs, pxs, op, mode=mode)
+    barrier(world)
+    torch.cuda.synchronize()
+    dev_ms, launches, stage, ftimes, fcounts = 0.0, 0, {}, {}, {}
+    res = None
+    for _ in range(steps):
+        res = ctx.run_batch(imgs, pxs, op, mode=mode)
+        st = ctx.stage_times()
+        dev_ms += st["total"]
+        for k, v in st.items():
+            stage[k] = stage.get(k, 0.0) + v / steps
+        launches += ctx.launch_count()
+        if mode != 0:
+            for k, v in ctx.fast_times().items():
+                ftimes[k] = ftimes.get(k, 0.0) + v / steps
+            fcounts = ctx.fast_counts()
+    torch.cuda.synchronize()
+    barrier(world)
+    return {"ms": max_over_ranks(dev_ms / steps, world), "results": res, "stage": stage,
+            "launches": launches // steps, "fast_ms": ftimes, "fast_counts": fcounts,
+            "search_counts": ctx.search_counts()}
+
+
+def timed_single_file(ctx, imgs, pxs, op, steps, world):
+    """The reference's single-file mode: one plain search call per
+    micrograph, one pass over the batch per step."""
+    import torch
+    for k in range(len(imgs)):
+        ctx.run_batch([imgs[k]], [pxs[k]], op, mode=0)
+    barrier(world)
+    torch.cuda.synchronize()
+    dev_ms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for k in range(len(imgs)):
+            ctx.run_batch([imgs[k]], [pxs[k]], op, mode=0)
+            dev_ms += ctx.stage_times()["total"]
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) * 1000.0 / steps
+    barrier(world)
+    return max_over_ranks(dev_ms / steps, world), max_over_ranks(wall, world)
+
+
+def cpu_baseline(host, specs, budget_s=20.0):
+    """FP64 OpenMP oracle on the host cores: the plain full search (rescale,
+    spectrum, 1D + 2D) of the batch's micrographs in order, as many as fit
+    the time budget (at least one)."""
+    from gctffind_b200 import synth
     from oracle import oracle as O
     O.build()
     cores = O.num_threads(os.cpu_count() or 1)
-    p = O.params(pixel_size=PX, tile_size=512)
     t0 = time.perf_counter()
-    z = order[0]
-    r0 = O.find_ctf_image(imgs_host[z], PX, p, mode=0)
-    done = 1
-    for idx in order[1:]:
-        if time.perf_counter() - t0 > budget_s:
+    done = 0
+    for img, s in zip(host, specs):
+        if done and time.perf_counter() - t0 > budget_s:
             break
-        dmin, dmax = r0.df_min, r0.df_max
-        mean = 0.5 * (dmin + dmax)
-        rin = [mean, max(mean * 0.5, 5000.0 * PX * PX), (dmax - dmin) * 0.5 / mean, 0.0,
-               r0.azimuth, 0.0, r0.ext_phase, 0.0]
-        O.find_ctf_image(imgs_host[idx], PX, p, mode=1, refine_in=rin)
+        nw, nh, px_n, _ = O.rescale_dims(img.shape[1], img.shape[0], s.pixel_size)
+        im = O.rescale(img, s.pixel_size) if px_n != s.pixel_size else img
+        O.find_ctf_image(im, px_n, O.params(pixel_size=px_n, tile_size=512), mode=0)
         done += 1
     dt = time.perf_counter() - t0
+    del synth
     return {"value": done / dt, "unit": "micrographs/s", "cores": cores, "kind": "port",
-            "sample": f"{done} of the series' 4096^2 micrographs (zero-tilt full search + "
-                      f"{done - 1} refinements), FP64 oracle, {cores} OpenMP threads, {dt:.1f} s"}
+            "sample": f"the first {done} micrographs of the batch (rescale + spectrum + 1D + 2D full "
+                      f"search), FP64 oracle, {cores} OpenMP threads, {dt:.1f} s"}
 
 
-def _reference_cuda_step(host, order, tilts, sample_refines):
-    """One step of the reference arm on the reference's own CUDA build:
-    the zero-tilt full search alone, then the zero tilt plus
-    `sample_refines` packages spread evenly over the rest of the processing
-    order (high tilts refine at a different cost than low ones).  Returns
-    (seconds of the full search, mean seconds of one refined package)."""
-    from oracle import refimpl
-    rest = order[1:]
-    stride = max(1, len(rest) // max(1, sample_refines))
-    sub = [order[0]] + rest[stride - 1::stride][:sample_refines]
-    imgs = [host[i] for i in sub]
-    t = [tilts[i] for i in sub]
-    _, _, t_full = refimpl.run_series(imgs[:1], PX, [0], tilts=t[:1], tile=512)
-    _, _, t_sub = refimpl.run_series(imgs, PX, list(range(len(imgs))), tilts=t, tile=512)
-    return t_full, max(t_sub - t_full, 0.0) / max(1, len(sub) - 1)
+def series_figures(ctx, G, steps, warmup, world, rank):
+    """41-tilt 4096^2 series at 1.35 A/px, reference series policy, plain
+    search: device-resident and end to end (full spectra requested, as the
+    reference's CFindSeriesCtfs produces them per package)."""
+    import torch
+    from gctffind_b200 import synth
+    specs = synth.tilt_series_specs(n_tilts=41, step_deg=3.0, size=4096, pixel_size=SERIES_PX, dose=3.0,
+                                    df0=30000.0, seed=1 + rank)
+    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
+    order = G.series_order(synth.tilt_angles(41, 3.0)).order
+    op = G.make_optics(pixel_size=SERIES_PX)
+    for _ in range(warmup):
+        ctx.run_series(imgs, op, order, is_tomo=True, want_full=True)
+    torch.cuda.synchronize()
+    ms = 0.0
+    for _ in range(steps):
+        ctx.run_series(imgs, op, order, is_tomo=True, want_full=True)
+        ms += ctx.stage_times()["total"]
+    ms = max_over_ranks(ms / steps, world)
+    host = [im.cpu().pin_memory() for im in imgs]
+    del imgs
+    torch.cuda.empty_cache()
+    ctx.run_series(host, op, order, is_tomo=True, want_full=True)
+    wall = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ctx.run_series(host, op, order, is_tomo=True, want_full=True)
+        wall += time.perf_counter() - t0
+    wall = max_over_ranks(wall / steps * 1000.0, world)
+    return {"workload": "tilt series 41 x 4096^2 float32 @ 1.35 A/px, 3 e/A^2, df 30000 A + tilt gradient; "
+                        "CFindSeriesCtfs policy (zero tilt full, rest refined), plain FP32 search, full "
+                        "diagnostic spectra returned",
+            "value": round(world * 41 / (ms / 1000.0), 2), "unit": "micrographs/s", "ms_per_step": round(ms, 3),
+            "e2e": {"value": round(world * 41 / (wall / 1000.0), 2), "unit": "micrographs/s",
+                    "ms_per_step": round(wall, 3), "h2d_bytes_per_step": 41 * 4096 * 4096 * 4,
+                    "d2h_bytes_per_step": 41 * (512 * 512 * 4 + 40), "timing": "host clock around the call"}}
+
+
+def single_1p0(ctx, G, steps):
+    """One 4096^2 micrograph at 1.0 A/px (Fourier-cropped to 3412^2 at
+    1.2 A/px first), plain search, single-file mode."""
+    import torch
+    from gctffind_b200 import synth
+    spec = synth.MicrographSpec(width=4096, height=4096, pixel_size=1.0, df_min=14850.0, df_max=15150.0,
+                                azimuth_deg=20.0, dose=1.0, seed=2024)
+    img = synth.make_micrograph(spec, device="cuda")
+    op = G.make_optics()
+    for _ in range(3):
+        ctx.run_batch([img], [1.0], op, mode=0)
+    ms, st = 0.0, {}
+    for _ in range(steps):
+        r = ctx.run_batch([img], [1.0], op, mode=0)[0]
+        s = ctx.stage_times()
+        ms += s["total"]
+        for k, v in s.items():
+            st[k] = st.get(k, 0.0) + v / steps
+    torch.cuda.synchronize()
+    return {"workload": "one 4096^2 micrograph @ 1.0 A/px (rescaled to 3412^2 @ 1.2 A/px), df 15000 A, "
+                        "astig 300 A at 20 deg, 1 e/A^2; plain search, one call",
+            "value": round(1000.0 / (ms / steps), 2), "unit": "micrographs/s", "ms": round(ms / steps, 3),
+            "stage_ms": {k: round(v, 3) for k, v in st.items()},
+            "result": {"df_min": round(r.df_min, 1), "df_max": round(r.df_max, 1), "azimuth": round(r.azimuth, 2)}}
+
+
+def tile_kernel_roofline(stage, imgs_dims, pk):
+    """k_fused_spectrum (+ its cluster-less companion) over every tile of the
+    batch: algorithmic bytes = each (rescaled) image the kernel reads, read
+    once; time = the union of its launches inside the timed calls."""
+    ms = stage.get("tile_kernel", 0.0)
+    algo = sum(4 * w * h for w, h in imgs_dims)
+    achieved = algo / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+    peak = pk.get("hbm_gbs", 6650.0)
+    return {"kernel": "k_fused_spectrum (8-CTA clusters) + k_fused_spectrum_solo (the SMs the clusters leave free)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": "fallback" if pk.get("_fallback") else "measured",
+            "traffic": int(algo * TILE_KERNEL_TRAFFIC_RATIO),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per image byte on a 3 x 4096^2 "
+                              "capture of k_fused_spectrum, scaled by the batch's image bytes",
+            "algorithmic_bytes_per_launch": algo, "launch_ms": round(ms, 3)}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference implementation of the path on this
-    box.  GCtfFind has no CPU path: its own CUDA code, built from its
-    sources (oracle/_ref/libgcfref.so), runs on the same B200 when present;
-    otherwise the FP64 oracle port times the host cores."""
+    """--impl reference: the reference's own CTF path (built from its
+    sources, oracle/_ref/libgcfref.so) on the same B200, in its single-file
+    mode, on a rotating sample of the batch: step k takes micrographs
+    3k, 3k+1, 3k+2 (mod the batch), so the steps together cover different
+    sizes and pixel sizes.  Rank 0 alone runs it."""
     if rank != 0:
         return 0
+    import numpy as np
     import torch
-    from gctffind_b200 import synth
-    from gctffind_b200.api import series_order
     from oracle import refimpl
     on_gpu = torch.cuda.is_available()
-    specs, imgs = make_series(0, args.n_tilts, args.size, "cuda" if on_gpu else "cpu")
-    host = [im.cpu().numpy() for im in imgs]
-    del imgs
+    n = args.batch
+    per_step = 3
+    need = min(n, (args.warmup + args.steps) * per_step)
+    from gctffind_b200 import synth
+    specs = batch_specs(n, 2, args.shrink)
+    sel = [specs[i % n] for i in range(need)]
+    host = [synth.make_micrograph(s, device="cuda" if on_gpu else "cpu").cpu().numpy() for s in sel]
     if on_gpu:
         torch.cuda.empty_cache()
-    tilts = synth.tilt_angles(args.n_tilts, 3.0)
-    order = series_order(tilts).order
-    n = args.n_tilts
-    workload = (f"tilt series {n} x {args.size}^2 float32 @ {PX} A/px, CFindSeriesCtfs policy "
-                "(zero tilt full, rest refined)")
-    if on_gpu and refimpl.available():
-        k_ref = min(8, n - 1)
-        fulls, refs = [], []
-        for k in range(args.warmup + args.steps):
-            tf, tr = _reference_cuda_step(host, order, tilts, k_ref)
-            if k >= args.warmup:
-                fulls.append(tf)
-                refs.append(tr)
-        t_full, t_ref = statistics.median(fulls), statistics.median(refs)
-        t_series = t_full + (n - 1) * t_ref
-        v = n / t_series
-        sample = (f"reference CUDA build on the B200 (GCtfFind has no CPU path): per step the "
-                  f"zero-tilt full search ({t_full:.2f} s) and {k_ref} refined tilts spread over "
-                  f"the processing order "
-                  f"({t_ref:.2f} s each, medians over {args.steps} steps); value = {n} / "
-                  f"(full + {n - 1} x refine) = {t_series:.1f} s per series")
-        line = {"metric": METRIC, "value": round(v, 4), "unit": "micrographs/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 * t_series, 1),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+    workload = workload_name(n)
+    if not (on_gpu and refimpl.available()):
+        cb = cpu_baseline(host, sel, budget_s=30.0 if args.shrink == 1 else 2.0)
+        line = {"metric": METRIC, "value": round(cb["value"], 4), "unit": "micrographs/s", "n_gpus": 1,
+                "steps": 1, "warmup": 0, "ms_per_step": round(1000.0 / cb["value"], 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "impl": "reference",
-                "config": {"workload": workload, "tile": 512, "l2": "inputs larger than L2",
-                           "timing": "host wall clock around CFindSeriesCtfs::DoIt (it blocks on "
-                                     "every candidate), images in host memory"},
-                "cpu_baseline": {"value": round(v, 4), "unit": "micrographs/s", "cores": 1,
-                                 "kind": "reference", "sample": sample},
-                "e2e": {"value": round(v, 4), "unit": "micrographs/s",
-                        "h2d_bytes_per_step": n * args.size * args.size * 4,
-                        "d2h_bytes_per_step": n * (512 * 512 * 4 + 20)}}
+                "config": {"workload": workload, "note": "reference CUDA build unavailable here: FP64 oracle "
+                                                         "port on the host"},
+                "cpu_baseline": cb,
+                "e2e": {"value": round(cb["value"], 4), "unit": "micrographs/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
-    vals = []
-    cb = None
-    for k in range(max(1, args.warmup) + max(1, args.steps)):
-        cb = cpu_baseline(host, order, budget_s=8.0)
-        if k >= max(1, args.warmup):
-            vals.append(cb["value"])
-        if len(vals) >= args.steps:
-            break
-    v = statistics.median(vals)
-    cb["value"] = v
-    line = {"metric": METRIC, "value": v, "unit": "micrographs/s", "n_gpus": world,
-            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1000.0 * n / v,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+    secs, cnt = [], 0
+    for k in range(args.warmup + args.steps):
+        t = 0.0
+        for q in range(per_step):
+            i = (k * per_step + q) % len(sel)
+            _, _, dt = refimpl.run_series([host[i]], sel[i].pixel_size, [0], is_tomo=False, tile=512)
+            t += dt
+        if k >= args.warmup:
+            secs.append(t)
+            cnt += per_step
+    total = sum(secs)
+    v = cnt / total
+    sizes = sorted({(s.width, s.height) for s in sel[args.warmup * per_step:]})
+    sample = (f"reference CUDA build on the B200 (GCtfFind has no CPU path), single-file mode: {per_step} "
+              f"micrographs per step from the batch, different ones each step ({cnt} timed, sizes {sizes}); "
+              f"host clock around CFindSeriesCtfs::DoIt per micrograph, images in host memory")
+    line = {"metric": METRIC, "value": round(v, 4), "unit": "micrographs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 * total / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload + " (sampled: zero-tilt full search + refinements)",
-                       "l2": "inputs larger than L2",
-                       "note": "reference CUDA build unavailable here: FP64 oracle port on the host"},
-            "cpu_baseline": cb,
-            "e2e": {"value": v, "unit": "micrographs/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "config": {"workload": workload, "tile": 512, "search": "the reference's FP32 search",
+                       "ranks": "rank 0 only (n_gpus counts the GPUs this line used)"},
+            "cpu_baseline": {"value": round(v, 4), "unit": "micrographs/s", "cores": 1, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(v, 4), "unit": "micrographs/s",
+                    "h2d_bytes_per_step": int(np.mean([4 * s.width * s.height for s in sel]) * per_step),
+                    "d2h_bytes_per_step": per_step * 20}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def main():
     args = parse()
-    rank, world, local = dist_setup(args.gpus)
+    rank, world, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, rank, world)
     import numpy as np
     import torch
     import gctffind_b200 as G
-    from gctffind_b200 import synth
     torch.cuda.set_device(local)
-    specs, imgs = make_series(rank, args.n_tilts, args.size, f"cuda:{local}")
-    order = G.series_order(synth.tilt_angles(args.n_tilts, 3.0)).order
     ctx = G.Context(local, 512, 0)
-    if args.spectrum == "cufft":
-        ctx.set_spectrum_impl(G.GCF_SPECT_CUFFT)
-    elif args.spectrum == "fused":
-        ctx.set_spectrum_impl(G.GCF_SPECT_FUSED)
-    else:
-        try:
-            ctx.set_spectrum_impl(G.GCF_SPECT_FUSED)
-        except G.GcfError:
-            ctx.set_spectrum_impl(G.GCF_SPECT_CUFFT)
-    op = G.make_optics(pixel_size=PX)
+    op = G.make_optics()
+    specs, imgs = make_batch(rank, args.batch, f"cuda:{local}", args.shrink)
+    pxs = [s.pixel_size for s in specs]
+    learned = args.mode == "learned" or (args.mode == "auto" and G.learned_available())
+    fast_mode = G.GCF_SEARCH_LEARNED if learned else G.GCF_SEARCH_BF16
+    if learned:
+        G.load_learned(ctx)
 
-    # ---- device-resident inputs -------------------------------------------------
-    # clocks are sampled from the warm-up on through the end-to-end steps, so
-    # the short device-resident region gets samples on both sides as well
     clk = ClockSampler(local)
     clk.start()
-    for _ in range(args.warmup):
-        ctx.run_series(imgs, op, order, is_tomo=True)
-    barrier(world)
-    torch.cuda.synchronize()
-    dev_ms, stage = 0.0, {}
-    launches = 0
-    results = None
-    torch.cuda.nvtx.range_push("device_steps")   # lets ncu --nvtx-include select the timed launches
-    counts = None
-    for _ in range(args.steps):
-        results = ctx.run_series(imgs, op, order, is_tomo=True)
-        counts = ctx.search_counts()
-        st = ctx.stage_times()
-        dev_ms += st["total"]
-        for k, v in st.items():
-            stage[k] = stage.get(k, 0.0) + v
-        launches += ctx.launch_count()
-    torch.cuda.synchronize()
+    # ---- the headline path, device-resident ----
+    torch.cuda.nvtx.range_push("fast_steps")
+    fast = timed_batch(ctx, imgs, pxs, op, fast_mode, args.steps, args.warmup, world)
     torch.cuda.nvtx.range_pop()
-    barrier(world)
-    t_step = max_over_ranks(dev_ms / args.steps, world)
-    value = world * args.n_tilts / (t_step / 1000.0)
-
-    # ---- end to end: pinned host inputs, H2D + results D2H inside the timed region ----
+    # ---- plain FP32 search: batched, and single-file mode ----
+    plain = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_PLAIN, args.steps, min(args.warmup, 2), world)
+    single_ms, single_wall = timed_single_file(ctx, imgs, pxs, op, max(1, min(args.steps, 2)), world)
+    # ---- end to end: pinned host inputs, host clock around the call ----
     host = [im.cpu().pin_memory() for im in imgs]
-    for _ in range(max(1, min(args.warmup, 2))):
-        ctx.run_series(host, op, order, is_tomo=True)
+    dims = [(G.rescale_dims(s.width, s.height, s.pixel_size)[0], G.rescale_dims(s.width, s.height, s.pixel_size)[1])
+            for s in specs]
+    del imgs
+    torch.cuda.empty_cache()
+    ctx.run_batch(host, pxs, op, mode=fast_mode)
     barrier(world)
-    e2e_ms = 0.0
-    torch.cuda.nvtx.range_push("e2e_steps")
+    e2e_wall = 0.0
     for _ in range(args.steps):
-        ctx.run_series(host, op, order, is_tomo=True)
-        e2e_ms += ctx.stage_times()["total"]
-    torch.cuda.nvtx.range_pop()
+        t0 = time.perf_counter()
+        ctx.run_batch(host, pxs, op, mode=fast_mode)
+        e2e_wall += time.perf_counter() - t0
+    e2e_ms = max_over_ranks(e2e_wall / args.steps * 1000.0, world)
     clocks = clk.stop()
-    barrier(world)
-    t_e2e = max_over_ranks(e2e_ms / args.steps, world)
-    e2e = world * args.n_tilts / (t_e2e / 1000.0)
-    h2d = sum(int(im.numel()) * 4 for im in imgs)
-    d2h = args.n_tilts * 40
-
-    if args.trace and rank == 0:
-        # kernel start/end times on every stream, recorded without serialising
-        # the launches (unlike ncu): shows how the searches overlap the tiles
-        from torch.profiler import profile, ProfilerActivity
-        with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            ctx.run_series(imgs, op, order, is_tomo=True)
-            torch.cuda.synchronize()
-        prof.export_chrome_trace(args.trace)
-
-    # ---- roofline of the dominant kernel: the fused tile-spectrum kernel.
-    # In a series step its launches share the GPU with the searches, so it is
-    # timed alone here: a batch call makes one launch over all micrographs of
-    # the series and runs the searches only after it ----
+    n = args.batch
+    value = world * n / (fast["ms"] / 1000.0)
     pk = peaks()
-    pxs = [PX] * args.n_tilts
-    ctx.run_batch(imgs, pxs, op)
-    kt = []
-    st2d = []
-    torch.cuda.nvtx.range_push("tile_kernel_alone")   # ncu --nvtx-include selects these launches
-    for _ in range(max(1, min(args.steps, 3))):
-        ctx.run_batch(imgs, pxs, op)
-        bt = ctx.stage_times()
-        kt.append(bt["tile_kernel"])
-        st2d.append(bt["search2d"])
-    torch.cuda.nvtx.range_pop()
-    kern_ms = statistics.median(kt)
-    bcounts = ctx.search_counts()
-    T = 512
-    ov = T // 2
-    nt1 = ((args.size - ov) // (T - ov)) ** 2            # tiles per micrograph
-    nch = -(-nt1 // 24)                                   # work items per micrograph (<= 24 tiles)
-    img_bytes = args.n_tilts * 4 * args.size * args.size  # every pixel read once
-    part_bytes = args.n_tilts * nch * (T // 2 + 1) * T * 4  # per-item partial spectra written
-    algo_bytes = img_bytes + part_bytes
-    # real 2D FFT of a T x T tile: 2.5 T^2 log2(T^2) flops, plus mean removal,
-    # taper, |F| and accumulation (~6 flops per pixel)
-    tile_flops = 2.5 * T * T * 2 * 9 + 6 * T * T
-    algo_flops = args.n_tilts * nt1 * tile_flops
-    sec = kern_ms / 1000.0
-    achieved = algo_bytes / sec / 1e9 if sec > 0 else 0.0
-    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12          # nominal FP32 FMA rate at max clock
-    roof = {"kernel": "k_fused_spectrum (8-CTA clusters) + k_fused_spectrum_solo (the SMs the clusters leave "
-                      "free): one launch pair over all tiles of the series, timed alone",
-            "bound": "hbm", "achieved": round(achieved, 1), "peak": pk.get("hbm_gbs"),
-            "unit": "GB/s", "frac": round(achieved / pk.get("hbm_gbs", 6650.0), 4),
-            "traffic": TILE_KERNEL_TRAFFIC_PER_MICROGRAPH * args.n_tilts if TILE_KERNEL_TRAFFIC_PER_MICROGRAPH else None,
-            "peak_source": "fallback" if pk.get("_fallback") else "measured",
-            "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(kern_ms, 3),
-            "compute": {"flops_per_launch": algo_flops,
-                        "achieved_tflops": round(algo_flops / sec / 1e12, 2) if sec > 0 else 0.0,
-                        "fp32_peak_tflops": round(fp32_peak, 1), "peak_source": "nominal FP32 FMA",
-                        "frac": round(algo_flops / sec / 1e12 / fp32_peak, 4) if sec > 0 else 0.0}}
-
-    # ---- the candidate contraction: 2 flops (model x spectrum multiply-add)
-    # per (candidate, in-band pixel) pair, counted on the device; its rate is
-    # taken on the batch call, whose 2D searches (41 full Do2D) run alone ----
-    s2d_ms = statistics.median(st2d)
-    bflops = 2 * bcounts["pairs2d"]
-    search = {"per_step": dict(counts, flops=2 * (counts["pairs2d"] + counts["pairs1d"])),
-              "batch_full_search": {"cand2d": bcounts["cand2d"], "flops_2d": bflops,
-                                    "ms_2d_stage": round(s2d_ms, 3),
-                                    "achieved_tflops": round(bflops / (s2d_ms * 1e-3) / 1e12, 2) if s2d_ms > 0 else 0.0,
-                                    "fp32_peak_tflops": round(fp32_peak, 1),
-                                    "frac": round(bflops / (s2d_ms * 1e-3) / 1e12 / fp32_peak, 4) if s2d_ms > 0 else 0.0,
-                                    "note": f"{args.n_tilts} full searches (Do2D) after one tile launch"}}
-
+    fc, ft = fast["fast_counts"], fast["fast_ms"]
+    prod_ms = ft.get("product", 0.0)
+    tflops = 2.0 * fc.get("tensor_macs", 0) / (prod_ms / 1000.0) / 1e12 if prod_ms > 0 else 0.0
+    bf16_peak = pk.get("bf16_tflops", 1590.0)
     line = {"metric": METRIC, "value": round(value, 2), "unit": "micrographs/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(fast["ms"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
             "data": "synthetic",
-            "config": {"workload": f"tilt series {args.n_tilts} x {args.size}^2 float32 @ {PX} A/px, "
-                                   "3 e/A^2, df 30000 A + tilt gradient, astig 0-800 A; "
-                                   "CFindSeriesCtfs policy (zero tilt full, rest refined)",
-                       "tile": 512, "spectrum": ["fused", "cufft"][0 if args.spectrum == "fused" else 1]
-                       if args.spectrum != "auto" else "auto",
-                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (2.75 GB per step)"},
-            "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage.items()},
-            "e2e": {"value": round(e2e, 2), "unit": "micrographs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": round(t_e2e, 3)},
-            "gpu_launches": launches,
-            "roofline": roof,
-            "search": search,
+            "config": {"workload": workload_name(n), "search": ["bf16", "learned"][int(learned)],
+                       "tile": 512, "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({sum(4 * s.width * s.height for s in specs) / 1e9:.1f} GB "
+                             "per step)"},
+            "plain": {"batched": {"value": round(world * n / (plain["ms"] / 1000.0), 2), "ms_per_step": round(plain["ms"], 3),
+                                  "stage_ms": {k: round(v, 3) for k, v in plain["stage"].items()}},
+                      "single_file": {"value": round(world * n / (single_ms / 1000.0), 2),
+                                      "ms_per_step": round(single_ms, 3),
+                                      "wall_ms_per_step": round(single_wall, 3),
+                                      "note": "one plain call per micrograph (the reference's single-file mode); "
+                                              "device time summed over the calls"}},
+            "speedup": {"vs_plain_single_file": round(single_ms / fast["ms"], 3),
+                        "vs_plain_batched": round(plain["ms"] / fast["ms"], 3)},
+            "defocus_error": defocus_error(fast["results"], plain["results"], specs),
+            "stage_ms_per_step": {k: round(v, 3) for k, v in fast["stage"].items()},
+            "contraction": {"stage_ms": {k: round(v, 3) for k, v in ft.items()}, "counts": fc,
+                            "tensor_tflops": round(tflops, 1), "peak_tflops": bf16_peak,
+                            "frac": round(tflops / bf16_peak, 4),
+                            "fp32_candidates_fast": fast["search_counts"]["cand2d"],
+                            "fp32_candidates_plain": plain["search_counts"]["cand2d"]},
+            "e2e": {"value": round(world * n / (e2e_ms / 1000.0), 2), "unit": "micrographs/s",
+                    "h2d_bytes_per_step": sum(4 * s.width * s.height for s in specs),
+                    "d2h_bytes_per_step": n * 40, "ms_per_step": round(e2e_ms, 3),
+                    "timing": "host clock around gcf_run_batch_mode (pinned host images)"},
+            "gpu_launches": fast["launches"],
+            "roofline": tile_kernel_roofline(fast["stage"], dims, pk),
             "clocks": clocks}
+    if not args.no_secondary:
+        line["series_41x4096"] = series_figures(ctx, G, max(2, min(args.steps, 3)), 2, world, rank)
+        line["single_4096_1p0"] = single_1p0(ctx, G, max(2, min(args.steps, 5)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        host_np = [h.numpy() for h in host]
-        line["cpu_baseline"] = cpu_baseline(host_np, order)
+        line["cpu_baseline"] = cpu_baseline([h.numpy() for h in host], specs)
     if rank == 0:
-        r0 = results[order[0]]
-        line["sample_result"] = {"zero_tilt": {"df_min": round(r0.df_min, 1), "df_max": round(r0.df_max, 1),
-                                               "azimuth": round(r0.azimuth, 2), "score": round(r0.score, 4)},
-                                 "truth": {"df_min": round(specs[order[0]].df_min, 1),
-                                           "df_max": round(specs[order[0]].df_max, 1),
-                                           "azimuth": round(specs[order[0]].azimuth_deg, 2)}}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -24,6 +24,10 @@ CLI_PATH = os.path.join(HERE, "bin", "GCtfFind")
 GCF_SPECT_FUSED = 0
 GCF_SPECT_CUFFT = 1
 
+GCF_SEARCH_PLAIN = 0
+GCF_SEARCH_BF16 = 1
+GCF_SEARCH_LEARNED = 2
+
 # Every symbol include/gctf_b200.h declares.
 EXPORTS = [
     "gcf_create", "gcf_destroy", "gcf_strerror", "gcf_last_error", "gcf_set_spectrum_impl",
@@ -34,6 +38,10 @@ EXPORTS = [
     "gcf_get_radial_average", "gcf_rescale_dims", "gcf_rescale", "gcf_run_series",
     "gcf_run_batch", "gcf_mrc_info", "gcf_mrc_read", "gcf_mrc_read_tilts", "gcf_mrc_write",
     "gcf_get_stage_times", "gcf_get_launch_count", "gcf_get_search_counts", "gcf_avg_spectrum_noalloc",
+    "gcf_gemm_bf16", "gcf_run_batch_mode", "gcf_get_fast_counts", "gcf_get_fast_times",
+    "gcf_nn_param_count", "gcf_nn_init", "gcf_nn_set_params", "gcf_nn_get_params", "gcf_nn_save",
+    "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs",
+    "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
     "gcf_write_ctf_file",
     "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
@@ -128,6 +136,24 @@ def load_library(path: str = LIB_PATH):
     L.gcf_get_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_get_search_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
+    ll = C.c_longlong
+    L.gcf_gemm_bf16.argtypes = [vp, ll, vp, ll, i, i, i, vp, ll, i, i, vp]
+    L.gcf_run_batch_mode.argtypes = [vp, C.POINTER(Item), i, i, C.POINTER(Optics), i, C.POINTER(Result)]
+    L.gcf_get_fast_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.gcf_get_fast_times.argtypes = [vp, C.POINTER(f)]
+    ull, sz = C.c_ulonglong, C.c_size_t
+    L.gcf_nn_param_count.argtypes = []
+    L.gcf_nn_param_count.restype = sz
+    L.gcf_nn_init.argtypes = [vp, ull]
+    L.gcf_nn_set_params.argtypes = [vp, vp, sz]
+    L.gcf_nn_get_params.argtypes = [vp, vp, sz]
+    L.gcf_nn_save.argtypes = [vp, C.c_char_p]
+    L.gcf_nn_load.argtypes = [vp, C.c_char_p]
+    L.gcf_set_learned_threshold.argtypes = [vp, f]
+    L.gcf_nn_train.argtypes = [vp, C.POINTER(Optics), i, i, ull, ull, f, vp]
+    L.gcf_nn_synth_inputs.argtypes = [vp, C.POINTER(Optics), ull, ull, i, vp, vp, vp, vp]
+    L.gcf_nn_forward_backward.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
+    L.gcf_nn_eval_synthetic.argtypes = [vp, C.POINTER(Optics), ull, ull, i, i, C.POINTER(Result), vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
     L.gcf_background1d.argtypes = [vp, vp, i, i, vp, C.POINTER(i)]
     L.gcf_remove_background1d.argtypes = [vp, vp, i, vp, i, i, i]
@@ -329,7 +355,9 @@ class Context:
         out = [res[i] for i in range(n)]
         return (out, full) if want_full else out
 
-    def run_batch(self, images, pixel_sizes, optics: Optics):
+    def run_batch(self, images, pixel_sizes, optics: Optics, mode: int = GCF_SEARCH_PLAIN):
+        """Independent searches of micrographs of any size (one call);
+        mode: GCF_SEARCH_PLAIN, GCF_SEARCH_BF16 or GCF_SEARCH_LEARNED."""
         imgs = [_as_f32(a) for a in images]
         n = len(imgs)
         items = (Item * n)()
@@ -341,8 +369,77 @@ class Context:
                 raise ValueError("images must all be on the host or all on the GPU")
             items[k] = Item(p, a.shape[1], a.shape[0], float(pixel_sizes[k]))
         res = (Result * n)()
-        _check(self.L.gcf_run_batch(self._h, items, n, dev, C.byref(optics), res), self._h)
+        _check(self.L.gcf_run_batch_mode(self._h, items, n, dev, C.byref(optics), int(mode), res), self._h)
         return [res[i] for i in range(n)]
+
+    def fast_counts(self):
+        """Contraction work of the last batched call (gcf_get_fast_counts)."""
+        c = (C.c_longlong * 4)()
+        _check(self.L.gcf_get_fast_counts(self._h, c), self._h)
+        return dict(zip(["table_cand", "tensor_macs", "rescored", "fallbacks"], list(c)))
+
+    # -- learned initialiser ------------------------------------------------------
+    def nn_init(self, seed: int = 0):
+        _check(self.L.gcf_nn_init(self._h, seed), self._h)
+
+    def nn_params(self) -> np.ndarray:
+        n = self.L.gcf_nn_param_count()
+        out = np.zeros(n, np.float32)
+        _check(self.L.gcf_nn_get_params(self._h, out.ctypes.data, n), self._h)
+        return out
+
+    def nn_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        _check(self.L.gcf_nn_set_params(self._h, p.ctypes.data, p.size), self._h)
+
+    def save_weights(self, path: str):
+        _check(self.L.gcf_nn_save(self._h, path.encode()), self._h)
+
+    def load_weights(self, path: str):
+        _check(self.L.gcf_nn_load(self._h, path.encode()), self._h)
+
+    def set_learned_threshold(self, tau: float):
+        _check(self.L.gcf_set_learned_threshold(self._h, tau), self._h)
+
+    def nn_train(self, optics: Optics, steps: int, batch: int, seed: int, first: int = 0, lr: float = 1e-3):
+        losses = np.zeros(steps, np.float32)
+        _check(self.L.gcf_nn_train(self._h, C.byref(optics), steps, batch, seed, first, lr,
+                                   losses.ctypes.data), self._h)
+        return losses
+
+    def nn_synth_inputs(self, optics: Optics, seed: int, first: int, n: int):
+        x1 = np.zeros((n, 256), np.float32)
+        x2 = np.zeros((n, 256, 256), np.float32)
+        t = np.zeros((n, 3), np.float32)
+        p = np.zeros((n, 8), np.float32)
+        _check(self.L.gcf_nn_synth_inputs(self._h, C.byref(optics), seed, first, n, x1.ctypes.data,
+                                          x2.ctypes.data, t.ctypes.data, p.ctypes.data), self._h)
+        return x1, x2, t, p
+
+    def nn_forward_backward(self, x1, x2, target):
+        x1 = np.ascontiguousarray(x1, np.float32)
+        x2 = np.ascontiguousarray(x2, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        n = x1.shape[0]
+        loss = np.zeros(1, np.float32)
+        grads = np.zeros(self.L.gcf_nn_param_count(), np.float32)
+        pred = np.zeros((n, 3), np.float32)
+        _check(self.L.gcf_nn_forward_backward(self._h, x1.ctypes.data, x2.ctypes.data, target.ctypes.data, n,
+                                              loss.ctypes.data, grads.ctypes.data, pred.ctypes.data), self._h)
+        return float(loss[0]), grads, pred
+
+    def nn_eval_synthetic(self, optics: Optics, seed: int, first: int, n: int, mode: int):
+        res = (Result * n)()
+        p = np.zeros((n, 8), np.float32)
+        _check(self.L.gcf_nn_eval_synthetic(self._h, C.byref(optics), seed, first, n, int(mode), res,
+                                            p.ctypes.data), self._h)
+        return [res[i] for i in range(n)], p
+
+    def fast_times(self):
+        """Device ms of the contraction stages of the last batched call."""
+        t = (C.c_float * 4)()
+        _check(self.L.gcf_get_fast_times(self._h, t), self._h)
+        return dict(zip(["bin", "product", "table", "finish"], list(t)))
 
     def stage_times(self):
         t = (C.c_float * 7)()

@@ -160,6 +160,32 @@ struct gcf_ctx {
     // GBackground1D
     DBuf<float> bg_spec, bg_curve;
     DBuf<int> bg_start;
+
+    // BF16 candidate contraction (search mode GCF_SEARCH_BF16 / _LEARNED)
+    PolarGrid model_grid{};          // grid the model rows were made for
+    bool have_model = false;
+    DBuf<__nv_bfloat16> cA, cA2, cB, cE;
+    DBuf<float> cP, cDz;
+    DBuf<double> cSS;
+    DBuf<int2> cRows, cTiles;
+    DBuf<int> cNtiles, cErr;
+    DBuf<float4> cPrior;
+    int gemm_bn = 256, gemm_stages = 4;     // tile of the P product (tuned)
+    float contract_dz = 10.0f;              // defocus row step, Angstrom
+    int contract_ns = 512, contract_nth = 64;
+    // [0] candidates scored on the table, [1] tensor-core multiply-adds,
+    // [2] candidates re-scored in FP32, [3] learned searches that fell back
+    long long fast_counts[4] = {0, 0, 0, 0};
+    // events around the contraction stages: bin | product | table | FP32 finish
+    cudaEvent_t fev[5] = {};
+    float fast_ms[4] = {0, 0, 0, 0};
+
+    // learned initialiser
+    NnNet* nn = nullptr;
+    bool nn_ready = false;            // weights set (loaded, trained or given)
+    float learned_tau = 0.1f;         // refined CC below which the full search runs
+    DBuf<__nv_bfloat16> nx1, nx2;     // network inputs of a chunk of jobs
+    DBuf<float> npx, nparams, ntarget, nloss;
 };
 
 namespace {
@@ -317,6 +343,10 @@ gcf_status build_tile_tables(gcf_ctx* ctx)
     }
     CK(ctx->tw512.ensure(T));
     CK(cudaMemcpy(ctx->tw512.p, tw.data(), T * sizeof(float2), cudaMemcpyHostToDevice));
+    // A copy from pageable memory may return before its DMA lands, and the
+    // context's streams are non-blocking (not ordered after these copies):
+    // wait for the tables once, at creation.
+    CK(cudaDeviceSynchronize());
     return GCF_OK;
 }
 
@@ -377,12 +407,14 @@ gcf_status get_band(gcf_ctx* ctx, const gcf_optics& op, float px_n, int* slot)
         delete b;
         return cuda_fail(ctx, e, "band alloc");
     }
-    CK(cudaMemcpy(b->idx.p, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->a.p, va.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->d.p, vd.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->env.p, ve.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->c2t.p, vc.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->s2t.p, vs.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    // On the compute stream, so the kernels that read the band are ordered
+    // after the copies (a pageable source is staged before the call returns).
+    CK(cudaMemcpyAsync(b->idx.p, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(b->a.p, va.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(b->d.p, vd.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(b->env.p, ve.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(b->c2t.p, vc.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(b->s2t.p, vs.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
     b->dev.n = b->n;
     b->dev.cx = cx;
     b->dev.cy = cy;
@@ -405,7 +437,7 @@ gcf_status upload_bands(gcf_ctx* ctx)
     std::vector<BandDev> v;
     for (auto* b : ctx->bands) v.push_back(b->dev);
     CK(ctx->d_bands.ensure(v.size()));
-    CK(cudaMemcpy(ctx->d_bands.p, v.data(), v.size() * sizeof(BandDev), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->d_bands.p, v.data(), v.size() * sizeof(BandDev), cudaMemcpyHostToDevice, ctx->st));
     ctx->bands_dirty = false;
     return GCF_OK;
 }
@@ -928,6 +960,351 @@ gcf_status run_search(gcf_ctx* ctx, const std::vector<JobSpec>& specs, std::vect
     return run_search_collect(ctx, pend, out);
 }
 
+// ---------------------------------------------------------------------------
+// BF16 contraction search (mode 4 jobs).  Every step is enqueued on ctx->st
+// with no host round trip until the results are read back:
+//   polar binning of the ctf spectra -> tile plan -> P = A B^T and
+//   Dz = E A2^T on the tensor cores -> table search (1D scan + mIterate, or
+//   the learned window) -> FP32 re-score of the table's best candidates and
+//   kLocalPasses local passes (k_eval2d) -> GSpectralCC2D resolution ->
+//   result rows.
+// `prior` (device, nullable): per job (mean A, ratio, angle, window scale);
+// jobs with prior.x > 0 search the window around it.
+
+// The batch's polar grid: the s^2 band common to all jobs (the 2D band of
+// CFindDefocus2D::Setup2, FindCTF/CFindDefocus2D.cpp:86-92, in 1/A), and the
+// defocus rows that cover every job's search.
+PolarGrid polar_grid(gcf_ctx* ctx, const std::vector<JobSpec>& specs)
+{
+    double s_lo = 0.0, s_hi = 1e30, z_lo = 1e30, z_hi = 0.0;
+    for (const JobSpec& sp : specs) {
+        float rr[2];
+        res_range_of(sp.px_n, rr);
+        s_lo = std::max(s_lo, 1.0 / rr[0]);
+        s_hi = std::min(s_hi, 1.0 / rr[1]);
+        const double px2 = (double)sp.px_n * sp.px_n;
+        z_lo = std::min(z_lo, 3000.0 * px2 * 0.82 * 0.96);
+        z_hi = std::max(z_hi, 30000.0 * px2 * 1.2 * 1.04);
+    }
+    PolarGrid g{};
+    g.ns = ctx->contract_ns;
+    g.nth = ctx->contract_nth;
+    g.s2_lo = (float)(s_lo * s_lo);
+    g.ds2 = (float)((s_hi * s_hi - s_lo * s_lo) / g.ns);
+    g.dz = ctx->contract_dz;
+    g.z0 = (float)(std::floor(z_lo / g.dz) * g.dz);
+    g.nz = (int)std::ceil((z_hi - g.z0) / g.dz) + 2;
+    g.nz = (g.nz + 127) / 128 * 128;
+    const gcf_optics& op = specs[0].optics;
+    const double wl = 12.26 / std::sqrt((double)op.kv * 1000.0 + 0.9784 * (double)op.kv * op.kv);
+    g.wl = (float)wl;
+    g.cs = (float)((double)op.cs_mm * 1e7);
+    const float ac = op.amp_contrast;
+    g.amp_phase = (float)atanf(ac / sqrtf(1.0f - ac * ac)) + specs[0].phase_deg * 0.01745329f;
+    return g;
+}
+
+bool same_grid(const PolarGrid& a, const PolarGrid& b)
+{
+    return a.ns == b.ns && a.nth == b.nth && a.nz == b.nz && a.s2_lo == b.s2_lo && a.ds2 == b.ds2 &&
+           a.z0 == b.z0 && a.dz == b.dz && a.wl == b.wl && a.cs == b.cs && a.amp_phase == b.amp_phase;
+}
+
+gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, const float4* prior,
+                            SearchPending& pend)
+{
+    const int nj = (int)specs.size();
+    pend.nj = nj;
+    pend.st = ctx->st;
+    pend.band.assign(nj, 0);
+    if (nj == 0) return GCF_OK;
+    const int T = ctx->tile, cx = T / 2 + 1;
+    const size_t cmp_n = (size_t)cx * T;
+    std::vector<SearchJob> jh(nj);
+    std::vector<int> soff(nj);
+    int tot = 0, max_band = 0;
+    for (int j = 0; j < nj; ++j) {
+        const JobSpec& sp = specs[j];
+        SearchJob& J = jh[j];
+        std::memset(&J, 0, sizeof(J));
+        int slot = -1;
+        CKS(get_band(ctx, sp.optics, sp.px_n, &slot));
+        J.mic = sp.mic;
+        J.band = slot;
+        J.mode = 4;
+        J.o = make_optics(sp.optics, sp.px_n);
+        J.ext_phase_in = sp.phase_deg;
+        J.held_phase = sp.held_phase;
+        J.step = STEP_DONE;
+        soff[j] = tot;
+        const int bn = ctx->bands[slot]->n;
+        tot += bn;
+        max_band = std::max(max_band, bn);
+    }
+    CKS(upload_bands(ctx));
+    const int max_chunks = std::max(1, (max_band + kEvalChunk - 1) / kEvalChunk);
+    CK(ctx->jobs.ensure(nj));
+    CK(ctx->spec_off.ensure(nj));
+    CK(ctx->band_spec.ensure(std::max(tot, 1)));
+    CK(ctx->sum_ss.ensure(nj));
+    CK(ctx->cand.ensure((size_t)nj * kMaxCand));
+    CK(ctx->cval.ensure((size_t)nj * kMaxCand));
+    CK(ctx->part.ensure((size_t)nj * kMaxCand * max_chunks));
+    CK(ctx->cc_res.ensure((size_t)nj * cx));
+    CK(ctx->d_res.ensure(nj));
+    CK(ctx->arrive.ensure(nj));
+    CK(cudaMemsetAsync(ctx->arrive.p, 0, nj * sizeof(int), ctx->st));
+    CK(cudaMemcpyAsync(ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->spec_off.p, soff.data(), nj * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    launch_band_gather(ctx->ctf.p, (int)cmp_n, ctx->jobs.p, ctx->d_bands.p, ctx->spec_off.p, nj, ctx->band_spec.p,
+                       ctx->sum_ss.p, ctx->st);
+    CKL();
+    // model rows of the grid (kept while the grid and optics stay the same)
+    const PolarGrid g = polar_grid(ctx, specs);
+    if (!ctx->have_model || !same_grid(g, ctx->model_grid)) {
+        CK(ctx->cA.ensure((size_t)g.nz * g.ns));
+        CK(ctx->cA2.ensure((size_t)g.nz * g.ns));
+        launch_polar_model(g, ctx->cA.p, ctx->cA2.p, ctx->st);
+        CKL();
+        ctx->launches += 1;
+        ctx->model_grid = g;
+        ctx->have_model = true;
+    }
+    const long long ncols = (long long)nj * g.nth;
+    CK(ctx->cB.ensure((size_t)ncols * g.ns));
+    CK(ctx->cE.ensure((size_t)nj * g.ns));
+    CK(ctx->cSS.ensure(nj));
+    CK(ctx->cP.ensure((size_t)g.nz * ncols));
+    CK(ctx->cDz.ensure((size_t)nj * g.nz));
+    CK(ctx->cRows.ensure(nj));
+    const int bn = ctx->gemm_bn;
+    if (bn < g.nth || bn % g.nth) return fail(ctx, GCF_ERR_INVALID_ARG, "contraction tile narrower than a job's angle bins");
+    const int ncb = (int)((ncols + bn - 1) / bn);
+    const int max_tiles = ncb * (g.nz / 128);
+    CK(ctx->cTiles.ensure(max_tiles));
+    CK(ctx->cNtiles.ensure(1));
+    CK(ctx->cErr.ensure(1));
+    for (auto& e : ctx->fev)
+        if (!e) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ctx->fev[0], ctx->st));
+    CK(launch_polar_bin(ctx->ctf.p, T, ctx->jobs.p, nj, g, ctx->cB.p, ctx->cE.p, ctx->cSS.p, ctx->st));
+    launch_job_rows(ctx->jobs.p, nj, prior, g, ctx->cRows.p, ctx->st);
+    CKL();
+    CK(cudaMemsetAsync(ctx->cNtiles.p, 0, sizeof(int), ctx->st));
+    CK(cudaMemsetAsync(ctx->cErr.p, 0, sizeof(int), ctx->st));
+    CK(cudaEventRecord(ctx->fev[1], ctx->st));
+    launch_plan_tiles(ctx->cRows.p, nj, g.nth, g.nz, bn, ctx->cTiles.p, ctx->cNtiles.p, max_tiles, ctx->st);
+    CKL();
+    // P = A B^T over the planned tiles; Dz = E A2^T (every row of every job)
+    GemmArgs ga;
+    ga.M = g.nz;
+    ga.N = (int)ncols;
+    ga.K = g.ns;
+    ga.D = ctx->cP.p;
+    ga.ldd = ncols;
+    ga.tiles = ctx->cTiles.p;
+    ga.ntiles = ctx->cNtiles.p;
+    ga.err = ctx->cErr.p;
+    CK(launch_umma_gemm(ctx->cA.p, g.ns, ctx->cB.p, g.ns, ga, bn, ctx->gemm_stages, max_tiles, ctx->st));
+    GemmArgs gd;
+    gd.M = nj;
+    gd.N = g.nz;
+    gd.K = g.ns;
+    gd.D = ctx->cDz.p;
+    gd.ldd = g.nz;
+    gd.err = ctx->cErr.p;
+    CK(launch_umma_gemm(ctx->cE.p, g.ns, ctx->cA2.p, g.ns, gd, 256, 4, 0, ctx->st));
+    ctx->launches += 6;
+    CK(cudaEventRecord(ctx->fev[2], ctx->st));
+    TableArgs ta;
+    ta.jobs = ctx->jobs.p;
+    ta.njobs = nj;
+    ta.P = ctx->cP.p;
+    ta.ldp = ncols;
+    ta.Dz = ctx->cDz.p;
+    ta.ldd = g.nz;
+    ta.ss = ctx->cSS.p;
+    ta.g = g;
+    ta.rows = ctx->cRows.p;
+    ta.prior = prior;
+    ta.cand = ctx->cand.p;
+    ta.cval = ctx->cval.p;
+    launch_table_search(ta, ctx->st);
+    CKL();
+    ctx->launches += 1;
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    CK(cudaEventRecord(ctx->fev[3], ctx->st));
+    EvalArgs a;
+    a.jobs = ctx->jobs.p;
+    a.bands = ctx->d_bands.p;
+    a.band_spec = ctx->band_spec.p;
+    a.sum_ss = ctx->sum_ss.p;
+    a.spec_off = ctx->spec_off.p;
+    a.cand = ctx->cand.p;
+    a.cval = ctx->cval.p;
+    a.part = ctx->part.p;
+    a.arrive = ctx->arrive.p;
+    a.max_chunks = max_chunks;
+    a.njobs = nj;
+    // FP32 re-score + local passes: candidate blocks of 16 (<= 27 per step)
+    for (int k = 0; k < 1 + kLocalPasses; ++k) {
+        launch_eval2d(a, 2, max_band, ctx->st);
+        CKL();
+        ctx->launches += 1;
+    }
+    CK(cudaEventRecord(ctx->fev[4], ctx->st));
+    CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
+    launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p, ctx->ring_geo.p,
+                   ctx->ring_sums.p, ctx->cc_res.p, ctx->st);
+    CKL();
+    launch_shell_select(ctx->jobs.p, nj, ctx->cc_res.p, cx, T, ctx->st);
+    CKL();
+    CK(ctx->d_counts.ensure(3 * (size_t)nj));
+    launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->d_counts.p, ctx->st);
+    CKL();
+    ctx->launches += 4;
+    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    for (int j = 0; j < nj; ++j) pend.band[j] = jh[j].band;
+    return GCF_OK;
+}
+
+// Reads back a contraction search: results, per-job work, the product's
+// error flag.
+gcf_status run_fast_collect(gcf_ctx* ctx, const SearchPending& pend, std::vector<gcf_result>& out,
+                            std::vector<int>* n_table)
+{
+    CKS(run_search_collect(ctx, pend, out));
+    const int nj = pend.nj;
+    if (nj == 0) return GCF_OK;
+    std::vector<SearchJob> jh(nj);
+    int err = 0, nt = 0;
+    CK(cudaMemcpyAsync(jh.data(), ctx->jobs.p, nj * sizeof(SearchJob), cudaMemcpyDeviceToHost, pend.st));
+    CK(cudaMemcpyAsync(&err, ctx->cErr.p, sizeof(int), cudaMemcpyDeviceToHost, pend.st));
+    CK(cudaMemcpyAsync(&nt, ctx->cNtiles.p, sizeof(int), cudaMemcpyDeviceToHost, pend.st));
+    CK(cudaStreamSynchronize(pend.st));
+    if (err) return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core product: a bounded wait gave up");
+    for (int k = 0; k < 4; ++k) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, ctx->fev[k], ctx->fev[k + 1]) == cudaSuccess) ctx->fast_ms[k] += t;
+    }
+    cudaGetLastError();
+    // tensor-core multiply-adds: the planned tiles of P and all of Dz
+    const PolarGrid& g = ctx->model_grid;
+    ctx->fast_counts[1] += (long long)nt * 128 * ctx->gemm_bn * g.ns + (long long)nj * g.nz * g.ns;
+    if (n_table) n_table->assign(nj, 0);
+    for (int j = 0; j < nj; ++j) {
+        ctx->fast_counts[0] += jh[j].n_table;
+        ctx->fast_counts[2] += jh[j].n_cand2d;
+        if (n_table) (*n_table)[j] = jh[j].n_table;
+    }
+    return GCF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Searches of the spectra in slots 0 .. n-1 (already post-processed) with
+// the chosen method; px_n: pixel size of each slot, optics with the raw
+// pixel sizes in px_raw (unused by the searches themselves).
+constexpr int kNnChunk = 512;   // network inputs of at most this many jobs at once
+
+gcf_status nn_ensure(gcf_ctx* ctx)
+{
+    if (ctx->nn) return GCF_OK;
+    ctx->nn = nn_create();
+    if (!ctx->nn) return fail(ctx, GCF_ERR_NO_MEMORY, "network buffers");
+    return GCF_OK;
+}
+
+// Learned priors (mean, ratio, angle, window) of slots 0 .. n-1 into cPrior.
+gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
+{
+    const int n = (int)px_n.size();
+    CKS(nn_ensure(ctx));
+    if (!ctx->nn_ready) return fail(ctx, GCF_ERR_STATE, "learned search: no network weights (gcf_nn_load / gcf_nn_train)");
+    CK(ctx->npx.ensure(n));
+    CK(ctx->cPrior.ensure(n));
+    CK(ctx->nx1.ensure((size_t)kNnChunk * kNnProfile));
+    CK(ctx->nx2.ensure((size_t)kNnChunk * kNnMap * kNnMap));
+    CK(cudaMemcpyAsync(ctx->npx.p, px_n.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    const size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
+    for (int c0 = 0; c0 < n; c0 += kNnChunk) {
+        const int cn = std::min(kNnChunk, n - c0);
+        CK(launch_nn_input(ctx->ctf.p + cmp_n * c0, ctx->tile, ctx->npx.p + c0, 1, cn, ctx->nx1.p, ctx->nx2.p, ctx->st));
+        CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, cn, ctx->st));
+        launch_prior(nn_pred(ctx->nn), kNnPredPitch, cn, ctx->cPrior.p + c0, ctx->st);
+        CKL();
+        ctx->launches += 13;
+    }
+    return GCF_OK;
+}
+
+gcf_status search_slots(gcf_ctx* ctx, const std::vector<float>& px_n, const gcf_optics& op, int mode,
+                        std::vector<gcf_result>& out)
+{
+    const int n = (int)px_n.size();
+    std::vector<JobSpec> js(n);
+    for (int i = 0; i < n; ++i) {
+        std::memset(&js[i], 0, sizeof(JobSpec));
+        js[i].mic = i;
+        js[i].mode = mode == GCF_SEARCH_PLAIN ? 0 : 4;
+        js[i].optics = op;
+        js[i].px_n = px_n[i];
+        js[i].phase_deg = op.ext_phase_deg;
+        js[i].phase_range = mode == GCF_SEARCH_PLAIN ? fmaxf(op.ext_phase_range, 0.0f) : 0.0f;
+    }
+    if (mode == GCF_SEARCH_PLAIN) return run_search(ctx, js, out);
+    const float4* prior = nullptr;
+    if (mode == GCF_SEARCH_LEARNED) {
+        CKS(learned_priors(ctx, px_n));
+        prior = ctx->cPrior.p;
+    }
+    SearchPending pend;
+    CKS(run_fast_enqueue(ctx, js, prior, pend));
+    CKS(run_fast_collect(ctx, pend, out, nullptr));
+    if (mode != GCF_SEARCH_LEARNED) return GCF_OK;
+    // Fallback to the full contraction search where the learned window's
+    // refined result is not trusted: its CC is below the threshold, or its
+    // mean defocus ends within one local step of the window's edge (the
+    // optimum may lie outside).
+    std::vector<SearchJob> jh(n);
+    CK(cudaMemcpy(jh.data(), ctx->jobs.p, n * sizeof(SearchJob), cudaMemcpyDeviceToHost));
+    std::vector<JobSpec> redo;
+    std::vector<int> idx;
+    for (int i = 0; i < n; ++i) {
+        const SearchJob& J = jh[i];
+        const float edge = 2.0f * fmaxf(20.0f, 0.105f * J.df_mean / 31.0f);
+        const bool at_edge = J.df_mean - J.df_range[0] < edge || J.df_range[1] - J.df_mean < edge;
+        if (out[i].score < ctx->learned_tau || at_edge) {
+            redo.push_back(js[i]);
+            idx.push_back(i);
+        }
+    }
+    ctx->fast_counts[3] += (long long)redo.size();
+    if (redo.empty()) return GCF_OK;
+    std::vector<gcf_result> r2;
+    SearchPending p2;
+    CKS(run_fast_enqueue(ctx, redo, nullptr, p2));
+    CKS(run_fast_collect(ctx, p2, r2, nullptr));
+    for (size_t k = 0; k < idx.size(); ++k) out[idx[k]] = r2[k];
+    return GCF_OK;
+}
+
+// Synthetic raw spectra of samples first .. first + n - 1 of the generator
+// (seed) into slots 0 .. n-1, post-processed like measured ones; their
+// pixel sizes to px_n and parameters (8 floats each) to nparams.
+gcf_status synth_slots(gcf_ctx* ctx, const gcf_optics& op, unsigned long long seed, unsigned long long first, int n)
+{
+    CKS(spectra_alloc(ctx, n));
+    CK(ctx->nparams.ensure((size_t)n * 8));
+    CK(ctx->ntarget.ensure((size_t)n * 3));
+    launch_synth_params(seed, first, n, ctx->nparams.p, ctx->ntarget.p, ctx->st);
+    launch_synth_raw(seed, first, ctx->nparams.p, n, ctx->tile, make_optics(op, 1.0f), ctx->raw.p, ctx->st);
+    CKL();
+    CKS(spectra_post(ctx, n));
+    ctx->launches += 2;
+    return GCF_OK;
+}
+
 gcf_status set_device(gcf_ctx* ctx)
 {
     CK(cudaSetDevice(ctx->dev));
@@ -1266,6 +1643,27 @@ void gcf_destroy(gcf_ctx* ctx)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
     for (auto& ev : ctx->kev) cudaEventDestroy(ev);
+    for (auto& ev : ctx->fev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->nn) nn_destroy(ctx->nn);
+    ctx->nx1.release();
+    ctx->nx2.release();
+    ctx->npx.release();
+    ctx->nparams.release();
+    ctx->ntarget.release();
+    ctx->nloss.release();
+    ctx->cA.release();
+    ctx->cA2.release();
+    ctx->cB.release();
+    ctx->cE.release();
+    ctx->cP.release();
+    ctx->cDz.release();
+    ctx->cSS.release();
+    ctx->cRows.release();
+    ctx->cTiles.release();
+    ctx->cNtiles.release();
+    ctx->cErr.release();
+    ctx->cPrior.release();
     if (ctx->st_copy) cudaStreamDestroy(ctx->st_copy);
     if (ctx->st_search) cudaStreamDestroy(ctx->st_search);
     if (ctx->st_solo) cudaStreamDestroy(ctx->st_solo);
@@ -1965,6 +2363,264 @@ gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_devi
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     return st;
+}
+
+gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
+                              const gcf_optics* optics, int mode, gcf_result* results)
+{
+    if (mode == GCF_SEARCH_PLAIN) return gcf_run_batch(ctx, items, n, on_device, optics, results);
+    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
+    if (mode != GCF_SEARCH_BF16 && mode != GCF_SEARCH_LEARNED) return GCF_ERR_INVALID_ARG;
+    if (optics->ext_phase_range > 0) {
+        // the table search has no extra-phase dimension: phase-plate data
+        // take the plain search
+        return gcf_run_batch(ctx, items, n, on_device, optics, results);
+    }
+    if (mode == GCF_SEARCH_LEARNED && !ctx->nn_ready)
+        return fail(ctx, GCF_ERR_STATE, "learned search: no network weights (gcf_nn_load / gcf_nn_train)");
+    std::vector<const float*> imgs(n);
+    std::vector<int> ws(n), hs(n);
+    std::vector<float> pxs(n);
+    for (int i = 0; i < n; ++i) {
+        if (!items[i].image || items[i].width <= 0 || items[i].height <= 0 || !(items[i].pixel_size > 0))
+            return GCF_ERR_INVALID_ARG;
+        imgs[i] = items[i].image;
+        ws[i] = items[i].width;
+        hs[i] = items[i].height;
+        pxs[i] = items[i].pixel_size;
+    }
+    CKS(set_device(ctx));
+    for (float& t : ctx->stage_ms) t = 0.0f;
+    for (long long& c : ctx->search_counts) c = 0;
+    for (long long& c : ctx->fast_counts) c = 0;
+    for (float& t : ctx->fast_ms) t = 0.0f;
+    ctx->kev_used = 0;
+    ctx->launches = 0;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, ctx->st));
+    std::vector<MicImage> mics;
+    gcf_status st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics);
+    if (st == GCF_OK) {
+        std::vector<float> pxn(n);
+        for (int i = 0; i < n; ++i) pxn[i] = mics[i].px_n;
+        std::vector<gcf_result> r;
+        st = search_slots(ctx, pxn, *optics, mode, r);
+        if (st == GCF_OK)
+            for (int i = 0; i < n; ++i) results[i] = r[i];
+    }
+    cudaEventRecord(t1, ctx->st);
+    cudaEventSynchronize(t1);
+    if (st == GCF_OK) accumulate_stage_times(ctx);
+    float tt = 0;
+    cudaEventElapsedTime(&tt, t0, t1);
+    ctx->stage_ms[6] = tt;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// Learned initialiser
+// ---------------------------------------------------------------------------
+size_t gcf_nn_param_count(void) { return nn_param_count(); }
+
+gcf_status gcf_nn_init(gcf_ctx* ctx, unsigned long long seed)
+{
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    CKS(nn_ensure(ctx));
+    CK(nn_init_random(ctx->nn, seed, ctx->st));
+    ctx->nn_ready = true;
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_set_params(gcf_ctx* ctx, const float* params, size_t n)
+{
+    if (!ctx || !params || n != nn_param_count()) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    CKS(nn_ensure(ctx));
+    CK(nn_set_params(ctx->nn, params, ctx->st));
+    ctx->nn_ready = true;
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_get_params(gcf_ctx* ctx, float* params, size_t n)
+{
+    if (!ctx || !params || n != nn_param_count()) return GCF_ERR_INVALID_ARG;
+    if (!ctx->nn) return fail(ctx, GCF_ERR_STATE, "no network");
+    CKS(set_device(ctx));
+    CK(nn_get_params(ctx->nn, params, ctx->st));
+    return GCF_OK;
+}
+
+static const char kNnMagic[8] = {'G', 'C', 'F', 'N', 'N', '0', '0', '1'};
+
+gcf_status gcf_nn_save(gcf_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return GCF_ERR_INVALID_ARG;
+    const size_t n = nn_param_count();
+    std::vector<float> h(n);
+    CKS(gcf_nn_get_params(ctx, h.data(), n));
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(ctx, GCF_ERR_IO, "cannot open the weights file for writing");
+    unsigned long long cnt = n;
+    bool ok = fwrite(kNnMagic, 1, 8, f) == 8 && fwrite(&cnt, sizeof(cnt), 1, f) == 1 &&
+              fwrite(h.data(), sizeof(float), n, f) == n;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? GCF_OK : fail(ctx, GCF_ERR_IO, "weights file write failed");
+}
+
+gcf_status gcf_nn_load(gcf_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return GCF_ERR_INVALID_ARG;
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(ctx, GCF_ERR_IO, "cannot open the weights file");
+    char magic[8];
+    unsigned long long cnt = 0;
+    const size_t n = nn_param_count();
+    std::vector<float> h(n);
+    bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kNnMagic, 8) == 0 &&
+              fread(&cnt, sizeof(cnt), 1, f) == 1 && cnt == n && fread(h.data(), sizeof(float), n, f) == n;
+    fclose(f);
+    if (!ok) return fail(ctx, GCF_ERR_IO, "not a weights file of this network");
+    return gcf_nn_set_params(ctx, h.data(), n);
+}
+
+gcf_status gcf_set_learned_threshold(gcf_ctx* ctx, float tau)
+{
+    if (!ctx || !(tau >= -1.0f && tau <= 1.0f)) return GCF_ERR_INVALID_ARG;
+    ctx->learned_tau = tau;
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_train(gcf_ctx* ctx, const gcf_optics* optics, int steps, int batch, unsigned long long seed,
+                        unsigned long long first, float lr, float* losses)
+{
+    if (!ctx || !valid_optics(optics) || steps <= 0 || batch <= 0 || batch > 4096 || !(lr > 0)) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    CKS(nn_ensure(ctx));
+    if (!ctx->nn_ready) {
+        CK(nn_init_random(ctx->nn, seed ^ 0x9E3779B97F4A7C15ull, ctx->st));
+        ctx->nn_ready = true;
+    }
+    CK(ctx->nloss.ensure(steps));
+    CK(cudaMemsetAsync(ctx->nloss.p, 0, steps * sizeof(float), ctx->st));
+    CK(ctx->nx1.ensure((size_t)batch * kNnProfile));
+    CK(ctx->nx2.ensure((size_t)batch * kNnMap * kNnMap));
+    CK(cudaMemsetAsync(nn_err_flag(ctx->nn), 0, sizeof(int), ctx->st));
+    for (int k = 0; k < steps; ++k) {
+        const unsigned long long f0 = first + (unsigned long long)k * batch;
+        CKS(synth_slots(ctx, *optics, seed, f0, batch));
+        CK(launch_nn_input(ctx->ctf.p, ctx->tile, ctx->nparams.p + 3, 8, batch, ctx->nx1.p, ctx->nx2.p, ctx->st));
+        CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, batch, ctx->st));
+        CK(nn_backward(ctx->nn, ctx->ntarget.p, batch, ctx->nloss.p + k, ctx->st));
+        // cosine decay to 5 % of lr
+        const float c = 0.5f * (1.0f + std::cos(3.14159265f * (float)k / (float)steps));
+        CK(nn_adam(ctx->nn, lr * (0.05f + 0.95f * c), ctx->st));
+    }
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, nn_err_flag(ctx->nn), sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    if (losses) CK(cudaMemcpyAsync(losses, ctx->nloss.p, steps * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (err) return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core product: a bounded wait gave up");
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_synth_inputs(gcf_ctx* ctx, const gcf_optics* optics, unsigned long long seed,
+                               unsigned long long first, int n, float* x1, float* x2, float* target, float* params)
+{
+    if (!ctx || !valid_optics(optics) || n <= 0 || n > kNnChunk) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    CKS(synth_slots(ctx, *optics, seed, first, n));
+    CK(ctx->nx1.ensure((size_t)n * kNnProfile));
+    CK(ctx->nx2.ensure((size_t)n * kNnMap * kNnMap));
+    CK(launch_nn_input(ctx->ctf.p, ctx->tile, ctx->nparams.p + 3, 8, n, ctx->nx1.p, ctx->nx2.p, ctx->st));
+    std::vector<__nv_bfloat16> h1((size_t)n * kNnProfile), h2((size_t)n * kNnMap * kNnMap);
+    CK(cudaMemcpyAsync(h1.data(), ctx->nx1.p, h1.size() * 2, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h2.data(), ctx->nx2.p, h2.size() * 2, cudaMemcpyDeviceToHost, ctx->st));
+    if (target) CK(cudaMemcpyAsync(target, ctx->ntarget.p, (size_t)n * 3 * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (params) CK(cudaMemcpyAsync(params, ctx->nparams.p, (size_t)n * 8 * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (x1)
+        for (size_t i = 0; i < h1.size(); ++i) x1[i] = __bfloat162float(h1[i]);
+    if (x2)
+        for (size_t i = 0; i < h2.size(); ++i) x2[i] = __bfloat162float(h2[i]);
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_forward_backward(gcf_ctx* ctx, const float* x1, const float* x2, const float* target, int n,
+                                   float* loss, float* grads, float* pred)
+{
+    if (!ctx || !x1 || !x2 || !target || n <= 0 || n > kNnChunk) return GCF_ERR_INVALID_ARG;
+    if (!ctx->nn || !ctx->nn_ready) return fail(ctx, GCF_ERR_STATE, "no network weights");
+    CKS(set_device(ctx));
+    std::vector<__nv_bfloat16> h1((size_t)n * kNnProfile), h2((size_t)n * kNnMap * kNnMap);
+    for (size_t i = 0; i < h1.size(); ++i) h1[i] = __float2bfloat16_rn(x1[i]);
+    for (size_t i = 0; i < h2.size(); ++i) h2[i] = __float2bfloat16_rn(x2[i]);
+    CK(ctx->nx1.ensure(h1.size()));
+    CK(ctx->nx2.ensure(h2.size()));
+    CK(ctx->ntarget.ensure((size_t)n * 3));
+    CK(ctx->nloss.ensure(1));
+    CK(cudaMemcpyAsync(ctx->nx1.p, h1.data(), h1.size() * 2, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->nx2.p, h2.data(), h2.size() * 2, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->ntarget.p, target, (size_t)n * 3 * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(ctx->nloss.p, 0, sizeof(float), ctx->st));
+    CK(cudaMemsetAsync(nn_err_flag(ctx->nn), 0, sizeof(int), ctx->st));
+    CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, n, ctx->st));
+    CK(nn_backward(ctx->nn, ctx->ntarget.p, n, ctx->nloss.p, ctx->st));
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, nn_err_flag(ctx->nn), sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    if (loss) CK(cudaMemcpyAsync(loss, ctx->nloss.p, sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    if (pred)
+        CK(cudaMemcpy2DAsync(pred, 3 * sizeof(float), nn_pred(ctx->nn), kNnPredPitch * sizeof(float),
+                             3 * sizeof(float), n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (err) return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core product: a bounded wait gave up");
+    if (grads) CK(nn_get_grads(ctx->nn, grads, ctx->st));
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_eval_synthetic(gcf_ctx* ctx, const gcf_optics* optics, unsigned long long seed,
+                                 unsigned long long first, int n, int mode, gcf_result* results, float* params)
+{
+    if (!ctx || !valid_optics(optics) || n <= 0 || !results) return GCF_ERR_INVALID_ARG;
+    if (mode != GCF_SEARCH_PLAIN && mode != GCF_SEARCH_BF16 && mode != GCF_SEARCH_LEARNED) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    for (long long& c : ctx->search_counts) c = 0;
+    for (long long& c : ctx->fast_counts) c = 0;
+    for (float& t : ctx->fast_ms) t = 0.0f;
+    gcf_optics op = *optics;
+    op.ext_phase_range = 0.0f;
+    for (int c0 = 0; c0 < n; c0 += kNnChunk) {
+        const int cn = std::min(kNnChunk, n - c0);
+        CKS(synth_slots(ctx, op, seed, first + (unsigned long long)c0, cn));
+        std::vector<float> prm((size_t)cn * 8);
+        CK(cudaMemcpyAsync(prm.data(), ctx->nparams.p, prm.size() * 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        std::vector<float> pxn(cn);
+        for (int i = 0; i < cn; ++i) pxn[i] = prm[(size_t)i * 8 + 3];
+        std::vector<gcf_result> r;
+        CKS(search_slots(ctx, pxn, op, mode, r));
+        for (int i = 0; i < cn; ++i) results[c0 + i] = r[i];
+        if (params) std::memcpy(params + (size_t)c0 * 8, prm.data(), prm.size() * 4);
+    }
+    return GCF_OK;
+}
+
+gcf_status gcf_get_fast_counts(gcf_ctx* ctx, long long counts[4])
+{
+    if (!ctx || !counts) return GCF_ERR_INVALID_ARG;
+    for (int i = 0; i < 4; ++i) counts[i] = ctx->fast_counts[i];
+    return GCF_OK;
+}
+
+gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[4])
+{
+    if (!ctx || !times_ms) return GCF_ERR_INVALID_ARG;
+    for (int i = 0; i < 4; ++i) times_ms[i] = ctx->fast_ms[i];
+    return GCF_OK;
 }
 
 gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7])

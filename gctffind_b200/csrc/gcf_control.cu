@@ -154,6 +154,18 @@ __device__ Cand cand_of(const SearchJob& J, int i, const float2* cval)
     case STEP_PHASE:
         c.phase = cval[i].x;
         break;
+    case STEP_RESCORE:   // the table's best candidates, in table order
+        c.dfmean = J.rs_df[i];
+        c.ast = J.rs_ast[i];
+        c.ang = J.rs_ang[i];
+        break;
+    case STEP_LOCAL: {   // 3 x 3 x 3 grid around the current best
+        const int a = i % 3 - 1, b = (i / 3) % 3 - 1, d = i / 9 - 1;
+        c.dfmean = J.df_mean + (float)a * J.loc_ddf;
+        c.ast = fmaxf(J.ast_ratio + (float)b * J.loc_dast, 0.0f);
+        c.ang = J.ast_angle + (float)d * J.loc_dang;
+        break;
+    }
     default:
         break;
     }
@@ -256,6 +268,10 @@ __device__ int prepare_step(SearchJob& J, float2* cval)
         }
         return k;
     }
+    case STEP_RESCORE:
+        return kRescore;
+    case STEP_LOCAL:
+        return 27;
     default:
         return 0;
     }
@@ -323,6 +339,36 @@ __device__ void finish_step(SearchJob& J, float best, int bi, float cc0, const f
         }
         J.iter += 1;
         J.step = (J.iter < 20) ? STEP_ASTMAG : STEP_DONE;
+        return;
+    case STEP_RESCORE:   // the best re-scored table candidate (first strict maximum)
+        if (bi >= 0) {
+            const Cand c = cand_of(J, bi, cval);
+            J.df_mean = c.dfmean;
+            J.ast_ratio = c.ast;
+            J.ast_angle = c.ang;
+            J.cc_max = best;
+        }
+        J.iter = 0;
+        J.step = STEP_LOCAL;
+        return;
+    case STEP_LOCAL:
+        if (bi >= 0 && best > J.cc_max) {
+            const Cand c = cand_of(J, bi, cval);
+            J.df_mean = c.dfmean;
+            J.ast_ratio = c.ast;
+            J.ast_angle = c.ang;
+            J.cc_max = best;
+        }
+        J.loc_ddf *= 0.5f;
+        J.loc_dast *= 0.5f;
+        J.loc_dang *= 0.5f;
+        J.iter += 1;
+        if (J.iter >= kLocalPasses) {
+            // the azimuth is defined modulo 180 degrees: report it in (-90, 90]
+            if (J.ast_angle > 90.0f) J.ast_angle -= 180.0f;
+            if (J.ast_angle <= -90.0f) J.ast_angle += 180.0f;
+            J.step = STEP_DONE;
+        }
         return;
     default:
         J.step = STEP_DONE;
@@ -746,7 +792,7 @@ __global__ void k_search1d(SearchJob* __restrict__ jobs, const float* __restrict
     const int j = blockIdx.x;
     if (threadIdx.x == 0) sJ = jobs[j];
     __syncthreads();
-    if (sJ.mode == 1) return;   // Refine has no 1D stage
+    if (sJ.mode == 1 || sJ.mode == 4) return;   // Refine and the contraction search have no 1D stage here
     const PixOptics o = sJ.o;
     const float* rad = radial + (size_t)sJ.mic * cx;
     // CFindDefocus1D::mCorrelate band (FindCTF/CFindDefocus1D.cpp:128-137)
@@ -891,7 +937,7 @@ __global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const i
         counts[3 * j + 2] = J.n_pairs1d;
     }
     gcf_result r;
-    if (J.mode >= 2) {   // CFindCtf1D results: m_fDfMin = m_fDfMax = 1D defocus
+    if (J.mode == 2 || J.mode == 3) {   // CFindCtf1D results: m_fDfMin = m_fDfMax = 1D defocus
         r.df_min = J.df_1d;
         r.df_max = J.df_1d;
         r.azimuth = 0.0f;
@@ -911,11 +957,225 @@ __global__ void k_results(const SearchJob* __restrict__ jobs, int njobs, const i
     r.ext_phase = J.ext_phase;
     r.score = J.cc_max;
     r.ctf_res = J.ctf_res;
-    r.df_1d = J.mode == 0 ? J.df_1d : 0.0f;
-    r.phase_1d = J.mode == 0 ? J.phase_1d : 0.0f;
-    r.score_1d = J.mode == 0 ? J.score_1d : 0.0f;
+    r.df_1d = (J.mode == 0 || J.mode == 4) ? J.df_1d : 0.0f;
+    r.phase_1d = (J.mode == 0 || J.mode == 4) ? J.phase_1d : 0.0f;
+    r.score_1d = (J.mode == 0 || J.mode == 4) ? J.score_1d : 0.0f;
     r.lowpassed = lowpassed ? lowpassed[J.mic] : 0;
     out[j] = r;
+}
+
+// ---------------------------------------------------------------------------
+// Search on the contraction's table (mode 4).  The table P[z][(j, t)] holds,
+// for micrograph j, angle bin t and defocus row z, the correlation numerator
+// of the model with defocus z over that angle bin; Dz[z][j] the normaliser
+// sum C^2 over the whole band at defocus z.  A candidate (mean, ratio,
+// angle) then costs nth interpolated reads instead of a pass over the band:
+//   num = sum_t P[mean (1 + ratio cos 2(theta_t - angle))][t]
+//   den = (1/nth) sum_t Dz[same row],     CC = num / sqrt(den * sum S^2).
+// One CTA per job runs, on this evaluator, the reference's own control flow:
+// a 1D scan over the defocus rows of CFindCtf1D's range (FindCTF/
+// CFindCtf1D.cpp:73-90) -- or, with a learned prior, a window around it --
+// then CFindDefocus2D::mIterate (FindCTF/CFindDefocus2D.cpp:153-183) through
+// the same prepare_step / finish_step state machine as the FP32 search.  Its
+// best candidates go to the FP32 re-score (STEP_RESCORE) and local
+// refinement (STEP_LOCAL) of k_eval2d on the job's own band.
+constexpr int kTabThreads = 256;
+constexpr int kTabMaxTheta = 128;
+
+struct TabCtx {
+    const float* P;    // column 0 of this job's angle bins
+    long long ldp;
+    const float* D;    // this job's normaliser row Dz[j][.]
+    int lo, hi;        // computed rows [lo, hi)
+    int nth;
+    float z0, dz;
+    double ss;
+};
+
+__device__ __forceinline__ float table_cc(const TabCtx& T, const float* c2, const float* s2, float mean,
+                                          float ratio, float angle_deg)
+{
+    const float a = angle_deg * kD2R2D;
+    const float ca = cosf(2.0f * a), sa = sinf(2.0f * a);
+    const float sig = mean * ratio;
+    const float inv_dz = 1.0f / T.dz;
+    const float umax = (float)(T.hi - 1) - 1e-3f;
+    float num = 0.0f, den = 0.0f;
+    for (int t = 0; t < T.nth; ++t) {
+        const float z = fmaf(sig, fmaf(c2[t], ca, s2[t] * sa), mean);
+        float u = (z - T.z0) * inv_dz;
+        u = fminf(fmaxf(u, (float)T.lo), umax);
+        const int i0 = (int)u;
+        const float f = u - (float)i0;
+        const float p0 = __ldg(T.P + (size_t)i0 * T.ldp + t), p1 = __ldg(T.P + (size_t)(i0 + 1) * T.ldp + t);
+        const float d0 = __ldg(T.D + i0), d1 = __ldg(T.D + i0 + 1);
+        num += fmaf(f, p1 - p0, p0);
+        den += fmaf(f, d1 - d0, d0);
+    }
+    const double d = (double)den / T.nth * T.ss;
+    return d > 0.0 ? (float)((double)num / sqrt(d)) : 0.0f;
+}
+
+__global__ void __launch_bounds__(kTabThreads)
+k_table_search(TableArgs A)
+{
+    __shared__ SearchJob sJ;
+    __shared__ ArgMax shm[32];
+    __shared__ float s_c2[kTabMaxTheta], s_s2[kTabMaxTheta];
+    __shared__ float2 s_cval[kMaxCand];
+    __shared__ float s_cc0;
+    __shared__ int s_n;
+    __shared__ float s_top[45];
+    const int j = blockIdx.x, tid = threadIdx.x;
+    if (tid == 0) sJ = A.jobs[j];
+    const int2 rr = A.rows[j];
+    TabCtx T;
+    T.P = A.P + (size_t)j * A.g.nth;
+    T.ldp = A.ldp;
+    T.D = A.Dz + (size_t)j * A.ldd;
+    T.lo = max(rr.x, 0);
+    T.hi = min(rr.y, A.g.nz);
+    T.nth = min(A.g.nth, kTabMaxTheta);
+    T.z0 = A.g.z0;
+    T.dz = A.g.dz;
+    T.ss = A.ss[j];
+    for (int t = tid; t < T.nth; t += blockDim.x) {
+        const float th = (-90.0f + ((float)t + 0.5f) * 180.0f / (float)T.nth) * kD2R2D;
+        s_c2[t] = cosf(2.0f * th);
+        s_s2[t] = sinf(2.0f * th);
+    }
+    __syncthreads();
+    if (sJ.mode != 4 || T.hi - T.lo < 2) {
+        if (tid == 0 && sJ.mode == 4) {   // nothing computed for this job: no search
+            sJ.step = STEP_DONE;
+            sJ.ncand = 0;
+            A.jobs[j] = sJ;
+        }
+        return;
+    }
+    const float4 pr = A.prior ? A.prior[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool learned = pr.x > 0.0f;
+    const float px2 = sJ.o.px * sJ.o.px;
+    float mu;
+    if (!learned) {
+        // 1D: the rows of CFindCtf1D's defocus range, angle bins summed
+        const int r0 = max(T.lo, (int)ceilf((3000.0f * px2 - T.z0) / T.dz));
+        const int r1 = min(T.hi - 1, (int)floorf((30000.0f * px2 - T.z0) / T.dz));
+        ArgMax m{(float)-1e20, -1};
+        for (int i = r0 + tid; i <= r1; i += blockDim.x) {
+            const float* row = T.P + (size_t)i * T.ldp;
+            float num = 0.0f;
+            for (int t = 0; t < T.nth; ++t) num += __ldg(row + t);
+            const double d = (double)__ldg(T.D + i) * T.ss;
+            const float v = d > 0.0 ? (float)((double)num / sqrt(d)) : 0.0f;
+            if (v > m.v) m = ArgMax{v, i};
+        }
+        m = block_argmax(m, shm);
+        mu = T.z0 + (float)(m.i >= 0 ? m.i : r0) * T.dz;
+        if (tid == 0) {
+            sJ.df_1d = mu;
+            sJ.phase_1d = sJ.ext_phase_in;
+            sJ.score_1d = m.v;
+            sJ.n_table += max(r1 - r0 + 1, 0);
+            // CFindCtf2D::Do2D ranges (FindCTF/CFindDefocus2D.cpp:110-124)
+            sJ.df_mean = mu;
+            sJ.ast_ratio = 0.0f;
+            sJ.ast_angle = 0.0f;
+            sJ.df_range[0] = mu * 0.9f;
+            sJ.df_range[1] = mu * 1.1f;
+            sJ.ast_range[0] = 0.0f;
+            sJ.ast_range[1] = 0.06f;
+            sJ.ang_range[0] = -90.0f;
+            sJ.ang_range[1] = 90.0f;
+        }
+    } else if (tid == 0) {
+        // learned prior: a window of +-5 search steps around the prediction
+        // (steps of the full search: mean defocus 0.2 mu / 31, ratio 0.06 / 51,
+        // angle 180 / 51 degrees), scaled by pr.w
+        mu = pr.x;
+        const float w = pr.w > 0.0f ? pr.w : 1.0f;
+        const float hdf = 5.0f * w * 0.2f * mu / 31.0f;
+        const float hast = 5.0f * w * 0.06f / 51.0f;
+        const float hang = 5.0f * w * 180.0f / 51.0f;
+        sJ.df_1d = mu;
+        sJ.phase_1d = sJ.ext_phase_in;
+        sJ.score_1d = 0.0f;
+        sJ.df_mean = mu;
+        sJ.ast_ratio = fminf(fmaxf(pr.y, 0.0f), 0.06f);
+        sJ.ast_angle = pr.z;
+        sJ.df_range[0] = mu - hdf;
+        sJ.df_range[1] = mu + hdf;
+        sJ.ast_range[0] = fmaxf(sJ.ast_ratio - hast, 0.0f);
+        sJ.ast_range[1] = fminf(sJ.ast_ratio + hast, 0.06f);
+        sJ.ang_range[0] = sJ.ast_angle - hang;
+        sJ.ang_range[1] = sJ.ast_angle + hang;
+    }
+    if (tid == 0) {
+        sJ.phase_range[0] = sJ.ext_phase_in;
+        sJ.phase_range[1] = 0.0f;   // no extra-phase search on the table
+        sJ.ext_phase = sJ.ext_phase_in;
+        sJ.step = STEP_CC0;
+    }
+    __syncthreads();
+    // CFindDefocus2D::mIterate on the table
+    for (int guard = 0; guard < 256; ++guard) {
+        if (tid == 0) s_n = advance(sJ, s_cval);
+        __syncthreads();
+        const int n = s_n;
+        if (sJ.step == STEP_DONE || n <= 0) break;
+        ArgMax m{(float)-1e20, -1};
+        for (int c = tid; c < n; c += blockDim.x) {
+            const Cand cd = cand_of(sJ, c, s_cval);
+            const float v = table_cc(T, s_c2, s_s2, cd.dfmean, cd.ast, cd.ang);
+            if (c == 0) s_cc0 = v;
+            if (v > m.v) m = ArgMax{v, c};
+        }
+        m = block_argmax(m, shm);   // synchronises: s_cc0 is visible
+        if (tid == 0) {
+            sJ.n_table += n;
+            finish_step(sJ, m.i >= 0 ? m.v : (float)-1e20, m.i, s_cc0, s_cval);
+        }
+        __syncthreads();
+    }
+    // the table's best candidates: a 5 x 3 x 3 neighbourhood of its optimum
+    // (half a final mean-defocus step, 0.001 in ratio, 2 degrees), the top
+    // kRescore go to the FP32 re-score
+    const float hmu = 0.5f * fmaxf(20.0f, 0.105f * sJ.df_mean / 31.0f);
+    if (tid < 45) {
+        const int a = tid % 5 - 2, b = (tid / 5) % 3 - 1, d = tid / 15 - 1;
+        s_top[tid] = table_cc(T, s_c2, s_s2, sJ.df_mean + (float)a * hmu,
+                              fmaxf(sJ.ast_ratio + 0.001f * (float)b, 0.0f), sJ.ast_angle + 2.0f * (float)d);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        sJ.n_table += 45;
+        unsigned long long used = 0ull;
+        for (int r = 0; r < kRescore; ++r) {
+            int bi = 22;   // the optimum itself
+            float bv = (float)-1e30;
+            for (int q = 0; q < 45; ++q)
+                if (!((used >> q) & 1ull) && s_top[q] > bv) {
+                    bv = s_top[q];
+                    bi = q;
+                }
+            used |= 1ull << bi;
+            const int a = bi % 5 - 2, b = (bi / 5) % 3 - 1, d = bi / 15 - 1;
+            sJ.rs_df[r] = sJ.df_mean + (float)a * hmu;
+            sJ.rs_ast[r] = fmaxf(sJ.ast_ratio + 0.001f * (float)b, 0.0f);
+            sJ.rs_ang[r] = sJ.ast_angle + 2.0f * (float)d;
+        }
+        sJ.loc_ddf = hmu;
+        sJ.loc_dast = 0.001f;
+        sJ.loc_dang = 1.0f;
+        sJ.cc_max = (float)-1e20;
+        sJ.iter = 0;
+        sJ.step = STEP_RESCORE;
+        s_n = advance(sJ, s_cval);
+        sJ.ncand = s_n;
+        A.jobs[j] = sJ;
+    }
+    __syncthreads();
+    write_candidates(sJ, s_n, A.cand + (size_t)j * kMaxCand, A.cval + (size_t)j * kMaxCand);
 }
 
 }  // namespace
@@ -940,6 +1200,12 @@ void launch_search1d(SearchJob* jobs, int njobs, const float* radial, int cx, fl
     if (njobs <= 0) return;
     size_t sm = sizeof(Bins1D);   // 16.4 KB, below the default dynamic limit
     k_search1d<<<njobs, 256, sm, st>>>(jobs, radial, cx, cand, cval);
+}
+
+void launch_table_search(const TableArgs& a, cudaStream_t st)
+{
+    if (a.njobs <= 0) return;
+    k_table_search<<<a.njobs, kTabThreads, 0, st>>>(a);
 }
 
 void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, int cy,

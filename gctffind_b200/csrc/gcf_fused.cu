@@ -837,18 +837,31 @@ unsigned char* g_na_base[kNaMaxDevices] = {};
 int g_na_clusters[kNaMaxDevices] = {};
 int g_na_shape[kNaMaxDevices] = {};
 
+// Writes one call's descriptors into the scratch.  They travel as a kernel
+// parameter (by value), so no host buffer has to outlive the call.
+__global__ void k_na_meta(NaMeta m, NaMeta* dst)
+{
+    const int n = (int)(sizeof(NaMeta) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(&m);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+}
+
 // Once per device, with that device current: find the scratch address and
-// fill the constant taper / twiddle tables inside it.
+// fill the constant taper / twiddle tables inside it.  The address is looked
+// up on every call (cheap) and compared with the cached one, so a context
+// that was torn down and re-created (cudaDeviceReset) is set up again.
 gcf_status na_setup(int dev, unsigned char** base, int* clusters)
 {
     std::lock_guard<std::mutex> lk(g_na_mutex);
-    if (g_na_base[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GCF_ERR_CUDA;
+    if (g_na_base[dev] == static_cast<unsigned char*>(p)) {
         *base = g_na_base[dev];
         *clusters = g_na_clusters[dev];
         return GCF_OK;
     }
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GCF_ERR_CUDA;
+    g_na_base[dev] = nullptr;
     std::vector<float> taper((size_t)FT * FT);
     const double c = FT * 0.5, s = FT;
     for (int y = 0; y < FT; ++y)
@@ -871,6 +884,9 @@ gcf_status na_setup(int dev, unsigned char** base, int* clusters)
             cudaSuccess ||
         cudaMemcpy(b + kNaTwOff, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
         return GCF_ERR_CUDA;
+    // the copies come from pageable memory and may return before their DMA
+    // lands; the caller's stream may be non-blocking: wait for them here
+    if (cudaDeviceSynchronize() != cudaSuccess) return GCF_ERR_CUDA;
     int n = 0, shape = 0;
     if (fused_max_clusters(&n, &shape) != cudaSuccess || n <= 0) return GCF_ERR_CUDA;
     g_na_base[dev] = b;
@@ -930,8 +946,8 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
     // nothing in the scratch has to start at zero; the descriptors below are
     // rewritten on every call.
     NaMeta* dmeta = reinterpret_cast<NaMeta*>(base + kNaMetaOff);
-    if (cudaMemcpyAsync(dmeta, &meta, sizeof(meta), cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return GCF_ERR_CUDA;
+    k_na_meta<<<1, 128, 0, st>>>(meta, dmeta);
+    if (cudaGetLastError() != cudaSuccess) return GCF_ERR_CUDA;
     int ncl = clusters < nitems ? clusters : nitems;
     cudaError_t e = launch_fused(&dmeta->desc, dmeta->bsum_ptr, (ntx + 1) * (nty + 1), dmeta->items,
                                  nitems, dmeta->first, dmeta->inv, 0, 1,
@@ -940,6 +956,5 @@ extern "C" gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, 
                                  reinterpret_cast<float*>(base), dev_raw_out, &dmeta->next_item, ncl,
                                  g_na_shape[dev], st, nullptr, nullptr);
     if (e != cudaSuccess) return GCF_ERR_CUDA;
-    // a copy from pageable memory has consumed `meta` when cudaMemcpyAsync returns
     return GCF_OK;
 }

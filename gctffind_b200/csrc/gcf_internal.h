@@ -12,6 +12,7 @@
 //   jobs       : one SearchJob per micrograph being searched
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -34,8 +35,15 @@ enum StepKind : int {
     STEP_ASTANG = 3,
     STEP_DFMEAN = 4,
     STEP_PHASE = 5,
-    STEP_DONE = 6
+    STEP_DONE = 6,
+    // finish of the BF16 contraction search (mode 4): the best of the
+    // table's top candidates re-scored in FP32, then local 3 x 3 x 3 grids
+    STEP_RESCORE = 7,
+    STEP_LOCAL = 8
 };
+
+constexpr int kRescore = 4;      // table candidates re-scored in FP32
+constexpr int kLocalPasses = 4;  // local 3 x 3 x 3 passes after the re-score
 
 // Optics in pixel units (CCTFTheory::Setup, FindCTF/CCTFTheory.cpp:69-86).
 struct PixOptics {
@@ -51,7 +59,8 @@ struct SearchJob {
     // inputs
     int mic;            // spectrum slot
     int band;           // band-table slot
-    int mode;           // 0 = Do2D (after the 1D search), 1 = Refine, 2 = Do1D, 3 = Refine1D
+    int mode;           // 0 = Do2D (after the 1D search), 1 = Refine, 2 = Do1D, 3 = Refine1D,
+                        // 4 = contraction search (table search, then the FP32 finish)
     int pad0;
     PixOptics o;
     float phase_range_in;   // CFindCtfBase::m_fPhaseRange (Do2D)
@@ -84,6 +93,12 @@ struct SearchJob {
     // work done: 2D candidates evaluated (each over the whole band), 1D grid
     // points evaluated, and 1D (grid point, bin) pairs
     int n_cand2d, n_cand1d, n_pairs1d;
+    // contraction search (mode 4): candidates scored on the BF16 table, the
+    // table's best candidates for the FP32 re-score, the local steps
+    int n_table;
+    float rs_df[kRescore], rs_ast[kRescore], rs_ang[kRescore];
+    float loc_ddf, loc_dast, loc_dang;
+    int pad3;
 };
 
 // Per-band device pointers (structure of arrays).
@@ -198,6 +213,129 @@ void launch_shell_select(SearchJob* jobs, int njobs, const float* cc, int cx, in
 // counts (nullable): per job n_cand2d, n_cand1d, n_pairs1d
 void launch_results(const SearchJob* jobs, int njobs, const int* lowpassed, gcf_result* out, int* counts,
                     cudaStream_t st);
+
+// gcf_umma.cu: BF16 x BF16 -> FP32 tensor-core product D = A * B^T (A: M x K,
+// B: N x K, both K-major), 128 x bn tiles (bn = 32, 64, 128 or 256),
+// `stages`-deep TMA ring (see the file for the supported pairs).
+struct GemmArgs {
+    int M = 0, N = 0, K = 0;
+    float* D = nullptr;            // FP32 row-major output (nullable), pitch ldd
+    long long ldd = 0;
+    __nv_bfloat16* Db = nullptr;   // BF16 row-major copy (nullable), pitch ldd
+    __nv_bfloat16* Dt = nullptr;   // BF16 transposed copy Dt[n][m] (nullable), pitch ldt
+    long long ldt = 0;
+    const float* bias = nullptr;   // added per column n before the ReLU (nullable)
+    int relu = 0;
+    int accumulate = 0;            // D += A B^T (FP32 output only)
+    int vec4 = 0;                  // set by the launcher
+    const int2* tiles = nullptr;   // (m0, n0) of each CTA's tile; null: the whole grid
+    const int* ntiles = nullptr;   // device count of `tiles` (CTAs beyond it exit at once)
+    int* err = nullptr;            // device flag: 0 ok, else the wait that ran out
+};
+int umma_tile_n_supported(int bn);
+cudaError_t launch_umma_gemm(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B, long long ldb,
+                             GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st);
+
+// gcf_contract.cu: the BF16 candidate contraction.
+// Common polar grid of a batch: ns bins uniform in s^2 (1/A^2) over the
+// band [s2_lo, s2_lo + ns * ds2), nth angle bins over [-90, 90) degrees, and
+// nz defocus rows z_i = z0 + i * dz (Angstrom).
+struct PolarGrid {
+    int ns, nth, nz, pad;
+    float s2_lo, ds2;
+    float z0, dz;
+    float wl, cs;          // wavelength and Cs, Angstrom
+    float amp_phase;       // amplitude-contrast phase + extra phase, radian
+    float pad2;
+};
+// Model rows A[i][k] = |sin(chi(z_i, s2_k))| - 1/2 and A2 = A^2, BF16,
+// nz x ns (row pitch ns).
+void launch_polar_model(const PolarGrid& g, __nv_bfloat16* A, __nv_bfloat16* A2, cudaStream_t st);
+// Per job j (spectrum slot mic[j], pixel size px[j]): the background-
+// removed half spectrum summed into (s^2, angle) cells, times the job's
+// envelope exp(-16 s^2 px^2), as BF16 rows B[j * nth + t][k]; the
+// envelope^2-weighted pixel count per s^2 bin E[j][k]; sum of S^2 over the
+// band's pixels ss[j].
+cudaError_t launch_polar_bin(const float* ctf, int tile, const SearchJob* jobs, int njobs, const PolarGrid& g,
+                             __nv_bfloat16* B, __nv_bfloat16* E, double* ss, cudaStream_t st);
+// Rows [lo, hi) of the defocus grid each job's table search can touch
+// (prior: optional learned (mean, ratio, angle, window scale) per job).
+void launch_job_rows(const SearchJob* jobs, int njobs, const float4* prior, const PolarGrid& g, int2* rows,
+                     cudaStream_t st);
+// Row tiles of P = A B^T that the jobs need: job j needs rows rows[j] =
+// [lo, hi); a column block of bn columns (bn / nth jobs) gets the row tiles
+// covering the union of its jobs' rows.  tiles: (m0, n0), *ntiles their
+// count (capacity max_tiles).
+void launch_plan_tiles(const int2* rows, int njobs, int nth, int nz, int bn, int2* tiles, int* ntiles,
+                       int max_tiles, cudaStream_t st);
+
+// gcf_control.cu: the search on the contraction's table (one CTA per job).
+struct TableArgs {
+    SearchJob* jobs;
+    int njobs;
+    const float* P;          // [nz][ldp]: job j's angle bins at columns j * nth ..
+    long long ldp;
+    const float* Dz;         // [njobs][ldd]: job j's normaliser sum C^2 at each row
+    long long ldd;
+    const double* ss;        // [njobs]
+    PolarGrid g;
+    const int2* rows;        // [njobs] rows computed for each job
+    const float4* prior;     // [njobs] (mean A, ratio, angle deg, window scale) or null
+    float4* cand;
+    float2* cval;
+};
+void launch_table_search(const TableArgs& a, cudaStream_t st);
+
+// gcf_nn.cu: the learned initialiser's kernels (see the file for the network).
+constexpr int kNnProfile = 256;            // x1 bins
+constexpr int kNnMap = 256;                // x2 is kNnMap x kNnMap
+constexpr int kNnOut = 3;                  // (mean, ax, ay)
+constexpr int kNnPredPitch = 16;           // FP32 prediction rows
+// spectra in slots 0 .. n-1 of ctf; px[j * px_stride]: pixel size of slot j
+cudaError_t launch_nn_input(const float* ctf, int tile, const float* px, int px_stride, int n, __nv_bfloat16* x1,
+                            __nv_bfloat16* x2, cudaStream_t st);
+// params: 8 floats per sample; target: 3 floats per sample
+void launch_synth_params(unsigned long long seed, unsigned long long first, int n, float* params, float* target,
+                         cudaStream_t st);
+// base: optics with the wavelength and Cs in Angstrom
+void launch_synth_raw(unsigned long long seed, unsigned long long first, const float* params, int n, int tile,
+                      const PixOptics& base, float* raw, cudaStream_t st);
+void launch_im2col_p4(const __nv_bfloat16* x, int B, __nv_bfloat16* cols, cudaStream_t st);
+void launch_im2col_3s2(const __nv_bfloat16* x, int B, int H, int W, int C, __nv_bfloat16* cols, cudaStream_t st);
+void launch_col2im_3s2_relu(const float* dcols, const __nv_bfloat16* y, int B, int H, int W, int C,
+                            __nv_bfloat16* dz, cudaStream_t st);
+void launch_relu_bwd(const float* dy, long long ldy, const __nv_bfloat16* y, long long ldyy, int rows, int n,
+                     __nv_bfloat16* dz, long long ldz, cudaStream_t st);
+void launch_concat(const __nv_bfloat16* x1, const __nv_bfloat16* y4, int B, __nv_bfloat16* h0, cudaStream_t st);
+void launch_wgrad(const __nv_bfloat16* dz, long long ldz, const __nv_bfloat16* x, long long ldx, int rows, int nout,
+                  int nin, float* dw, float* db, cudaStream_t st);
+void launch_mse(const float* pred, long long ldp, const float* target, int B, float* loss, __nv_bfloat16* dpred,
+                cudaStream_t st);
+void launch_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
+                 float c1, float c2, int nout, int nin, __nv_bfloat16* wb, __nv_bfloat16* wt, long long ldt,
+                 cudaStream_t st);
+void launch_copy_weights(const float* w, int nout, int nin, __nv_bfloat16* wb, __nv_bfloat16* wt, long long ldt,
+                         cudaStream_t st);
+void launch_prior(const float* pred, long long ldp, int n, float4* prior, cudaStream_t st);
+
+// gcf_learned.cpp: the network's state and passes (device buffers, one stream).
+struct NnNet;
+NnNet* nn_create();
+void nn_destroy(NnNet* n);
+size_t nn_param_count();
+// He-normal weights from the seed, zero biases
+cudaError_t nn_init_random(NnNet* n, unsigned long long seed, cudaStream_t st);
+cudaError_t nn_set_params(NnNet* n, const float* host, cudaStream_t st);
+cudaError_t nn_get_params(NnNet* n, float* host, cudaStream_t st);
+cudaError_t nn_get_grads(NnNet* n, float* host, cudaStream_t st);
+// x1 [B][256], x2 [B][256][256] BF16 (device) -> pred [B][kNnPredPitch] FP32 (device, owned by the net)
+cudaError_t nn_forward(NnNet* n, const __nv_bfloat16* x1, const __nv_bfloat16* x2, int B, cudaStream_t st);
+const float* nn_pred(NnNet* n);
+// after nn_forward: gradients of the mean squared error against target
+// [B][3] (device) into the net's FP32 gradient buffer, loss (device) += mean
+cudaError_t nn_backward(NnNet* n, const float* target, int B, float* loss, cudaStream_t st);
+cudaError_t nn_adam(NnNet* n, float lr, cudaStream_t st);
+int* nn_err_flag(NnNet* n);
 
 // gcf_background.cu: GBackground1D
 constexpr int kMaxBackgroundBins = 12288;   // one block's shared memory (48 KB)

@@ -152,3 +152,41 @@ def tilt_series_specs(n_tilts: int = 41, step_deg: float = 3.0, size: int = 4096
 def tilt_angles(n_tilts: int = 41, step_deg: float = 3.0) -> list[float]:
     half = (n_tilts - 1) / 2.0
     return [(i - half) * step_deg for i in range(n_tilts)]
+
+
+UNEVEN_SIZES = ((4096, 4096), (5760, 4092), (3838, 3710))
+
+
+def uneven_batch_specs(n: int = 256, seed: int = 2, sizes=UNEVEN_SIZES) -> list[MicrographSpec]:
+    """A seeded batch of independent micrographs of uneven size: each a
+    uniform pick of `sizes`, pixel size U(0.8, 1.5) A, mean defocus
+    U(5000, 40000) A, astigmatism (df_max - df_min) U(0, 1000) A at an angle
+    U(0, 180) degrees (reported in (-90, 90]), dose U(0.5, 2) e/A^2."""
+    g = torch.Generator().manual_seed(int(seed))
+
+    def u(lo, hi):
+        return lo + (hi - lo) * float(torch.rand((), generator=g, dtype=torch.float64))
+
+    specs = []
+    for k in range(n):
+        w, h = sizes[int(torch.randint(0, len(sizes), (), generator=g))]
+        px = u(0.8, 1.5)
+        df = u(5000.0, 40000.0)
+        ast = u(0.0, 1000.0)
+        ang = u(0.0, 180.0)
+        specs.append(MicrographSpec(width=w, height=h, pixel_size=px, df_min=df - 0.5 * ast,
+                                    df_max=df + 0.5 * ast, azimuth_deg=ang if ang <= 90.0 else ang - 180.0,
+                                    dose=u(0.5, 2.0), seed=int(seed) * 100003 + k))
+    return specs
+
+
+def inside_reference_envelope(spec: MicrographSpec) -> bool:
+    """Whether the reference's full search can reach this micrograph's
+    parameters: mean defocus inside CFindCtf1D's range [3000, 30000] px^2 A
+    (FindCTF/CFindCtf1D.cpp:78-79; px after rescaling to >= 1.2 A) with 10 %
+    to spare, and astigmatism ratio (df_max - df_min) / (df_max + df_min) at
+    most the full search's 0.06 (FindCTF/CFindDefocus2D.cpp:117-118)."""
+    px_n = max(spec.pixel_size, 1.2)
+    mean = 0.5 * (spec.df_min + spec.df_max)
+    ratio = (spec.df_max - spec.df_min) / (spec.df_max + spec.df_min)
+    return 3300.0 * px_n * px_n <= mean <= 27000.0 * px_n * px_n and ratio <= 0.06

@@ -237,6 +237,76 @@ typedef struct {
 gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int images_are_device,
                          const gcf_optics* optics, gcf_result* results);
 
+/* Search method of a batch. */
+typedef enum {
+    GCF_SEARCH_PLAIN = 0,    /* the reference's FP32 search per micrograph
+                                (CFindCtf1D::Do1D + CFindCtf2D::Do2D)       */
+    GCF_SEARCH_BF16 = 1,     /* all candidates x all spectra as one BF16
+                                tensor-core contraction, the table searched
+                                with the reference's control flow, the best
+                                candidates re-scored in FP32 (FP64 sums) and
+                                refined locally                             */
+    GCF_SEARCH_LEARNED = 2   /* as BF16, the search window set by the learned
+                                initialiser, full search as the fallback    */
+} gcf_search_mode;
+
+/* gcf_run_batch with a search method.  GCF_SEARCH_PLAIN is gcf_run_batch.
+ * The contraction has no extra-phase dimension: with ext_phase_range > 0
+ * every mode runs the plain search.  Replaces the per-candidate
+ * GCalcCTF2D + GCC2D loop of CFindDefocus2D (FindCTF/CFindDefocus2D.cpp:
+ * 153-380) and the 1D brute force of CFindDefocus1D
+ * (FindCTF/CFindDefocus1D.cpp:76-119) in the contraction modes. */
+gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int images_are_device,
+                              const gcf_optics* optics, int mode, gcf_result* results);
+
+/* ---------------------------------------------------------------------- */
+/* Learned initialiser.  No counterpart in the reference: it replaces the    */
+/* coarse searches of CFindCtf1D::mFindDefocus (FindCTF/CFindCtf1D.cpp:73-90)*/
+/* and CFindDefocus2D::mFindAstig (FindCTF/CFindDefocus2D.cpp:185-222) with  */
+/* a window of +-5 search steps around a prediction.                        */
+/* ---------------------------------------------------------------------- */
+/* A small network (4 convolutions over the 256 x 256 polar half spectrum,
+ * a 3-layer MLP over the 256-bin rotational profile and those features)
+ * predicts mean defocus, astigmatism and angle; its BF16 forward and
+ * backward passes and Adam run in this library's kernels.  Parameters are
+ * FP32, gcf_nn_param_count() of them. */
+size_t gcf_nn_param_count(void);
+gcf_status gcf_nn_init(gcf_ctx* ctx, unsigned long long seed);
+gcf_status gcf_nn_set_params(gcf_ctx* ctx, const float* params, size_t n);
+gcf_status gcf_nn_get_params(gcf_ctx* ctx, float* params, size_t n);
+/* Weights file: 8-byte tag "GCFNN001", the count (uint64), FP32 params. */
+gcf_status gcf_nn_save(gcf_ctx* ctx, const char* path);
+gcf_status gcf_nn_load(gcf_ctx* ctx, const char* path);
+/* Refined CC below which a learned search falls back to the full search
+ * (default 0.1); a result at the edge of its window always falls back. */
+gcf_status gcf_set_learned_threshold(gcf_ctx* ctx, float tau);
+/* `steps` Adam steps of `batch` synthetic pairs each, generated on the GPU
+ * from the seed (samples first, first + 1, ...): the expected averaged
+ * spectrum of the micrograph model (white object x CTF x B-factor
+ * envelope, smooth background, shot noise, tile averaging) for parameters
+ * drawn like the uneven batch, background-removed and lowpassed by this
+ * library's own post-processing.  Starts from random weights if none are
+ * set.  losses (nullable, host): the mean squared error of each step. */
+gcf_status gcf_nn_train(gcf_ctx* ctx, const gcf_optics* optics, int steps, int batch, unsigned long long seed,
+                        unsigned long long first, float lr, float* losses);
+/* The network inputs of n <= 512 synthetic samples, as host floats:
+ * x1 n x 256, x2 n x 256 x 256, target n x 3, params n x 8 (mean defocus,
+ * astigmatism, angle radian, pixel size, dose, tiles, raw pixel size,
+ * scale); each output nullable. */
+gcf_status gcf_nn_synth_inputs(gcf_ctx* ctx, const gcf_optics* optics, unsigned long long seed,
+                               unsigned long long first, int n, float* x1, float* x2, float* target,
+                               float* params);
+/* One forward and backward pass on given inputs (rounded to BF16): loss,
+ * the FP32 gradient of every parameter (gcf_nn_param_count floats) and the
+ * predictions (n x 3); outputs nullable.  For gradient checks. */
+gcf_status gcf_nn_forward_backward(gcf_ctx* ctx, const float* x1, const float* x2, const float* target, int n,
+                                   float* loss, float* grads, float* pred);
+/* Searches of n synthetic spectra (samples first .. first + n - 1 of the
+ * seed) with the given method: results and (nullable) the samples'
+ * parameters (n x 8 as above).  gcf_get_fast_counts then holds the work. */
+gcf_status gcf_nn_eval_synthetic(gcf_ctx* ctx, const gcf_optics* optics, unsigned long long seed,
+                                 unsigned long long first, int n, int mode, gcf_result* results, float* params);
+
 /* ---------------------------------------------------------------------- */
 /* MRC input/output (Mrc::CLoadMrc / Mrc::CSaveMrc subset,                  */
 /* Include/Mrcfile/CMrcFileInc.h:52-120, MrcUtil/CLoadImages.cpp:108-181)   */
@@ -262,6 +332,22 @@ gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, in
  * nm.  tilts and names may be NULL (0 and "" then). */
 gcf_status gcf_write_ctf_file(const char* path, const gcf_result* results, const float* tilts,
                               const char* const* names, int n, int is_tomo);
+
+/* ---------------------------------------------------------------------- */
+/* Tensor-core building block.  No counterpart in the reference (its        */
+/* candidate loop is one GCalcCTF2D + GCC2D launch pair per candidate,      */
+/* FindCTF/CFindDefocus2D.cpp:363-380); this is the dense product the       */
+/* batched candidate contraction is built on.                               */
+/* ---------------------------------------------------------------------- */
+/* d[m][n] = sum_k a[m][k] * b[n][k] on the tcgen05 tensor cores: a (m x k,
+ * row pitch lda) and b (n x k, row pitch ldb) are BF16 device arrays with
+ * 16-byte aligned bases and pitches, d (m x n, pitch ldd) FP32, FP32
+ * accumulation.  tile_n (32, 64, 128, 256) and stages pick the kernel's
+ * 128 x tile_n output tile and its load-pipeline depth (pairs: 256 x 2/3/4,
+ * 128 x 2/4/6, 64 x 2/4, 32 x 2/4).  Runs on `cuda_stream` of the current
+ * device and waits for it; GCF_ERR_TIMEOUT if a bounded device wait gave up. */
+gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b, long long ldb, int m, int n, int k,
+                         float* d, long long ldd, int tile_n, int stages, void* cuda_stream);
 
 /* ---------------------------------------------------------------------- */
 /* Allocation-free spectrum.  No counterpart in the reference.              */
@@ -290,6 +376,16 @@ gcf_status gcf_avg_spectrum_noalloc(const float* dev_img, int width, int height,
  * [3] background + lowpass + radial, [4] 1D search, [5] 2D search,
  * [6] total. */
 gcf_status gcf_get_stage_times(gcf_ctx* ctx, float times_ms[7]);
+/* Contraction work of the last gcf_run_batch_mode call: [0] candidates
+ * scored on the BF16 table, [1] tensor-core multiply-adds of the
+ * contraction, [2] candidates re-scored in FP32 on the micrographs' own
+ * bands, [3] learned searches that fell back to the full search. */
+gcf_status gcf_get_fast_counts(gcf_ctx* ctx, long long counts[4]);
+/* Device time (ms, CUDA events) of the contraction stages of the last
+ * gcf_run_batch_mode call: [0] polar binning of the spectra, [1] the
+ * tensor-core products (table and normaliser), [2] the table search,
+ * [3] FP32 re-score and local passes. */
+gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[4]);
 /* Number of kernels this library launched in the last batched call. */
 gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);
 /* Search work counted on the device since the last gcf_run_series /

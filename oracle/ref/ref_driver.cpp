@@ -16,7 +16,13 @@
 #include <unistd.h>
 
 #include "CMainInc.h"
+// CFindCtf2D keeps its CFindDefocus2D private; the driver reads that
+// object's GetCtfRes() (the spectral-CC resolution, FindCTF/CFindDefocus2D.cpp:
+// 65-68, 382-400), so the class is seen with its members public here.  The
+// reference sources themselves are compiled unchanged.
+#define private public
 #include "FindCTF/CFindCTFInc.h"
+#undef private
 #include "MrcUtil/CMrcUtilInc.h"
 
 #include "ref_state.h"
@@ -139,7 +145,7 @@ int gref_run_series(const float* const* images, int n, int width, int height,
 //   refine       : null for Do2D, else the four {centre, range} pairs of
 //                  CFindCtf2D::Refine (defocus mean, astig ratio, astig
 //                  angle, extra phase)
-//   result       : df_min, df_max, azimuth, ext_phase, score
+//   result       : df_min, df_max, azimuth, ext_phase, score, ctf_res (A)
 int gref_single(const float* image, int width, int height, float kv, float cs_mm,
                 float amp_contrast, float pixel_size, float ext_phase_deg, float ext_phase_range,
                 int tile, int log_spect, int gpu, const float* refine, int* new_dims,
@@ -210,6 +216,7 @@ int gref_single(const float* image, int width, int height, float kv, float cs_mm
     result[2] = find->m_fAstAng;
     result[3] = find->m_fExtPhase;
     result[4] = find->m_fScore;
+    result[5] = find->m_pFindDefocus2D ? find->m_pFindDefocus2D->GetCtfRes() : 0.0f;
     if (full) {
         float* f = find->GenFullSpectrum();
         memcpy(full, f, (size_t)tile * tile * sizeof(float));

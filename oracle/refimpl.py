@@ -16,7 +16,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libgcfref.so")
-REF_TREE = os.environ.get("GCF_REFERENCE_TREE", "/root/reference")
+# the GCtfFind source tree: $GCF_REFERENCE_TREE, else a "reference" folder
+# beside this repository
+REF_TREE = os.environ.get("GCF_REFERENCE_TREE",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 _lib = None
 _F = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -110,7 +113,7 @@ def single(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_
     raw = np.zeros((tile, cx), np.float32)
     ctf = np.zeros((tile, cx), np.float32)
     full = np.zeros((tile, tile), np.float32)
-    out = np.zeros(5, np.float32)
+    out = np.zeros(6, np.float32)
     rin = None
     if refine is not None:
         rarr = np.ascontiguousarray(refine, np.float32)
@@ -123,7 +126,7 @@ def single(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_
     nw, nh = dims[0], dims[1]
     return {"new_size": (nw, nh), "new_pixel_size": npx.value,
             "rescaled": resc[: nw * nh].reshape(nh, nw), "raw_half": raw, "ctf_half": ctf,
-            "full": full, "result": out}
+            "full": full, "result": out[:5], "ctf_res": float(out[5])}
 
 
 def single1d(image, pixel_size, kv=300.0, cs_mm=2.7, amp_contrast=0.07, ext_phase_deg=0.0,

@@ -1,0 +1,74 @@
+"""The learned initialiser on the GPU: its BF16 forward/backward kernels
+against the FP64 oracle (oracle/nn_oracle.py), training by the library's
+own kernels, and the learned window search against the plain search.
+
+Gradient check bar: the library stores activations and gradients in BF16
+(8 significant bits) between layers and multiplies BF16 operands with FP32
+accumulation; the oracle uses the same BF16-rounded weights in FP64 with
+unrounded activations.  So per layer the gradient must agree to a relative
+L2 error of 5e-2 with cosine similarity above 0.998, the loss to 2e-2
+relative and the predictions to 2e-2 of their spread.
+"""
+import numpy as np
+import pytest
+
+from oracle import nn_oracle as N
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gradients_match_oracle(gpu_lib):
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    ctx.nn_init(11)
+    op = G.make_optics()
+    x1, x2, t, p = ctx.nn_synth_inputs(op, seed=5, first=0, n=4)
+    assert np.all(np.isfinite(x1)) and np.all(np.isfinite(x2))
+    # inputs are standardised over their non-empty cells
+    assert abs(float(x1[x1 != 0].mean())) < 0.05 and 0.9 < float(x1[x1 != 0].std()) < 1.1
+    params = ctx.nn_params()
+    loss, grads, pred = ctx.nn_forward_backward(x1, x2, t)
+    ctx.close()
+    # the oracle sees the BF16-rounded inputs the library used
+    oloss, ograds, opred = N.forward_backward(params, N.bf16(x1), N.bf16(x2), t)
+    assert abs(loss - oloss) <= 2e-2 * abs(oloss), (loss, oloss)
+    assert np.abs(pred - opred).max() <= 2e-2 * (np.abs(opred).max() + 1e-3), (pred, opred)
+    for k, ((gw, gb), (ow, ob)) in enumerate(zip(N.split(grads), N.split(ograds))):
+        for a, b in ((gw, ow), (gb, ob)):
+            a = a.ravel().astype(np.float64)
+            b = b.ravel()
+            nb = np.linalg.norm(b)
+            if nb == 0:
+                assert np.linalg.norm(a) == 0
+                continue
+            rel = np.linalg.norm(a - b) / nb
+            cos = float(a @ b / (np.linalg.norm(a) * nb + 1e-300))
+            assert rel <= 5e-2 and cos >= 0.998, (k, rel, cos)
+
+
+def test_training_lowers_the_loss_and_weights_round_trip(gpu_lib, tmp_path):
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    op = G.make_optics()
+    ctx.nn_init(3)
+    losses = ctx.nn_train(op, steps=200, batch=64, seed=77, first=0, lr=1e-3)
+    assert np.all(np.isfinite(losses))
+    first, last = float(losses[:20].mean()), float(losses[-20:].mean())
+    assert last < 0.5 * first, (first, last)
+    path = str(tmp_path / "w.bin")
+    ctx.save_weights(path)
+    w = ctx.nn_params()
+    ctx2 = G.Context(0, 512, 0)
+    ctx2.load_weights(path)
+    assert np.array_equal(ctx2.nn_params(), w)
+    ctx.close()
+    ctx2.close()
+
+
+def test_learned_search_needs_weights(gpu_lib):
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    img = np.zeros((1024, 1024), np.float32)
+    with pytest.raises(G.GcfError):
+        ctx.run_batch([img], [1.35], G.make_optics(), mode=G.GCF_SEARCH_LEARNED)
+    ctx.close()
