@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=N_BATCH)
     ap.add_argument("--mode", default="auto", choices=["auto", "bf16", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true", help="launch every kernel from the host")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the tilt-series and 1.0 A/px single-micrograph figures")
     ap.add_argument("--shrink", type=int, default=1,
@@ -220,6 +221,7 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
     barrier(world)
     torch.cuda.synchronize()
     dev_ms, launches, stage, ftimes, fcounts = 0.0, 0, {}, {}, {}
+    graph_launches = 0
     res = None
     for _ in range(steps):
         res = ctx.run_batch(imgs, pxs, op, mode=mode)
@@ -228,6 +230,7 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
         for k, v in st.items():
             stage[k] = stage.get(k, 0.0) + v / steps
         launches += ctx.launch_count()
+        graph_launches += ctx.graph_info()["graph_launches"]
         if mode != 0:
             for k, v in ctx.fast_times().items():
                 ftimes[k] = ftimes.get(k, 0.0) + v / steps
@@ -236,7 +239,8 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
     barrier(world)
     return {"ms": max_over_ranks(dev_ms / steps, world), "results": res, "stage": stage,
             "launches": launches // steps, "fast_ms": ftimes, "fast_counts": fcounts,
-            "search_counts": ctx.search_counts()}
+            "search_counts": ctx.search_counts(), "graph_launches_per_step": graph_launches / steps,
+            "graph": ctx.graph_info()}
 
 
 def timed_single_file(ctx, imgs, pxs, op, steps, world):
@@ -441,6 +445,10 @@ def main():
     torch.cuda.set_device(local)
     ctx = G.Context(local, 512, 0)
     op = G.make_optics()
+    # the project's autotuner picks the tile-kernel shape and the contraction
+    # tile; repeated batch calls run as captured CUDA graphs
+    tuning = ctx.autotune()
+    ctx.set_graphs(not args.no_graphs)
     specs, imgs = make_batch(rank, args.batch, f"cuda:{local}", args.shrink)
     pxs = [s.pixel_size for s in specs]
     learned = args.mode == "learned" or (args.mode == "auto" and G.learned_available())
@@ -463,7 +471,8 @@ def main():
             for s in specs]
     del imgs
     torch.cuda.empty_cache()
-    ctx.run_batch(host, pxs, op, mode=fast_mode)
+    for _ in range(2):   # the second call captures the graph the timed calls replay
+        ctx.run_batch(host, pxs, op, mode=fast_mode)
     barrier(world)
     e2e_wall = 0.0
     for _ in range(args.steps):
@@ -508,6 +517,13 @@ def main():
                     "d2h_bytes_per_step": n * 40, "ms_per_step": round(e2e_ms, 3),
                     "timing": "host clock around gcf_run_batch_mode (pinned host images)"},
             "gpu_launches": fast["launches"],
+            "cuda_graphs": {"graph_launches_per_step": fast["graph_launches_per_step"],
+                            "graph_nodes": fast["graph"]["nodes"],
+                            "library_kernels_in_graph": fast["graph"]["kernels"],
+                            "note": "each timed step is one graph launch holding gpu_launches kernels of this "
+                                    "library (plus cuFFT's rescale and lowpass kernels) when graph_launches_per_step "
+                                    "is 1"},
+            "autotune": tuning,
             "roofline": tile_kernel_roofline(fast["stage"], dims, pk),
             "clocks": clocks}
     if not args.no_secondary:

@@ -42,7 +42,8 @@ EXPORTS = [
     "gcf_nn_param_count", "gcf_nn_init", "gcf_nn_set_params", "gcf_nn_get_params", "gcf_nn_save",
     "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs",
     "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
-    "gcf_write_ctf_file",
+    "gcf_write_ctf_file", "gcf_write_ctf_file_ex", "gcf_set_package_callback", "gcf_set_graphs",
+    "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load",
     "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
     "gcf_ctf_phase_shift", "gcf_ctf_defocus", "gcf_ctf_frequency", "gcf_ctf_nth_zero",
@@ -83,10 +84,26 @@ class CtfParam(C.Structure):
                 ("pixel_size", C.c_float)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("fused_shape", C.c_int), ("gemm_tile_n", C.c_int), ("gemm_stages", C.c_int),
+                ("fused_ms", C.c_float * 3), ("gemm_ms", C.c_float * 6)]
+
+    def as_dict(self):
+        return {"fused_shape": self.fused_shape, "gemm_tile_n": self.gemm_tile_n,
+                "gemm_stages": self.gemm_stages,
+                "fused_ms": dict(zip(["8", "816", "16"], [round(x, 4) for x in self.fused_ms])),
+                "gemm_ms": dict(zip(["256x2", "256x3", "256x4", "128x4", "128x6", "64x4"],
+                                    [round(x, 4) for x in self.gemm_ms]))}
+
+
 class Item(C.Structure):
     _fields_ = [("image", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
                 ("pixel_size", C.c_float)]
 
+
+# void (*)(void* user, int done, int image, const gcf_result* result)
+PACKAGE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.POINTER(Result))
+GCF_CTF_COLUMN_RES = 1
 
 _lib = None
 
@@ -155,6 +172,12 @@ def load_library(path: str = LIB_PATH):
     L.gcf_nn_forward_backward.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
     L.gcf_nn_eval_synthetic.argtypes = [vp, C.POINTER(Optics), ull, ull, i, i, C.POINTER(Result), vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
+    L.gcf_write_ctf_file_ex.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i, i]
+    L.gcf_set_package_callback.argtypes = [vp, PACKAGE_FN, vp]
+    L.gcf_set_graphs.argtypes = [vp, i]
+    L.gcf_mrc_load.argtypes = [vp, C.c_char_p, i, i, C.POINTER(vp)]
+    L.gcf_autotune.argtypes = [vp, i, C.POINTER(Tuning)]
+    L.gcf_get_graph_info.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_background1d.argtypes = [vp, vp, i, i, vp, C.POINTER(i)]
     L.gcf_remove_background1d.argtypes = [vp, vp, i, vp, i, i, i]
     L.gcf_remove_background2d.argtypes = [vp, vp, i, vp, i, i, i]
@@ -335,7 +358,23 @@ class Context:
 
     # -- batched paths -----------------------------------------------------------
     def run_series(self, images, optics: Optics, order=None, is_tomo: bool = True,
-                   want_full: bool = False):
+                   want_full: bool = False, on_package=None):
+        """CFindSeriesCtfs policy over equal-sized images (gcf_run_series);
+        on_package(done, image, result), if given, is called as each
+        package's result becomes final, in processing order."""
+        cb = None
+        if on_package is not None:
+            def _hook(user, done, image, r):
+                on_package(done, image, Result.from_buffer_copy(r.contents))
+            cb = PACKAGE_FN(_hook)
+            _check(self.L.gcf_set_package_callback(self._h, cb, None), self._h)
+        try:
+            return self._run_series(images, optics, order, is_tomo, want_full)
+        finally:
+            if cb is not None:
+                self.L.gcf_set_package_callback(self._h, PACKAGE_FN(), None)
+
+    def _run_series(self, images, optics, order, is_tomo, want_full):
         imgs = [_as_f32(a) for a in images]
         n = len(imgs)
         h, w = imgs[0].shape
@@ -371,6 +410,33 @@ class Context:
         res = (Result * n)()
         _check(self.L.gcf_run_batch_mode(self._h, items, n, dev, C.byref(optics), int(mode), res), self._h)
         return [res[i] for i in range(n)]
+
+    def mrc_load(self, path: str, z0: int = 0, n: int | None = None):
+        """Sections of an MRC file converted to float on the GPU
+        (gcf_mrc_load): device addresses, valid until the next load."""
+        if n is None:
+            n = mrc_info(path)["dims"][2] - z0
+        out = (C.c_void_p * n)()
+        _check(self.L.gcf_mrc_load(self._h, path.encode(), z0, n, out), self._h)
+        return [out[k] for k in range(n)]
+
+    def autotune(self, force: bool = False) -> dict:
+        """Timed trials of the tile-kernel shapes and contraction tiles
+        (gcf_autotune); the fastest become this context's choice."""
+        t = Tuning()
+        _check(self.L.gcf_autotune(self._h, 1 if force else 0, C.byref(t)), self._h)
+        return t.as_dict()
+
+    def set_graphs(self, on: bool = True):
+        """CUDA graphs for repeated batch calls (gcf_set_graphs)."""
+        _check(self.L.gcf_set_graphs(self._h, 1 if on else 0), self._h)
+
+    def graph_info(self):
+        """(graph launches of the last batch call, nodes and library kernels
+        of the cached graph) -- gcf_get_graph_info."""
+        c = (C.c_longlong * 3)()
+        _check(self.L.gcf_get_graph_info(self._h, c), self._h)
+        return dict(zip(["graph_launches", "nodes", "kernels"], list(c)))
 
     def fast_counts(self):
         """Contraction work of the last batched call (gcf_get_fast_counts)."""
@@ -627,15 +693,17 @@ def mrc_read_tilts(path: str, n: int) -> np.ndarray:
     return out
 
 
-def write_ctf_file(path: str, results, tilts=None, names=None, is_tomo: bool = False):
-    """CSaveCtfResults::SaveCTF (+ SaveImod for tilt series)."""
+def write_ctf_file(path: str, results, tilts=None, names=None, is_tomo: bool = False,
+                   ctf_res: bool = False):
+    """CSaveCtfResults::SaveCTF (+ SaveImod for tilt series); ctf_res adds
+    the spectral-CC resolution as a last column (not in the reference)."""
     L = load_library()
     n = len(results)
     res = (Result * n)(*results)
     t = np.ascontiguousarray(tilts if tilts is not None else np.zeros(n), np.float32)
     nm = (C.c_char_p * n)(*[(x or "").encode() for x in (names or [""] * n)])
-    _check(L.gcf_write_ctf_file(path.encode(), res, t.ctypes.data, C.cast(nm, C.c_void_p), n,
-                                1 if is_tomo else 0))
+    _check(L.gcf_write_ctf_file_ex(path.encode(), res, t.ctypes.data, C.cast(nm, C.c_void_p), n,
+                                   1 if is_tomo else 0, GCF_CTF_COLUMN_RES if ctf_res else 0))
 
 
 def mrc_write(path: str, data: np.ndarray, pixel_size: float = 1.0):

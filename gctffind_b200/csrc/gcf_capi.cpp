@@ -9,10 +9,12 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -24,7 +26,19 @@ using namespace gcf;
 namespace gcf {
 // Optional: fused spectrum path (gcf_fused.cu).
 int fused_tile_supported(int tile);
+
+namespace {
+std::atomic<unsigned long long> g_alloc_epoch{0};
+thread_local bool t_capturing = false;   // this thread is capturing a batch call
+}  // namespace
+
+void note_device_alloc() { g_alloc_epoch.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long device_alloc_epoch() { return g_alloc_epoch.load(std::memory_order_relaxed); }
+cudaError_t record_timing(cudaEvent_t ev, cudaStream_t st)
+{
+    return t_capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
 }
+}  // namespace gcf
 
 namespace {
 
@@ -38,6 +52,7 @@ struct DBuf {
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
+        gcf::note_device_alloc();
         cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(cnt, 1) * sizeof(T));
         if (e == cudaSuccess) n = cnt;
         return e;
@@ -61,6 +76,65 @@ struct BandHost {
 
 struct FftPlan {
     cufftHandle h = 0;
+};
+
+// Pinned host staging of the small host -> device uploads of one call
+// (job tables, work items, descriptors): the asynchronous copies read from
+// here, so the host vectors they came from may go away, and a CUDA graph
+// captured from the call keeps valid sources for its copy nodes (a graph
+// owns the arena it was captured with).  Blocks never move; reset() reuses
+// them once the copies of the previous call are complete.
+struct HostArena {
+    struct Block {
+        char* p;
+        size_t cap, used;
+    };
+    std::vector<Block> blocks;
+    size_t cur = 0;
+    void reset()
+    {
+        for (Block& b : blocks) b.used = 0;
+        cur = 0;
+    }
+    void* put(const void* src, size_t bytes)
+    {
+        const size_t need = (bytes + 255) & ~(size_t)255;
+        while (cur < blocks.size() && blocks[cur].cap - blocks[cur].used < need) ++cur;
+        if (cur == blocks.size()) {
+            Block b{nullptr, std::max<size_t>(need, (size_t)1 << 20), 0};
+            if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+            blocks.push_back(b);
+        }
+        Block& b = blocks[cur];
+        void* dst = b.p + b.used;
+        std::memcpy(dst, src, bytes);
+        b.used += need;
+        return dst;
+    }
+    void release()
+    {
+        for (Block& b : blocks) cudaFreeHost(b.p);
+        blocks.clear();
+        cur = 0;
+    }
+};
+
+// One captured batch call (gcf_run_batch / gcf_run_batch_mode with CUDA
+// graphs on): the graph of its device work, keyed by everything the work
+// depends on, and what the host needs to read its results back.
+struct BatchGraph {
+    unsigned long long key = 0;
+    int seen = 0;                      // eager calls with this key so far
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long epoch = 0;      // device-allocation epoch at capture
+    unsigned long long model_version = 0;   // contraction model rows it read
+    HostArena arena;                   // sources of the graph's upload nodes
+    int kev_used = 0;
+    long long launches = 0;            // kernels this library launched in it
+    int nodes = 0;                     // graph nodes
+    std::vector<float> pxn;            // search pixel size of each slot
+    std::vector<int> band;             // band slot of each job
+    int nj = 0;
 };
 
 }  // namespace
@@ -184,11 +258,53 @@ struct gcf_ctx {
     NnNet* nn = nullptr;
     bool nn_ready = false;            // weights set (loaded, trained or given)
     float learned_tau = 0.1f;         // refined CC below which the full search runs
+    gcf_package_fn pkg_fn = nullptr;  // per-package completion hook of gcf_run_series
+    void* pkg_user = nullptr;
     DBuf<__nv_bfloat16> nx1, nx2;     // network inputs of a chunk of jobs
     DBuf<float> npx, nparams, ntarget, nloss;
+    // MRC sections loaded to the device (gcf_mrc_load): float images, the
+    // raw section bytes of two in flight, their pinned host staging
+    DBuf<float> loaded;
+    DBuf<unsigned char> ingest_raw;
+    unsigned char* ingest_pin = nullptr;
+    size_t ingest_pin_bytes = 0;
+    cudaEvent_t ingest_copied[2] = {}, ingest_used[2] = {};
+    unsigned long long nn_version = 0;   // bumped whenever the weights change
+    unsigned long long model_version = 0;   // bumped whenever the model rows are remade
+
+    // host staging of this call's uploads; CUDA graphs of batch calls
+    HostArena arena;
+    bool graphs = false;              // gcf_set_graphs
+    bool capturing = false;           // inside a stream capture of ctx->st
+    BatchGraph bgraph;
+    cudaEvent_t fork_ev = nullptr;    // dependency-only fork of st_copy from st
+    long long graph_launches = 0;     // graph launches of the last batch call
 };
 
 namespace {
+
+// Host -> device upload of `bytes` from a transient host buffer, staged
+// through the context's pinned arena.  Outside a capture, an arena that has
+// grown past 64 MB is recycled once the context's streams are idle.
+cudaError_t h2d(gcf_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+    if (bytes == 0) return cudaSuccess;
+    if (!ctx->capturing) {
+        size_t used = 0;
+        for (const HostArena::Block& b : ctx->arena.blocks) used += b.used;
+        if (used > ((size_t)64 << 20)) {
+            for (cudaStream_t s : {ctx->st, ctx->st_copy, ctx->st_search, ctx->st_tile, ctx->st_solo})
+                if (s) {
+                    cudaError_t e = cudaStreamSynchronize(s);
+                    if (e != cudaSuccess) return e;
+                }
+            ctx->arena.reset();
+        }
+    }
+    void* h = ctx->arena.put(src, bytes);
+    if (!h) return cudaErrorMemoryAllocation;
+    return cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, st);
+}
 
 gcf_status fail(gcf_ctx* c, gcf_status s, const char* what)
 {
@@ -409,12 +525,12 @@ gcf_status get_band(gcf_ctx* ctx, const gcf_optics& op, float px_n, int* slot)
     }
     // On the compute stream, so the kernels that read the band are ordered
     // after the copies (a pageable source is staged before the call returns).
-    CK(cudaMemcpyAsync(b->idx.p, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(b->a.p, va.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(b->d.p, vd.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(b->env.p, ve.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(b->c2t.p, vc.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(b->s2t.p, vs.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, b->idx.p, idx.data(), n * sizeof(int), ctx->st));
+    CK(h2d(ctx, b->a.p, va.data(), n * sizeof(float), ctx->st));
+    CK(h2d(ctx, b->d.p, vd.data(), n * sizeof(float), ctx->st));
+    CK(h2d(ctx, b->env.p, ve.data(), n * sizeof(float), ctx->st));
+    CK(h2d(ctx, b->c2t.p, vc.data(), n * sizeof(float), ctx->st));
+    CK(h2d(ctx, b->s2t.p, vs.data(), n * sizeof(float), ctx->st));
     b->dev.n = b->n;
     b->dev.cx = cx;
     b->dev.cy = cy;
@@ -437,7 +553,7 @@ gcf_status upload_bands(gcf_ctx* ctx)
     std::vector<BandDev> v;
     for (auto* b : ctx->bands) v.push_back(b->dev);
     CK(ctx->d_bands.ensure(v.size()));
-    CK(cudaMemcpyAsync(ctx->d_bands.p, v.data(), v.size() * sizeof(BandDev), cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, ctx->d_bands.p, v.data(), v.size() * sizeof(BandDev), ctx->st));
     ctx->bands_dirty = false;
     return GCF_OK;
 }
@@ -582,17 +698,17 @@ gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
         bptr[i] = ctx->f_bsum.p + boff[i];
         d[i].bsum = bptr[i];
     }
-    CK(cudaMemcpyAsync(ctx->f_bsum_ptr.p, bptr.data(), nm * sizeof(double*), cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, ctx->f_bsum_ptr.p, bptr.data(), nm * sizeof(double*), ctx->st));
     CK(ctx->f_desc.ensure(nm));
     CK(ctx->f_items.ensure(ni));
     CK(ctx->f_first.ensure(nm + 1));
     CK(ctx->f_inv.ensure(nm));
     CK(ctx->f_partial.ensure((size_t)ni * cx * T));
     CK(ctx->f_next.ensure(nm));
-    CK(cudaMemcpyAsync(ctx->f_desc.p, d.data(), nm * sizeof(FusedImageDesc), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->f_items.p, items.data(), ni * sizeof(int4), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->f_inv.p, inv.data(), nm * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, ctx->f_desc.p, d.data(), nm * sizeof(FusedImageDesc), ctx->st));
+    CK(h2d(ctx, ctx->f_items.p, items.data(), ni * sizeof(int4), ctx->st));
+    CK(h2d(ctx, ctx->f_first.p, first.data(), (nm + 1) * sizeof(int), ctx->st));
+    CK(h2d(ctx, ctx->f_inv.p, inv.data(), nm * sizeof(float), ctx->st));
     return GCF_OK;
 }
 
@@ -751,11 +867,11 @@ gcf_status spectra(gcf_ctx* ctx, const std::vector<MicImage>& mics)
 {
     int nm = (int)mics.size();
     CKS(spectra_alloc(ctx, nm));
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(record_timing(ctx->ev[2], ctx->st));
     CKS(spectra_chunk(ctx, mics, 0, nm));
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(record_timing(ctx->ev[3], ctx->st));
     CKS(spectra_post(ctx, nm));
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(record_timing(ctx->ev[4], ctx->st));
     return GCF_OK;
 }
 
@@ -861,10 +977,8 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     CK(ctx->d_res.ensure(nj));
     CK(ctx->arrive.ensure(nj));
     CK(cudaMemsetAsync(ctx->arrive.p, 0, nj * sizeof(int), ctx->st));
-    CK(cudaMemcpyAsync(ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), cudaMemcpyHostToDevice,
-                       ctx->st));
-    CK(cudaMemcpyAsync(ctx->spec_off.p, soff.data(), nj * sizeof(int), cudaMemcpyHostToDevice,
-                       ctx->st));
+    CK(h2d(ctx, ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), ctx->st));
+    CK(h2d(ctx, ctx->spec_off.p, soff.data(), nj * sizeof(int), ctx->st));
     launch_band_gather(ctx->ctf.p, (int)cmp_n, ctx->jobs.p, ctx->d_bands.p, ctx->spec_off.p, nj,
                        ctx->band_spec.p, ctx->sum_ss.p, ctx->st);
     CKL();
@@ -881,7 +995,7 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     a.arrive = ctx->arrive.p;
     a.max_chunks = max_chunks;
     a.njobs = nj;
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    CK(record_timing(ctx->ev[5], ctx->st));
     if (any_full || any_1d) {
         launch_search1d(ctx->jobs.p, nj, ctx->radial.p, cx, ctx->cand.p, ctx->cval.p, ctx->st);
         CKL();
@@ -890,7 +1004,7 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     launch_init_jobs(a, ctx->st);   // Refine jobs: pending step CC0
     CKL();
     ctx->launches += 1;
-    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    CK(record_timing(ctx->ev[6], ctx->st));
     // Upper bound of non-empty steps: CC0 + astigmatism grid + 19 x 4 refinements.
     bool any_2d = false;
     for (const JobSpec& s : specs) any_2d = any_2d || s.mode <= 1;
@@ -923,7 +1037,7 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
     launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->d_counts.p, ctx->st);
     CKL();
     ctx->launches += 1;
-    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    CK(record_timing(ctx->ev[7], ctx->st));
     for (int j = 0; j < nj; ++j) pend.band[j] = jh[j].band;
     return GCF_OK;
 }
@@ -1054,9 +1168,9 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     CK(ctx->d_res.ensure(nj));
     CK(ctx->arrive.ensure(nj));
     CK(cudaMemsetAsync(ctx->arrive.p, 0, nj * sizeof(int), ctx->st));
-    CK(cudaMemcpyAsync(ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->spec_off.p, soff.data(), nj * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    CK(h2d(ctx, ctx->jobs.p, jh.data(), nj * sizeof(SearchJob), ctx->st));
+    CK(h2d(ctx, ctx->spec_off.p, soff.data(), nj * sizeof(int), ctx->st));
+    CK(record_timing(ctx->ev[5], ctx->st));
     launch_band_gather(ctx->ctf.p, (int)cmp_n, ctx->jobs.p, ctx->d_bands.p, ctx->spec_off.p, nj, ctx->band_spec.p,
                        ctx->sum_ss.p, ctx->st);
     CKL();
@@ -1070,6 +1184,7 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
         ctx->launches += 1;
         ctx->model_grid = g;
         ctx->have_model = true;
+        ctx->model_version += 1;
     }
     const long long ncols = (long long)nj * g.nth;
     CK(ctx->cB.ensure((size_t)ncols * g.ns));
@@ -1087,13 +1202,13 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     CK(ctx->cErr.ensure(1));
     for (auto& e : ctx->fev)
         if (!e) CK(cudaEventCreate(&e));
-    CK(cudaEventRecord(ctx->fev[0], ctx->st));
+    CK(record_timing(ctx->fev[0], ctx->st));
     CK(launch_polar_bin(ctx->ctf.p, T, ctx->jobs.p, nj, g, ctx->cB.p, ctx->cE.p, ctx->cSS.p, ctx->st));
     launch_job_rows(ctx->jobs.p, nj, prior, g, ctx->cRows.p, ctx->st);
     CKL();
     CK(cudaMemsetAsync(ctx->cNtiles.p, 0, sizeof(int), ctx->st));
     CK(cudaMemsetAsync(ctx->cErr.p, 0, sizeof(int), ctx->st));
-    CK(cudaEventRecord(ctx->fev[1], ctx->st));
+    CK(record_timing(ctx->fev[1], ctx->st));
     launch_plan_tiles(ctx->cRows.p, nj, g.nth, g.nz, bn, ctx->cTiles.p, ctx->cNtiles.p, max_tiles, ctx->st);
     CKL();
     // P = A B^T over the planned tiles; Dz = E A2^T (every row of every job)
@@ -1116,7 +1231,7 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     gd.err = ctx->cErr.p;
     CK(launch_umma_gemm(ctx->cE.p, g.ns, ctx->cA2.p, g.ns, gd, 256, 4, 0, ctx->st));
     ctx->launches += 6;
-    CK(cudaEventRecord(ctx->fev[2], ctx->st));
+    CK(record_timing(ctx->fev[2], ctx->st));
     TableArgs ta;
     ta.jobs = ctx->jobs.p;
     ta.njobs = nj;
@@ -1133,8 +1248,8 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     launch_table_search(ta, ctx->st);
     CKL();
     ctx->launches += 1;
-    CK(cudaEventRecord(ctx->ev[6], ctx->st));
-    CK(cudaEventRecord(ctx->fev[3], ctx->st));
+    CK(record_timing(ctx->ev[6], ctx->st));
+    CK(record_timing(ctx->fev[3], ctx->st));
     EvalArgs a;
     a.jobs = ctx->jobs.p;
     a.bands = ctx->d_bands.p;
@@ -1153,7 +1268,7 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
         CKL();
         ctx->launches += 1;
     }
-    CK(cudaEventRecord(ctx->fev[4], ctx->st));
+    CK(record_timing(ctx->fev[4], ctx->st));
     CK(ctx->ring_sums.ensure((size_t)nj * cx * 6));
     launch_ctf_res(ctx->ctf.p, T, ctx->jobs.p, nj, ctx->ring_off.p, ctx->ring_pix.p, ctx->ring_geo.p,
                    ctx->ring_sums.p, ctx->cc_res.p, ctx->st);
@@ -1164,7 +1279,7 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     launch_results(ctx->jobs.p, nj, ctx->lowpassed.p, ctx->d_res.p, ctx->d_counts.p, ctx->st);
     CKL();
     ctx->launches += 4;
-    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    CK(record_timing(ctx->ev[7], ctx->st));
     for (int j = 0; j < nj; ++j) pend.band[j] = jh[j].band;
     return GCF_OK;
 }
@@ -1225,7 +1340,7 @@ gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
     CK(ctx->cPrior.ensure(n));
     CK(ctx->nx1.ensure((size_t)kNnChunk * kNnProfile));
     CK(ctx->nx2.ensure((size_t)kNnChunk * kNnMap * kNnMap));
-    CK(cudaMemcpyAsync(ctx->npx.p, px_n.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, ctx->npx.p, px_n.data(), n * sizeof(float), ctx->st));
     const size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
     for (int c0 = 0; c0 < n; c0 += kNnChunk) {
         const int cn = std::min(kNnChunk, n - c0);
@@ -1238,8 +1353,9 @@ gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
     return GCF_OK;
 }
 
-gcf_status search_slots(gcf_ctx* ctx, const std::vector<float>& px_n, const gcf_optics& op, int mode,
-                        std::vector<gcf_result>& out)
+// Search jobs of slots 0 .. n-1 for a method.  raw_px (nullable): the raw
+// pixel size of each slot, kept in its optics as gcf_run_batch does.
+std::vector<JobSpec> slot_jobs(const std::vector<float>& px_n, const float* raw_px, const gcf_optics& op, int mode)
 {
     const int n = (int)px_n.size();
     std::vector<JobSpec> js(n);
@@ -1248,27 +1364,43 @@ gcf_status search_slots(gcf_ctx* ctx, const std::vector<float>& px_n, const gcf_
         js[i].mic = i;
         js[i].mode = mode == GCF_SEARCH_PLAIN ? 0 : 4;
         js[i].optics = op;
+        if (raw_px) js[i].optics.pixel_size = raw_px[i];
         js[i].px_n = px_n[i];
         js[i].phase_deg = op.ext_phase_deg;
         js[i].phase_range = mode == GCF_SEARCH_PLAIN ? fmaxf(op.ext_phase_range, 0.0f) : 0.0f;
     }
-    if (mode == GCF_SEARCH_PLAIN) return run_search(ctx, js, out);
+    return js;
+}
+
+// Enqueues the searches of slots 0 .. n-1 (already post-processed) with
+// the chosen method; nothing is read back.
+gcf_status search_enqueue(gcf_ctx* ctx, const std::vector<float>& px_n, const float* raw_px, const gcf_optics& op,
+                          int mode, SearchPending& pend)
+{
+    std::vector<JobSpec> js = slot_jobs(px_n, raw_px, op, mode);
+    if (mode == GCF_SEARCH_PLAIN) return run_search_enqueue(ctx, js, pend);
     const float4* prior = nullptr;
     if (mode == GCF_SEARCH_LEARNED) {
         CKS(learned_priors(ctx, px_n));
         prior = ctx->cPrior.p;
     }
-    SearchPending pend;
-    CKS(run_fast_enqueue(ctx, js, prior, pend));
+    return run_fast_enqueue(ctx, js, prior, pend);
+}
+
+// Reads back an enqueued search.  A learned search falls back to the full
+// contraction search where the learned window's refined result is not
+// trusted: its CC is below the threshold, or its mean defocus ends within
+// two final steps of the window's edge (the optimum may lie outside).
+gcf_status search_collect(gcf_ctx* ctx, const std::vector<float>& px_n, const float* raw_px, const gcf_optics& op,
+                          int mode, const SearchPending& pend, std::vector<gcf_result>& out)
+{
+    if (mode == GCF_SEARCH_PLAIN) return run_search_collect(ctx, pend, out);
     CKS(run_fast_collect(ctx, pend, out, nullptr));
     if (mode != GCF_SEARCH_LEARNED) return GCF_OK;
-    // Fallback to the full contraction search where the learned window's
-    // refined result is not trusted: its CC is below the threshold, or its
-    // mean defocus ends within one local step of the window's edge (the
-    // optimum may lie outside).
+    const int n = (int)px_n.size();
     std::vector<SearchJob> jh(n);
     CK(cudaMemcpy(jh.data(), ctx->jobs.p, n * sizeof(SearchJob), cudaMemcpyDeviceToHost));
-    std::vector<JobSpec> redo;
+    std::vector<JobSpec> js = slot_jobs(px_n, raw_px, op, mode), redo;
     std::vector<int> idx;
     for (int i = 0; i < n; ++i) {
         const SearchJob& J = jh[i];
@@ -1281,12 +1413,21 @@ gcf_status search_slots(gcf_ctx* ctx, const std::vector<float>& px_n, const gcf_
     }
     ctx->fast_counts[3] += (long long)redo.size();
     if (redo.empty()) return GCF_OK;
+    // the fallback's counts and times add to the first pass's
     std::vector<gcf_result> r2;
     SearchPending p2;
     CKS(run_fast_enqueue(ctx, redo, nullptr, p2));
     CKS(run_fast_collect(ctx, p2, r2, nullptr));
     for (size_t k = 0; k < idx.size(); ++k) out[idx[k]] = r2[k];
     return GCF_OK;
+}
+
+gcf_status search_slots(gcf_ctx* ctx, const std::vector<float>& px_n, const gcf_optics& op, int mode,
+                        std::vector<gcf_result>& out)
+{
+    SearchPending pend;
+    CKS(search_enqueue(ctx, px_n, nullptr, op, mode, pend));
+    return search_collect(ctx, px_n, nullptr, op, mode, pend, out);
 }
 
 // Synthetic raw spectra of samples first .. first + n - 1 of the generator
@@ -1405,9 +1546,13 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->chunk_ev.push_back(e);
     }
-    CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    if (!on_device) CK(cudaStreamWaitEvent(ctx->st_copy, ctx->ev[0], 0));
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(record_timing(ctx->ev[0], ctx->st));
+    if (!on_device) {
+        if (!ctx->fork_ev) CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ctx->fork_ev, ctx->st));
+        CK(cudaStreamWaitEvent(ctx->st_copy, ctx->fork_ev, 0));
+    }
+    CK(record_timing(ctx->ev[2], ctx->st));
     size_t roff = 0, roff_new = 0;
     for (int c = 0; c < nchunks; ++c) {
         int i0 = c * kChunk, i1 = std::min(n, i0 + kChunk);
@@ -1420,12 +1565,14 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
                 dimg[i - i0] = ctx->images.p + roff;
                 roff += cnt;
             }
+            // the timing record first: in a capture, the chunk event joins
+            // everything on the copy stream back into st
+            if (c == nchunks - 1) CK(record_timing(ctx->ev[1], ctx->st_copy));
             CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st_copy));
-            if (c == nchunks - 1) CK(cudaEventRecord(ctx->ev[1], ctx->st_copy));
             CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
         } else {
             for (int i = i0; i < i1; ++i) dimg[i - i0] = images[i];
-            if (c == 0) CK(cudaEventRecord(ctx->ev[1], ctx->st));
+            if (c == 0) CK(record_timing(ctx->ev[1], ctx->st));
         }
         for (int i = i0; i < i1; ++i) {
             size_t used = 0;
@@ -1435,9 +1582,9 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
         }
         CKS(spectra_chunk(ctx, mics, i0, i1 - i0));
     }
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(record_timing(ctx->ev[3], ctx->st));
     CKS(spectra_post(ctx, n));
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(record_timing(ctx->ev[4], ctx->st));
     return GCF_OK;
 }
 
@@ -1494,11 +1641,9 @@ gcf_status full_spectra(gcf_ctx* ctx, const std::vector<int>& mics,
     CK(ctx->mic_of.ensure(k));
     CK(ctx->d_res.ensure(std::max<size_t>(k, ctx->d_res.n)));
     CK(ctx->full.ensure((size_t)k * T * T));
-    CK(cudaMemcpyAsync(ctx->d_optics.p, o.data(), k * sizeof(PixOptics), cudaMemcpyHostToDevice,
-                       ctx->st));
-    CK(cudaMemcpyAsync(ctx->mic_of.p, mics.data(), k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->d_res.p, res.data(), k * sizeof(gcf_result), cudaMemcpyHostToDevice,
-                       ctx->st));
+    CK(h2d(ctx, ctx->d_optics.p, o.data(), k * sizeof(PixOptics), ctx->st));
+    CK(h2d(ctx, ctx->mic_of.p, mics.data(), k * sizeof(int), ctx->st));
+    CK(h2d(ctx, ctx->d_res.p, res.data(), k * sizeof(gcf_result), ctx->st));
     launch_full_spectrum(ctx->ctf.p, T, k, ctx->mic_of.p, ctx->d_res.p, ctx->d_optics.p,
                          ctx->moments2.p, 0.0f, ctx->full.p, ctx->st);
     CKL();
@@ -1645,6 +1790,17 @@ void gcf_destroy(gcf_ctx* ctx)
     for (auto& ev : ctx->kev) cudaEventDestroy(ev);
     for (auto& ev : ctx->fev)
         if (ev) cudaEventDestroy(ev);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->ingest_copied[k]) cudaEventDestroy(ctx->ingest_copied[k]);
+        if (ctx->ingest_used[k]) cudaEventDestroy(ctx->ingest_used[k]);
+    }
+    if (ctx->ingest_pin) cudaFreeHost(ctx->ingest_pin);
+    ctx->loaded.release();
+    ctx->ingest_raw.release();
+    if (ctx->bgraph.exec) cudaGraphExecDestroy(ctx->bgraph.exec);
+    ctx->bgraph.arena.release();
+    ctx->arena.release();
     if (ctx->nn) nn_destroy(ctx->nn);
     ctx->nx1.release();
     ctx->nx2.release();
@@ -1880,7 +2036,7 @@ gcf_status gcf_background1d(gcf_ctx* ctx, const float* spectrum, int n, int on_d
     if (!on_device) {
         CK(ctx->bg_spec.ensure(n));
         CK(ctx->bg_curve.ensure(n));
-        CK(cudaMemcpyAsync(ctx->bg_spec.p, spectrum, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        CK(h2d(ctx, ctx->bg_spec.p, spectrum, n * sizeof(float), ctx->st));
         d_in = ctx->bg_spec.p;
         d_out = ctx->bg_curve.p;
     }
@@ -1904,8 +2060,8 @@ static gcf_status remove_bg(gcf_ctx* ctx, float* spec, size_t spec_n, int n_or_t
     if (!on_device) {
         CK(ctx->bg_spec.ensure(spec_n));
         CK(ctx->bg_curve.ensure(bg_n));
-        CK(cudaMemcpyAsync(ctx->bg_spec.p, spec, spec_n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->bg_curve.p, bg, bg_n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        CK(h2d(ctx, ctx->bg_spec.p, spec, spec_n * sizeof(float), ctx->st));
+        CK(h2d(ctx, ctx->bg_curve.p, bg, bg_n * sizeof(float), ctx->st));
         d_spec = ctx->bg_spec.p;
         d_bg = ctx->bg_curve.p;
     }
@@ -1989,6 +2145,15 @@ struct SeriesLoop {
     std::vector<gcf_result> res;
     std::vector<int> ref_used;   // slot whose result seeded this slot's refine
     int cur_ref = -1;
+    const int* image_of = nullptr;   // slot -> caller's image index
+    int done = 0;
+
+    // Slot k's result is final: report it to the caller's hook.
+    void finalize(int k)
+    {
+        done = k + 1;
+        if (ctx->pkg_fn) ctx->pkg_fn(ctx->pkg_user, done, image_of ? image_of[k] : k, &res[k]);
+    }
 
     JobSpec full_job(int slot) const
     {
@@ -2038,6 +2203,7 @@ struct SeriesLoop {
             CKS(run_search(ctx, {full_job(0)}, r));
             res[0] = r[0];
             cur_ref = 0;
+            finalize(0);
             ++k;
         }
         bool batch_valid = false;
@@ -2072,6 +2238,7 @@ struct SeriesLoop {
                 cur_ref = new_ref;
                 batch_valid = false;
             }
+            finalize(k);
             ++k;
         }
         return GCF_OK;
@@ -2120,7 +2287,7 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->chunk_ev.push_back(e);
     }
-    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    CK(record_timing(ctx->ev[0], ctx->st));
     CK(cudaStreamWaitEvent(ctx->st_copy, ctx->ev[0], 0));
     const size_t cnt = (size_t)w * h;
     for (int c = 0; c < nchunks; ++c) {
@@ -2129,8 +2296,8 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
                                ctx->st_copy));
         CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st_copy));
     }
-    CK(cudaEventRecord(ctx->ev[1], ctx->st_copy));
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(record_timing(ctx->ev[1], ctx->st_copy));
+    CK(record_timing(ctx->ev[2], ctx->st));
     // every chunk's spectra on st as its copy lands ...
     for (int c = 0; c < nchunks; ++c) {
         const int k0 = bounds[c], k1 = bounds[c + 1];
@@ -2143,8 +2310,8 @@ gcf_status series_streamed(gcf_ctx* ctx, const std::vector<const float*>& imgs, 
         CKS(spectra_chunk(ctx, mics, k0, k1 - k0));
         CK(cudaEventRecord(ctx->chunk_ev[nchunks + c], ctx->st));
     }
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(record_timing(ctx->ev[3], ctx->st));
+    CK(record_timing(ctx->ev[4], ctx->st));
     // ... and its post-processing and package searches on the low-priority
     // search stream once they are done, so that no chunk's spectra wait for
     // the searches of the chunks before it
@@ -2201,9 +2368,9 @@ gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->chunk_ev.push_back(e);
     }
-    CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(record_timing(ctx->ev[0], ctx->st));
+    CK(record_timing(ctx->ev[1], ctx->st));
+    CK(record_timing(ctx->ev[2], ctx->st));
     for (int k = 0; k < n; ++k) {
         size_t used = 0;
         float* dst = rescaled ? ctx->rescaled.p + (size_t)nw * nh * k : nullptr;
@@ -2228,8 +2395,8 @@ gcf_status series_overlapped(gcf_ctx* ctx, const std::vector<const float*>& imgs
             CK(cudaEventRecord(ctx->chunk_ev[c], ctx->st));
         }
     }
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(record_timing(ctx->ev[3], ctx->st));
+    CK(record_timing(ctx->ev[4], ctx->st));
     auto search_phase = [&]() -> gcf_status {
         for (int c = 0; c < nchunks; ++c) {
             CK(cudaStreamWaitEvent(ctx->st, ctx->chunk_ev[c], 0));
@@ -2280,6 +2447,7 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
     float pxn;
     gcf_rescale_dims(w, h, optics->pixel_size, &nw, &nh, &pxn);
     SeriesLoop loop{ctx, *optics, pxn, is_tomo, std::vector<gcf_result>(n), std::vector<int>(n, -1)};
+    loop.image_of = order;
     std::vector<MicImage> mics;
     gcf_status st;
     if (on_device) {
@@ -2310,74 +2478,151 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
     return st;
 }
 
-gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
-                         const gcf_optics* optics, gcf_result* results)
+gcf_status gcf_set_package_callback(gcf_ctx* ctx, gcf_package_fn fn, void* user)
 {
-    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
-    std::vector<const float*> imgs(n);
-    std::vector<int> ws(n), hs(n);
-    std::vector<float> pxs(n);
-    for (int i = 0; i < n; ++i) {
-        if (!items[i].image || items[i].width <= 0 || items[i].height <= 0 ||
-            !(items[i].pixel_size > 0))
-            return GCF_ERR_INVALID_ARG;
-        imgs[i] = items[i].image;
-        ws[i] = items[i].width;
-        hs[i] = items[i].height;
-        pxs[i] = items[i].pixel_size;
-    }
-    CKS(set_device(ctx));
-    for (float& t : ctx->stage_ms) t = 0.0f;
-    for (long long& c : ctx->search_counts) c = 0;
-    ctx->kev_used = 0;
-    ctx->launches = 0;
-    cudaEvent_t t0, t1;
-    CK(cudaEventCreate(&t0));
-    CK(cudaEventCreate(&t1));
-    CK(cudaEventRecord(t0, ctx->st));
-    std::vector<MicImage> mics;
-    gcf_status st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics);
-    if (st == GCF_OK) {
-        std::vector<JobSpec> js(n);
-        for (int i = 0; i < n; ++i) {
-            std::memset(&js[i], 0, sizeof(JobSpec));
-            js[i].mic = i;
-            js[i].mode = 0;
-            js[i].optics = *optics;
-            js[i].optics.pixel_size = pxs[i];
-            js[i].px_n = mics[i].px_n;
-            js[i].phase_deg = optics->ext_phase_deg;
-            js[i].phase_range = fmaxf(optics->ext_phase_range, 0.0f);
-        }
-        std::vector<gcf_result> r;
-        st = run_search(ctx, js, r);
-        if (st == GCF_OK)
-            for (int i = 0; i < n; ++i) results[i] = r[i];
-    }
-    cudaEventRecord(t1, ctx->st);
-    cudaEventSynchronize(t1);
-    if (st == GCF_OK) accumulate_stage_times(ctx);
-    float tt = 0;
-    cudaEventElapsedTime(&tt, t0, t1);
-    ctx->stage_ms[6] = tt;
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    return st;
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    ctx->pkg_fn = fn;
+    ctx->pkg_user = fn ? user : nullptr;
+    return GCF_OK;
 }
 
-gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
-                              const gcf_optics* optics, int mode, gcf_result* results)
-{
-    if (mode == GCF_SEARCH_PLAIN) return gcf_run_batch(ctx, items, n, on_device, optics, results);
-    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
-    if (mode != GCF_SEARCH_BF16 && mode != GCF_SEARCH_LEARNED) return GCF_ERR_INVALID_ARG;
-    if (optics->ext_phase_range > 0) {
-        // the table search has no extra-phase dimension: phase-plate data
-        // take the plain search
-        return gcf_run_batch(ctx, items, n, on_device, optics, results);
+}  // extern "C"
+
+namespace {
+
+// FNV-1a over everything the device work of a batch call depends on.
+struct KeyHash {
+    unsigned long long h = 1469598103934665603ull;
+    void add(const void* p, size_t n)
+    {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
     }
-    if (mode == GCF_SEARCH_LEARNED && !ctx->nn_ready)
-        return fail(ctx, GCF_ERR_STATE, "learned search: no network weights (gcf_nn_load / gcf_nn_train)");
+    template <class T>
+    void v(const T& x)
+    {
+        add(&x, sizeof(T));
+    }
+};
+
+unsigned long long batch_key(const gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
+                             const gcf_optics& op, int mode)
+{
+    KeyHash k;
+    k.v(mode);
+    k.v(n);
+    k.v(on_device);
+    k.add(items, (size_t)n * sizeof(gcf_item));
+    k.v(op);
+    k.v(ctx->tile);
+    k.v(ctx->impl);
+    k.v(ctx->log_spect);
+    k.v(ctx->fused_shape);
+    k.v(ctx->fused_clusters);
+    k.v(ctx->gemm_bn);
+    k.v(ctx->gemm_stages);
+    k.v(ctx->contract_dz);
+    k.v(ctx->contract_ns);
+    k.v(ctx->contract_nth);
+    k.v(ctx->nn_version);
+    return k.h;
+}
+
+// Host inputs take a graph only from page-locked memory (a graph's copy
+// nodes read the same host addresses again on every replay).
+bool all_pinned(const float* const* imgs, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, imgs[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
+// Device work of a batch call: uploads (host inputs), rescale, spectra,
+// post-processing, searches enqueued; nothing read back.
+gcf_status batch_enqueue(gcf_ctx* ctx, const std::vector<const float*>& imgs, const std::vector<int>& ws,
+                         const std::vector<int>& hs, const std::vector<float>& pxs, int on_device,
+                         const gcf_optics& op, int mode, SearchPending& pend, std::vector<float>& pxn)
+{
+    const int n = (int)imgs.size();
+    std::vector<MicImage> mics;
+    CKS(prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics));
+    pxn.resize(n);
+    for (int i = 0; i < n; ++i) pxn[i] = mics[i].px_n;
+    return search_enqueue(ctx, pxn, mode == GCF_SEARCH_PLAIN ? pxs.data() : nullptr, op, mode, pend);
+}
+
+// Captures batch_enqueue into ctx->bgraph (the graph then owns the arena
+// its upload nodes read).  false: the capture did not produce a graph that
+// may be replayed (the caller runs the call eagerly).
+bool batch_capture(gcf_ctx* ctx, unsigned long long key, const std::vector<const float*>& imgs,
+                   const std::vector<int>& ws, const std::vector<int>& hs, const std::vector<float>& pxs,
+                   int on_device, const gcf_optics& op, int mode)
+{
+    BatchGraph& G = ctx->bgraph;
+    G.arena.reset();
+    std::swap(ctx->arena, G.arena);   // this capture's uploads go to the graph's arena
+    const unsigned long long ep0 = device_alloc_epoch();
+    const unsigned long long mv0 = ctx->model_version;
+    const long long launches0 = ctx->launches;
+    SearchPending pend;
+    std::vector<float> pxn;
+    cudaGraph_t g = nullptr;
+    gcf_status st = GCF_ERR_CUDA;
+    if (cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        ctx->capturing = true;
+        t_capturing = true;
+        st = batch_enqueue(ctx, imgs, ws, hs, pxs, on_device, op, mode, pend, pxn);
+        ctx->capturing = false;
+        t_capturing = false;
+        if (cudaStreamEndCapture(ctx->st, &g) != cudaSuccess) g = nullptr;
+    }
+    std::swap(ctx->arena, G.arena);
+    cudaGetLastError();
+    bool ok = st == GCF_OK && g && device_alloc_epoch() == ep0;
+    if (ok) {
+        cudaGraphExecUpdateResultInfo info;
+        if (!(G.exec && cudaGraphExecUpdate(G.exec, g, &info) == cudaSuccess)) {
+            cudaGetLastError();
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
+            ok = cudaGraphInstantiate(&G.exec, g, 0) == cudaSuccess;
+        }
+    }
+    if (ok) {
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        G.nodes = (int)nn;
+        G.key = key;
+        G.epoch = ep0;
+        G.model_version = mv0 == ctx->model_version ? mv0 : ctx->model_version;
+        G.kev_used = ctx->kev_used;
+        G.launches = ctx->launches - launches0;
+        G.pxn = pxn;
+        G.band = pend.band;
+        G.nj = pend.nj;
+    } else {
+        cudaGetLastError();
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+        G.key = 0;
+        G.seen = 0;
+    }
+    if (g) cudaGraphDestroy(g);
+    return ok;
+}
+
+// gcf_run_batch / gcf_run_batch_mode.  With CUDA graphs on, a call whose
+// key repeats an earlier call's is captured once and then replayed as one
+// graph launch.
+gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, const gcf_optics* optics, int mode,
+                     gcf_result* results)
+{
     std::vector<const float*> imgs(n);
     std::vector<int> ws(n), hs(n);
     std::vector<float> pxs(n);
@@ -2396,17 +2641,45 @@ gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int on
     for (float& t : ctx->fast_ms) t = 0.0f;
     ctx->kev_used = 0;
     ctx->launches = 0;
+    ctx->graph_launches = 0;
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     CK(cudaEventRecord(t0, ctx->st));
-    std::vector<MicImage> mics;
-    gcf_status st = prepare_images(ctx, imgs.data(), ws.data(), hs.data(), pxs.data(), n, on_device, mics);
+    BatchGraph& G = ctx->bgraph;
+    const bool graphable = ctx->graphs && (on_device || all_pinned(imgs.data(), n));
+    const unsigned long long key = graphable ? batch_key(ctx, items, n, on_device, *optics, mode) : 0;
+    bool replay = graphable && G.exec && G.key == key && G.epoch == device_alloc_epoch() &&
+                  G.model_version == ctx->model_version;
+    if (!replay && graphable && G.key == key && G.seen >= 1)
+        replay = batch_capture(ctx, key, imgs, ws, hs, pxs, on_device, *optics, mode);
+    SearchPending pend;
+    std::vector<float> pxn;
+    gcf_status st = GCF_OK;
+    if (replay) {
+        cudaError_t e = cudaGraphLaunch(G.exec, ctx->st);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "cudaGraphLaunch");
+        pend.nj = G.nj;
+        pend.st = ctx->st;
+        pend.band = G.band;
+        pxn = G.pxn;
+        ctx->kev_used = G.kev_used;
+        ctx->launches = G.launches;
+        ctx->graph_launches = 1;
+    } else {
+        ctx->arena.reset();   // every earlier call has completed
+        st = batch_enqueue(ctx, imgs, ws, hs, pxs, on_device, *optics, mode, pend, pxn);
+        if (graphable) {
+            if (G.key != key) {
+                G.key = key;
+                G.seen = 0;
+            }
+            G.seen += 1;
+        }
+    }
     if (st == GCF_OK) {
-        std::vector<float> pxn(n);
-        for (int i = 0; i < n; ++i) pxn[i] = mics[i].px_n;
         std::vector<gcf_result> r;
-        st = search_slots(ctx, pxn, *optics, mode, r);
+        st = search_collect(ctx, pxn, mode == GCF_SEARCH_PLAIN ? pxs.data() : nullptr, *optics, mode, pend, r);
         if (st == GCF_OK)
             for (int i = 0; i < n; ++i) results[i] = r[i];
     }
@@ -2421,6 +2694,266 @@ gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int on
     return st;
 }
 
+}  // namespace
+
+extern "C" {
+
+gcf_status gcf_run_batch(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
+                         const gcf_optics* optics, gcf_result* results)
+{
+    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
+    return batch_run(ctx, items, n, on_device, optics, GCF_SEARCH_PLAIN, results);
+}
+
+gcf_status gcf_run_batch_mode(gcf_ctx* ctx, const gcf_item* items, int n, int on_device,
+                              const gcf_optics* optics, int mode, gcf_result* results)
+{
+    if (mode == GCF_SEARCH_PLAIN) return gcf_run_batch(ctx, items, n, on_device, optics, results);
+    if (!ctx || !items || n <= 0 || !valid_optics(optics) || !results) return GCF_ERR_INVALID_ARG;
+    if (mode != GCF_SEARCH_BF16 && mode != GCF_SEARCH_LEARNED) return GCF_ERR_INVALID_ARG;
+    if (optics->ext_phase_range > 0) {
+        // the table search has no extra-phase dimension: phase-plate data
+        // take the plain search
+        return gcf_run_batch(ctx, items, n, on_device, optics, results);
+    }
+    if (mode == GCF_SEARCH_LEARNED && !ctx->nn_ready)
+        return fail(ctx, GCF_ERR_STATE, "learned search: no network weights (gcf_nn_load / gcf_nn_train)");
+    return batch_run(ctx, items, n, on_device, optics, mode, results);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Autotuner results, one per device for the life of the process.
+struct TuneCache {
+    bool done = false;
+    gcf_tuning t{};
+};
+std::mutex g_tune_mu;
+TuneCache g_tune[64];
+constexpr int kTuneShapes[3] = {8, 816, 16};
+constexpr int kTuneGemm[6][2] = {{256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {64, 4}};
+
+// Best of three timed runs after one warm-up of `run` on ctx->st, in ms.
+template <class F>
+gcf_status time_trial(gcf_ctx* ctx, cudaEvent_t a, cudaEvent_t b, F run, float* ms)
+{
+    *ms = 1e30f;
+    for (int r = 0; r < 4; ++r) {
+        CK(cudaEventRecord(a, ctx->st));
+        CKS(run());
+        CK(cudaEventRecord(b, ctx->st));
+        CK(cudaEventSynchronize(b));
+        float x = 0.0f;
+        CK(cudaEventElapsedTime(&x, a, b));
+        if (r > 0) *ms = std::min(*ms, x);
+    }
+    return GCF_OK;
+}
+
+gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b)
+{
+    // tile kernel: every cluster shape the device can hold, on four
+    // synthetic 4096 x 4096 micrographs
+    if (ctx->impl == GCF_SPECT_FUSED && fused_tile_supported(ctx->tile)) {
+        const int W = 4096, H = 4096, nm = 4;
+        DBuf<float> img;
+        CK(img.ensure((size_t)W * H * nm));
+        launch_fill_f32(img.p, (size_t)W * H * nm, 12345ull, 0.0f, 4.0f, ctx->st);
+        CKL();
+        std::vector<MicImage> mics(nm);
+        for (int i = 0; i < nm; ++i) mics[i] = MicImage{img.p + (size_t)i * W * H, W, H, W, 1.35f};
+        CKS(spectra_alloc(ctx, nm));
+        float best = 1e30f;
+        for (int si = 0; si < 3; ++si) {
+            int ncl = 0;
+            if (fused_clusters_of(kTuneShapes[si], &ncl) != cudaSuccess || ncl <= 0) {
+                cudaGetLastError();
+                t.fused_ms[si] = -1.0f;
+                continue;
+            }
+            ctx->fused_clusters = ncl;
+            ctx->fused_shape = kTuneShapes[si];
+            ctx->solo_n = -1;
+            CKS(fused_plan(ctx, mics));
+            float ms = 0.0f;
+            CKS(time_trial(ctx, a, b, [&] { return fused_launch(ctx, 0, nm, ctx->raw.p, ctx->st); }, &ms));
+            t.fused_ms[si] = ms;
+            if (ms < best) {
+                best = ms;
+                t.fused_shape = kTuneShapes[si];
+            }
+        }
+        CK(cudaStreamSynchronize(ctx->st));
+        img.release();
+    }
+    // contraction product: the table of a 128-micrograph batch (1024
+    // defocus rows x 128 micrographs' angle bins x the s^2 bins)
+    {
+        const int M = 1024, K = ctx->contract_ns, N = 128 * ctx->contract_nth;
+        DBuf<__nv_bfloat16> A, B;
+        DBuf<float> D;
+        DBuf<int> err;
+        CK(A.ensure((size_t)M * K));
+        CK(B.ensure((size_t)N * K));
+        CK(D.ensure((size_t)M * N));
+        CK(err.ensure(1));
+        launch_fill_bf16(A.p, (size_t)M * K, 7ull, ctx->st);
+        launch_fill_bf16(B.p, (size_t)N * K, 8ull, ctx->st);
+        CKL();
+        CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->st));
+        float best = 1e30f;
+        for (int q = 0; q < 6; ++q) {
+            const int bn = kTuneGemm[q][0], stages = kTuneGemm[q][1];
+            if (bn < ctx->contract_nth || bn % ctx->contract_nth) {
+                t.gemm_ms[q] = -1.0f;
+                continue;
+            }
+            GemmArgs g;
+            g.M = M;
+            g.N = N;
+            g.K = K;
+            g.D = D.p;
+            g.ldd = N;
+            g.err = err.p;
+            float ms = 0.0f;
+            CKS(time_trial(ctx, a, b, [&]() -> gcf_status {
+                CK(launch_umma_gemm(A.p, K, B.p, K, g, bn, stages, 0, ctx->st));
+                return GCF_OK;
+            }, &ms));
+            t.gemm_ms[q] = ms;
+            if (ms < best) {
+                best = ms;
+                t.gemm_tile_n = bn;
+                t.gemm_stages = stages;
+            }
+        }
+        int h = 0;
+        CK(cudaMemcpy(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core product trial: a bounded wait gave up");
+    }
+    return GCF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gcf_status gcf_autotune(gcf_ctx* ctx, int force, gcf_tuning* out)
+{
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    if (ctx->dev < 0 || ctx->dev >= 64) return GCF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    TuneCache& C = g_tune[ctx->dev];
+    if (!C.done || force) {
+        gcf_tuning t{};
+        cudaEvent_t a = nullptr, b = nullptr;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        gcf_status st = tune_device(ctx, t, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (st != GCF_OK) return st;
+        C.t = t;
+        C.done = true;
+    }
+    // the picks take effect from the next plan of this context
+    if (C.t.fused_shape) {
+        ctx->fused_shape_req = C.t.fused_shape;
+        ctx->fused_clusters = 0;
+        ctx->solo_n = -1;
+    }
+    if (C.t.gemm_tile_n) {
+        ctx->gemm_bn = C.t.gemm_tile_n;
+        ctx->gemm_stages = C.t.gemm_stages;
+    }
+    if (out) *out = C.t;
+    return GCF_OK;
+}
+
+gcf_status gcf_mrc_load(gcf_ctx* ctx, const char* path, int z0, int n, const float** dev_images)
+{
+    if (!ctx || !path || n <= 0 || z0 < 0 || !dev_images) return GCF_ERR_INVALID_ARG;
+    int dims[3], mode = 0;
+    bool swap = false;
+    long long off = 0;
+    if (!mrc_layout(path, dims, &mode, &swap, &off)) return fail(ctx, GCF_ERR_IO, "cannot read the MRC header");
+    const int mb = mrc_mode_bytes(mode);
+    if (mb == 0) return fail(ctx, GCF_ERR_IO, "MRC mode not supported (0, 1, 2, 5, 6 are)");
+    if ((long long)z0 + n > dims[2]) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    const size_t npx = (size_t)dims[0] * dims[1], sec = npx * mb;
+    const size_t slot = (sec + 255) / 256 * 256;
+    CK(ctx->loaded.ensure(npx * n));
+    CK(ctx->ingest_raw.ensure(2 * slot));
+    if (ctx->ingest_pin_bytes < 2 * slot) {
+        if (ctx->ingest_pin) cudaFreeHost(ctx->ingest_pin);
+        ctx->ingest_pin = nullptr;
+        ctx->ingest_pin_bytes = 0;
+        CK(cudaHostAlloc((void**)&ctx->ingest_pin, 2 * slot, cudaHostAllocDefault));
+        ctx->ingest_pin_bytes = 2 * slot;
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (!ctx->ingest_copied[k]) CK(cudaEventCreateWithFlags(&ctx->ingest_copied[k], cudaEventDisableTiming));
+        if (!ctx->ingest_used[k]) CK(cudaEventCreateWithFlags(&ctx->ingest_used[k], cudaEventDisableTiming));
+    }
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, GCF_ERR_IO, "cannot open the MRC file");
+    gcf_status st = GCF_OK;
+    // section k: wait until its staging pair is free (the copy of section
+    // k - 2 is done on the host side, its conversion on the device side),
+    // read it from disk while the GPU copies and converts section k - 1
+    for (int k = 0; k < n && st == GCF_OK; ++k) {
+        const int b = k & 1;
+        unsigned char* pin = ctx->ingest_pin + b * slot;
+        unsigned char* raw = ctx->ingest_raw.p + b * slot;
+        cudaError_t e = cudaSuccess;
+        if (k >= 2) e = cudaEventSynchronize(ctx->ingest_copied[b]);
+        if (e != cudaSuccess) {
+            st = cuda_fail(ctx, e, "mrc load");
+            break;
+        }
+        if (fseeko(f, (off_t)(off + (long long)(z0 + k) * (long long)sec), SEEK_SET) != 0 ||
+            std::fread(pin, 1, sec, f) != sec) {
+            st = fail(ctx, GCF_ERR_IO, "short MRC section");
+            break;
+        }
+        if ((e = cudaStreamWaitEvent(ctx->st_copy, ctx->ingest_used[b], 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(raw, pin, sec, cudaMemcpyHostToDevice, ctx->st_copy)) != cudaSuccess ||
+            (e = cudaEventRecord(ctx->ingest_copied[b], ctx->st_copy)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(ctx->st, ctx->ingest_copied[b], 0)) != cudaSuccess ||
+            (e = launch_mrc_to_float(raw, mode, swap ? 1 : 0, npx, ctx->loaded.p + (size_t)k * npx, ctx->st)) !=
+                cudaSuccess ||
+            (e = cudaEventRecord(ctx->ingest_used[b], ctx->st)) != cudaSuccess) {
+            st = cuda_fail(ctx, e, "mrc load");
+            break;
+        }
+        dev_images[k] = ctx->loaded.p + (size_t)k * npx;
+    }
+    std::fclose(f);
+    cudaError_t e = cudaStreamSynchronize(ctx->st);
+    if (st == GCF_OK && e != cudaSuccess) st = cuda_fail(ctx, e, "mrc load");
+    return st;
+}
+
+gcf_status gcf_set_graphs(gcf_ctx* ctx, int on)
+{
+    if (!ctx) return GCF_ERR_INVALID_ARG;
+    ctx->graphs = on != 0;
+    return GCF_OK;
+}
+
+gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[3])
+{
+    if (!ctx || !info) return GCF_ERR_INVALID_ARG;
+    info[0] = ctx->graph_launches;
+    info[1] = ctx->bgraph.exec ? ctx->bgraph.nodes : 0;
+    info[2] = ctx->bgraph.exec ? ctx->bgraph.launches : 0;
+    return GCF_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Learned initialiser
 // ---------------------------------------------------------------------------
@@ -2433,6 +2966,7 @@ gcf_status gcf_nn_init(gcf_ctx* ctx, unsigned long long seed)
     CKS(nn_ensure(ctx));
     CK(nn_init_random(ctx->nn, seed, ctx->st));
     ctx->nn_ready = true;
+    ctx->nn_version += 1;
     return GCF_OK;
 }
 
@@ -2443,6 +2977,7 @@ gcf_status gcf_nn_set_params(gcf_ctx* ctx, const float* params, size_t n)
     CKS(nn_ensure(ctx));
     CK(nn_set_params(ctx->nn, params, ctx->st));
     ctx->nn_ready = true;
+    ctx->nn_version += 1;
     return GCF_OK;
 }
 
@@ -2504,6 +3039,7 @@ gcf_status gcf_nn_train(gcf_ctx* ctx, const gcf_optics* optics, int steps, int b
     if (!ctx->nn_ready) {
         CK(nn_init_random(ctx->nn, seed ^ 0x9E3779B97F4A7C15ull, ctx->st));
         ctx->nn_ready = true;
+        ctx->nn_version += 1;
     }
     CK(ctx->nloss.ensure(steps));
     CK(cudaMemsetAsync(ctx->nloss.p, 0, steps * sizeof(float), ctx->st));
@@ -2563,9 +3099,9 @@ gcf_status gcf_nn_forward_backward(gcf_ctx* ctx, const float* x1, const float* x
     CK(ctx->nx2.ensure(h2.size()));
     CK(ctx->ntarget.ensure((size_t)n * 3));
     CK(ctx->nloss.ensure(1));
-    CK(cudaMemcpyAsync(ctx->nx1.p, h1.data(), h1.size() * 2, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->nx2.p, h2.data(), h2.size() * 2, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->ntarget.p, target, (size_t)n * 3 * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(h2d(ctx, ctx->nx1.p, h1.data(), h1.size() * 2, ctx->st));
+    CK(h2d(ctx, ctx->nx2.p, h2.data(), h2.size() * 2, ctx->st));
+    CK(h2d(ctx, ctx->ntarget.p, target, (size_t)n * 3 * 4, ctx->st));
     CK(cudaMemsetAsync(ctx->nloss.p, 0, sizeof(float), ctx->st));
     CK(cudaMemsetAsync(nn_err_flag(ctx->nn), 0, sizeof(int), ctx->st));
     CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, n, ctx->st));

@@ -93,6 +93,7 @@ struct Input {
     float kv = 300.0f, cs = 2.7f, ac = 0.07f, px = 1.0f;
     float ext_phase[2] = {0.0f, 0.0f}, tilt_range[2] = {0.0f, 0.0f};
     int tile = 512, log_spect = 0, gpu = 0, serial = 0;
+    int ctf_res = 0;   // 1: the CTF file gets the spectral-CC resolution column
 
     void parse(int argc, char** argv)
     {
@@ -115,6 +116,7 @@ struct Input {
         a.ints("-LogSpect", &log_spect);
         a.ints("-Serial", &serial);
         a.ints("-Gpu", &gpu);
+        a.ints("-CtfRes", &ctf_res);
     }
     void print() const
     {
@@ -134,6 +136,7 @@ struct Input {
         std::printf("%-15s  %d\n", "-LogSpect", log_spect);
         std::printf("%-15s  %d\n", "-Serial", serial);
         std::printf("%-15s  %d\n", "-Gpu", gpu);
+        if (ctf_res) std::printf("%-15s  %d\n", "-CtfRes", ctf_res);
         std::printf("\n");
     }
 };
@@ -157,7 +160,9 @@ void show_help()
         "-LogSpect     1: background from the spectrum instead of its square root\n"
         "-InSuffix     with -Serial 1, only files whose names end with this suffix\n"
         "-Serial       1: process every matching file in the folder of -InMrc\n"
-        "-Gpu          GPU id (0)\n\n");
+        "-Gpu          GPU id (0)\n"
+        "-CtfRes       1: add the spectral-CC resolution (A) as a last column of the\n"
+        "              CTF file (0: the reference's columns only)\n\n");
 }
 
 // CLoadAngFile::DoIt (CLoadAngFile.cpp:43-71)
@@ -313,6 +318,42 @@ void display(const Package& p, int idx, int done, int total)
                 p.res.azimuth, p.res.ext_phase, p.res.score);
 }
 
+// CSaveCtfResults::SaveCTF + SaveImod (CSaveCtfResults.cpp:34-117): every
+// package in image order; packages not processed yet have zero rows.
+void save_results(const Input& in, const std::vector<Package>& pk, bool tomo)
+{
+    if (in.out_ctf.empty()) return;
+    const int n = (int)pk.size();
+    std::vector<gcf_result> res(n);
+    std::vector<float> tilts(n);
+    std::vector<const char*> names(n);
+    for (int i = 0; i < n; ++i) {
+        res[i] = pk[i].res;
+        tilts[i] = pk[i].tilt;
+        names[i] = pk[i].file.c_str();
+    }
+    if (gcf_write_ctf_file_ex(in.out_ctf.c_str(), res.data(), tilts.data(), names.data(), n, tomo ? 1 : 0,
+                              in.ctf_res ? GCF_CTF_COLUMN_RES : 0) != GCF_OK)
+        std::printf("CTF file: %s\n   cannot be opened, CTF results not saved.\n\n", in.out_ctf.c_str());
+}
+
+// The crash-safety flush of CFindSeriesCtfs::DoIt (CFindSeriesCtfs.cpp:97-101):
+// the result files are rewritten after every 21st package.
+constexpr int kFlushEvery = 21;
+
+struct FlushState {
+    const Input* in;
+    std::vector<Package>* pk;
+    bool tomo;
+};
+
+void on_package(void* user, int done, int image, const gcf_result* r)
+{
+    FlushState* f = static_cast<FlushState*>(user);
+    (*f->pk)[image].res = *r;
+    if (done % kFlushEvery == 0) save_results(*f->in, *f->pk, f->tomo);
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -367,7 +408,10 @@ int main(int argc, char** argv)
     } else {
         for (int i = 0; i < n; ++i) order.push_back(i);
     }
-    for (int i = 0; i < n; ++i) {
+    // a stack goes to the GPU as stored (gcf_mrc_load widens it there);
+    // folders are read on the host, file by file
+    const bool gpu_load = in.serial == 0;
+    for (int i = 0; i < n && !gpu_load; ++i) {
         pk[i].img.resize((size_t)pk[i].w * pk[i].h);
         if (gcf_mrc_read(pk[i].file.c_str(), pk[i].section, pk[i].img.data()) != GCF_OK) {
             std::fprintf(stderr, "Error: cannot read %s (section %d)\n", pk[i].file.c_str(), pk[i].section);
@@ -383,11 +427,22 @@ int main(int argc, char** argv)
     double tp = now_s();
     if (same) {
         std::vector<const float*> ptr(n);
-        for (int i = 0; i < n; ++i) ptr[i] = pk[i].img.data();
+        if (gpu_load) {
+            st = gcf_mrc_load(ctx, in.in_mrc.c_str(), 0, n, ptr.data());
+            if (st != GCF_OK) {
+                std::fprintf(stderr, "Error: cannot load %s: %s\n", in.in_mrc.c_str(), gcf_last_error(ctx));
+                gcf_destroy(ctx);
+                return 1;
+            }
+        } else {
+            for (int i = 0; i < n; ++i) ptr[i] = pk[i].img.data();
+        }
         std::vector<gcf_result> res(n);
         std::vector<float> full(want_full ? (size_t)n * T * T : 0);
-        st = gcf_run_series(ctx, ptr.data(), n, pk[0].w, pk[0].h, 0, &op, order.data(), tomo ? 1 : 0,
-                            res.data(), want_full ? full.data() : nullptr);
+        FlushState fs{&in, &pk, tomo};
+        gcf_set_package_callback(ctx, on_package, &fs);
+        st = gcf_run_series(ctx, ptr.data(), n, pk[0].w, pk[0].h, gpu_load ? 1 : 0, &op, order.data(),
+                            tomo ? 1 : 0, res.data(), want_full ? full.data() : nullptr);
         if (st != GCF_OK) {
             std::fprintf(stderr, "Error: %s: %s\n", gcf_strerror(st), gcf_last_error(ctx));
             gcf_destroy(ctx);
@@ -450,6 +505,7 @@ int main(int argc, char** argv)
                     ref = order[k];
                 }
                 display(p, order[k], k, n);
+                if ((k + 1) % kFlushEvery == 0) save_results(in, pk, tomo);
                 if (want_full) {
                     float* f = find.GenFullSpectrum();
                     p.full.assign(f, f + (size_t)T * T);
@@ -478,19 +534,7 @@ int main(int argc, char** argv)
             }
         }
     }
-    if (!in.out_ctf.empty()) {
-        std::vector<gcf_result> res(n);
-        std::vector<float> tilts(n);
-        std::vector<const char*> names(n);
-        for (int i = 0; i < n; ++i) {
-            res[i] = pk[i].res;
-            tilts[i] = pk[i].tilt;
-            names[i] = pk[i].file.c_str();
-        }
-        if (gcf_write_ctf_file(in.out_ctf.c_str(), res.data(), tilts.data(), names.data(), n, tomo ? 1 : 0) != GCF_OK) {
-            std::printf("CTF file: %s\n   cannot be opened, CTF results not saved.\n\n", in.out_ctf.c_str());
-        }
-    }
+    save_results(in, pk, tomo);
     if (ctx) gcf_destroy(ctx);
     std::printf("Total time:  %.3f (s)\n\n", now_s() - t0);
     return 0;

@@ -157,7 +157,40 @@ __global__ void k_job_rows(const SearchJob* __restrict__ jobs, int njobs, const 
     rows[j] = make_int2(lo, max(hi, lo));
 }
 
+// Seeded uniform fill (SplitMix64 finaliser of the element index): trial
+// operands of the autotuner.
+__device__ __forceinline__ float hash_uniform(unsigned long long seed, size_t i)
+{
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (float)(z >> 40) * (1.0f / 16777216.0f);
+}
+
+__global__ void k_fill_f32(float* __restrict__ p, size_t n, unsigned long long seed, float lo, float hi)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = lo + (hi - lo) * hash_uniform(seed, i);
+}
+
+__global__ void k_fill_bf16(__nv_bfloat16* __restrict__ p, size_t n, unsigned long long seed)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = __float2bfloat16_rn(2.0f * hash_uniform(seed, i) - 1.0f);
+}
+
 }  // namespace
+
+void launch_fill_f32(float* p, size_t n, unsigned long long seed, float lo, float hi, cudaStream_t st)
+{
+    if (n) k_fill_f32<<<1184, 256, 0, st>>>(p, n, seed, lo, hi);
+}
+
+void launch_fill_bf16(__nv_bfloat16* p, size_t n, unsigned long long seed, cudaStream_t st)
+{
+    if (n) k_fill_bf16<<<1184, 256, 0, st>>>(p, n, seed);
+}
 
 void launch_polar_model(const PolarGrid& g, __nv_bfloat16* A, __nv_bfloat16* A2, cudaStream_t st)
 {

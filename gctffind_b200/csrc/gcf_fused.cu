@@ -753,7 +753,7 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(next_item, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
-    if (ev0 && (e = cudaEventRecord(ev0, st)) != cudaSuccess) return e;
+    if (ev0 && (e = record_timing(ev0, st)) != cudaSuccess) return e;
     const bool use_solo = solo && solo->n > 0 && nitems > nclusters;
     if (use_solo) {
         if ((e = cudaEventRecord(solo->fork, st)) != cudaSuccess) return e;
@@ -787,7 +787,7 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
         if ((e = cudaEventRecord(solo->join, solo->st)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(st, solo->join, 0)) != cudaSuccess) return e;
     }
-    if (ev1 && (e = cudaEventRecord(ev1, st)) != cudaSuccess) return e;
+    if (ev1 && (e = record_timing(ev1, st)) != cudaSuccess) return e;
     dim3 g((FCX * FT + 255) / 256, nimg);
     k_item_reduce<<<g, 256, 0, st>>>(partial, first + img0, inv + img0, raw);
     return cudaGetLastError();

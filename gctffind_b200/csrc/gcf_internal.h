@@ -20,6 +20,23 @@
 
 namespace gcf {
 
+// Device-allocation epoch: every (re)allocation of a context buffer bumps
+// it, so a captured CUDA graph (which holds raw device addresses) is only
+// replayed while the epoch it was captured in is current.
+void note_device_alloc();
+unsigned long long device_alloc_epoch();
+// Records a timing event on st; inside a stream capture it becomes an event
+// node of the graph (recorded again on every replay).
+cudaError_t record_timing(cudaEvent_t ev, cudaStream_t st);
+
+// gcf_mrc.cpp: section layout of an MRC file (false if unreadable) and the
+// bytes per pixel of a mode (0 if unsupported).
+bool mrc_layout(const char* path, int dims[3], int* mode, bool* swap, long long* data_off);
+int mrc_mode_bytes(int mode);
+// gcf_ingest.cu: raw MRC section bytes (mode 0/5 unsigned char, 1 short,
+// 6 unsigned short, 2 float; `swap`: big-endian file) to float.
+cudaError_t launch_mrc_to_float(const void* raw, int mode, int swap, size_t npx, float* out, cudaStream_t st);
+
 constexpr int kMaxCand = 2624;        // >= 51 * 51 astigmatism grid
 constexpr int kEvalThreads = 256;     // threads of the candidate kernel
 constexpr int kEvalPPT = 6;           // band pixels per thread per chunk
@@ -285,6 +302,9 @@ struct TableArgs {
     float2* cval;
 };
 void launch_table_search(const TableArgs& a, cudaStream_t st);
+// Seeded uniform fills (autotuner trial operands): floats in [lo, hi), BF16 in [-1, 1).
+void launch_fill_f32(float* p, size_t n, unsigned long long seed, float lo, float hi, cudaStream_t st);
+void launch_fill_bf16(__nv_bfloat16* p, size_t n, unsigned long long seed, cudaStream_t st);
 
 // gcf_nn.cu: the learned initialiser's kernels (see the file for the network).
 constexpr int kNnProfile = 256;            // x1 bins

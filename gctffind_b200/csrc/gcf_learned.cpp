@@ -34,6 +34,7 @@ struct Buf {
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
+        note_device_alloc();
         cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(cnt, 1) * sizeof(T));
         if (e == cudaSuccess) n = cnt;
         return e;

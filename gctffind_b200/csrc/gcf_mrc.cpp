@@ -93,6 +93,31 @@ int mode_bytes(int mode)
 
 }  // namespace
 
+namespace gcf {
+
+// Section layout of an MRC file: dims, mode, byte order and the offset of
+// section 0 (after the 1024-byte header and the extended header).
+bool mrc_layout(const char* path, int dims[3], int* mode, bool* swap, long long* data_off)
+{
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    Header h;
+    bool ok = read_header(f, h);
+    std::fclose(f);
+    if (!ok) return false;
+    dims[0] = h.nx;
+    dims[1] = h.ny;
+    dims[2] = h.nz;
+    *mode = h.mode;
+    *swap = h.swap;
+    *data_off = 1024LL + h.nsymbt;
+    return true;
+}
+
+int mrc_mode_bytes(int mode) { return mode_bytes(mode); }
+
+}  // namespace gcf
+
 extern "C" {
 
 gcf_status gcf_mrc_info(const char* path, int dims[3], int* mode, float* pixel_size,

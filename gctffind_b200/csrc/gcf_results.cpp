@@ -10,19 +10,25 @@
 
 extern "C" {
 
-gcf_status gcf_write_ctf_file(const char* path, const gcf_result* res, const float* tilts,
-                              const char* const* names, int n, int is_tomo)
+gcf_status gcf_write_ctf_file_ex(const char* path, const gcf_result* res, const float* tilts,
+                                 const char* const* names, int n, int is_tomo, int flags)
 {
-    if (!path || !res || n <= 0) return GCF_ERR_INVALID_ARG;
+    if (!path || !res || n <= 0 || (flags & ~GCF_CTF_COLUMN_RES)) return GCF_ERR_INVALID_ARG;
+    const bool col_res = (flags & GCF_CTF_COLUMN_RES) != 0;
     FILE* f = std::fopen(path, "w");
     if (!f) return GCF_ERR_IO;
-    // SaveCTF (CSaveCtfResults.cpp:34-66): 0-based image index
-    std::fprintf(f, "# Idx   tilt     dfMin      dfMax   azimuth extPhase  score    fileName\n");
+    // SaveCTF (CSaveCtfResults.cpp:34-66): 0-based image index; the opt-in
+    // resolution column goes after the file name, so the reference's columns
+    // keep their positions
+    std::fprintf(f, col_res ? "# Idx   tilt     dfMin      dfMax   azimuth extPhase  score    fileName  ctfRes\n"
+                            : "# Idx   tilt     dfMin      dfMax   azimuth extPhase  score    fileName\n");
     for (int i = 0; i < n; ++i) {
         float tilt = tilts ? tilts[i] : 0.0f;
         const char* nm = (names && names[i]) ? names[i] : "";
-        std::fprintf(f, "%4d  %6.2f %10.2f %10.2f %7.2f %7.2f %8.4f  %s\n", i, tilt, res[i].df_min,
+        std::fprintf(f, "%4d  %6.2f %10.2f %10.2f %7.2f %7.2f %8.4f  %s", i, tilt, res[i].df_min,
                      res[i].df_max, res[i].azimuth, res[i].ext_phase, res[i].score, nm);
+        if (col_res) std::fprintf(f, "  %7.2f", res[i].ctf_res);
+        std::fputc('\n', f);
     }
     bool ok = std::fclose(f) == 0;
     if (!ok) return GCF_ERR_IO;
@@ -47,6 +53,12 @@ gcf_status gcf_write_ctf_file(const char* path, const gcf_result* res, const flo
                          res[i].ext_phase);
     }
     return std::fclose(f) == 0 ? GCF_OK : GCF_ERR_IO;
+}
+
+gcf_status gcf_write_ctf_file(const char* path, const gcf_result* res, const float* tilts,
+                              const char* const* names, int n, int is_tomo)
+{
+    return gcf_write_ctf_file_ex(path, res, tilts, names, n, is_tomo, 0);
 }
 
 }  // extern "C"

@@ -226,6 +226,15 @@ gcf_status gcf_run_series(gcf_ctx* ctx, const float* const* images, int n, int w
                           const int* order, int is_tomo, gcf_result* results,
                           float* full_spectra);
 
+/* Called on the calling host thread during gcf_run_series each time one
+ * more package's result is final, in processing order: `done` packages are
+ * final so far, the last being image `image` with `result`.  This is the
+ * hook of the reference's crash-safety flush, which rewrites the CTF and
+ * Imod files after every 21st package (CFindSeriesCtfs.cpp:97-101).  The
+ * callback must not call into this context.  fn = NULL removes it. */
+typedef void (*gcf_package_fn)(void* user, int done, int image, const gcf_result* result);
+gcf_status gcf_set_package_callback(gcf_ctx* ctx, gcf_package_fn fn, void* user);
+
 /* Independent full searches (CFindCtf2D::Do2D per image, the single-file
  * mode of CInputFolder::mReadSingle, CInputFolder.cpp:159-192) of n images
  * of possibly different sizes and pixel sizes, batched on the GPU. */
@@ -277,6 +286,37 @@ gcf_status gcf_nn_get_params(gcf_ctx* ctx, float* params, size_t n);
 /* Weights file: 8-byte tag "GCFNN001", the count (uint64), FP32 params. */
 gcf_status gcf_nn_save(gcf_ctx* ctx, const char* path);
 gcf_status gcf_nn_load(gcf_ctx* ctx, const char* path);
+/* CUDA graphs for batch calls (gcf_run_batch, gcf_run_batch_mode), off by
+ * default.  With graphs on, a call that repeats an earlier call's inputs
+ * (the same image buffers, sizes, pixel sizes, optics and method; device
+ * images, or host images in page-locked memory) is captured once and then
+ * replayed as a single graph launch: rescale, spectra, post-processing and
+ * the search kernels, and the small uploads they read.  The image contents
+ * may change between calls; the results are those of an eager call.  No
+ * counterpart in the reference, whose package loop launches every kernel
+ * from the host (CFindSeriesCtfs.cpp:50-213). */
+gcf_status gcf_set_graphs(gcf_ctx* ctx, int on);
+/* Project autotuner.  Times, on this context's GPU, every cluster shape of
+ * the fused tile kernel that the device can hold (four synthetic 4096 x 4096
+ * micrographs) and the (tile N, pipeline depth) pairs of the contraction's
+ * tensor-core product (a 1024 x 8192 x 512 table), and makes the fastest of
+ * each this context's choice.  The trials run once per device and process;
+ * later calls (and other contexts) reuse them unless `force`.  Results do
+ * not depend on the choice, only speed.  No counterpart in the reference,
+ * whose kernels have fixed launch shapes. */
+typedef struct {
+    int fused_shape;     /* tile-kernel cluster shape picked: 8, 816 or 16 */
+    int gemm_tile_n;     /* contraction product tile picked: 128 x gemm_tile_n */
+    int gemm_stages;     /* its load-pipeline depth */
+    float fused_ms[3];   /* trial ms of shapes 8, 816, 16 (-1: cannot be resident) */
+    float gemm_ms[6];    /* trial ms of (256,2) (256,3) (256,4) (128,4) (128,6) (64,4) */
+} gcf_tuning;
+gcf_status gcf_autotune(gcf_ctx* ctx, int force, gcf_tuning* out);
+
+/* [0] graph launches of the last batch call (0: it ran eagerly), [1] nodes
+ * of the cached graph, [2] kernels of this library captured in it. */
+gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[3]);
+
 /* Refined CC below which a learned search falls back to the full search
  * (default 0.1); a result at the edge of its window always falls back. */
 gcf_status gcf_set_learned_threshold(gcf_ctx* ctx, float tau);
@@ -319,6 +359,16 @@ gcf_status gcf_mrc_info(const char* path, int dims[3], int* mode, float* pixel_s
 gcf_status gcf_mrc_read(const char* path, int z, float* out);
 /* Tilt angle of each of the first n sections from the extended header. */
 gcf_status gcf_mrc_read_tilts(const char* path, float* tilts, int n);
+/* Sections z0 .. z0+n-1 of an MRC file (modes 0, 1, 2, 5, 6) as float
+ * images in device memory owned by the context (CLoadImages::mLoadPackage +
+ * mToFloat, MrcUtil/CLoadImages.cpp:108-181).  The section bytes cross PCIe
+ * as stored (1, 2 or 4 bytes per pixel) through two pinned staging buffers
+ * -- the next section is read from disk while the GPU copies and widens the
+ * previous one -- and a kernel converts them to float.  dev_images[k]
+ * receives section z0+k's device address (dense nx x ny floats), valid
+ * until the next gcf_mrc_load on this context or gcf_destroy; pass them to
+ * gcf_run_series / gcf_run_batch with images_are_device = 1. */
+gcf_status gcf_mrc_load(gcf_ctx* ctx, const char* path, int z0, int n, const float** dev_images);
 /* float32 (mode 2) stack of nz sections. */
 gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, int nz,
                          float pixel_size);
@@ -332,6 +382,14 @@ gcf_status gcf_mrc_write(const char* path, const float* data, int nx, int ny, in
  * nm.  tilts and names may be NULL (0 and "" then). */
 gcf_status gcf_write_ctf_file(const char* path, const gcf_result* results, const float* tilts,
                               const char* const* names, int n, int is_tomo);
+/* gcf_write_ctf_file with output options.  GCF_CTF_COLUMN_RES adds the
+ * spectral-CC resolution (gcf_result.ctf_res, Angstrom) as a last
+ * "ctfRes" column of the CTF file; the reference computes it
+ * (FindCTF/CFindDefocus2D.cpp:382-400) but writes no such column, so the
+ * default (flags = 0) output is the reference's, byte for byte. */
+enum { GCF_CTF_COLUMN_RES = 1 };
+gcf_status gcf_write_ctf_file_ex(const char* path, const gcf_result* results, const float* tilts,
+                                 const char* const* names, int n, int is_tomo, int flags);
 
 /* ---------------------------------------------------------------------- */
 /* Tensor-core building block.  No counterpart in the reference (its        */

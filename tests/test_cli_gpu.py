@@ -61,6 +61,42 @@ def test_cli_tilt_series(gpu_lib, tmp_path):
     assert os.path.exists(str(tmp_path / "ts_ctf_Imod.txt"))
 
 
+def test_cli_flushes_every_21_packages_and_resolution_column(gpu_lib, tmp_path):
+    """A 23-tilt stack: the package hook of gcf_run_series reports every
+    package once, in processing order, with the call's own results; the
+    CLI's flush after the 21st package (CFindSeriesCtfs.cpp:97-101) and its
+    final write leave the complete file; -CtfRes 1 adds the resolution
+    column after the reference's columns."""
+    tilts = [3.0 * (k - 11) for k in range(23)]
+    imgs = np.stack([_img(512, 512, 1.35, (14000.0, 14300.0), 10.0, 600 + k, tilt=t)
+                     for k, t in enumerate(tilts)])
+    ctx = G.Context(0, 256, 0)
+    so = G.series_order(tilts)
+    seen = []
+    lib = ctx.run_series(list(imgs), G.make_optics(pixel_size=1.35), so.order, is_tomo=True,
+                         on_package=lambda done, image, r: seen.append((done, image, r.as_dict())))
+    assert [d for d, _, _ in seen] == list(range(1, 24))
+    assert [i for _, i, _ in seen] == list(so.order)
+    for _, i, r in seen:
+        assert r == lib[i].as_dict()
+    # the hook is removed after the call
+    again = ctx.run_series(list(imgs), G.make_optics(pixel_size=1.35), so.order, is_tomo=True)
+    assert [r.as_dict() for r in again] == [r.as_dict() for r in lib]
+    ctx.close()
+    stack = str(tmp_path / "ts23.mrc")
+    G.mrc_write(stack, imgs, 1.35)
+    out_ctf = str(tmp_path / "ts23_ctf.txt")
+    _run("-InMrc", stack, "-OutCtf", out_ctf, "-PixSize", "1.35", "-TileSize", "256",
+         "-TiltRange", "-33", "33", "-CtfRes", "1")
+    lines = open(out_ctf).read().splitlines()
+    assert lines[0].endswith("fileName  ctfRes") and len(lines) == 24
+    for line, l in zip(lines[1:], lib):
+        f = line.split()
+        assert len(f) == 9
+        assert float(f[2]) == pytest.approx(round(l.df_min, 2), abs=0.006)
+        assert float(f[8]) == pytest.approx(round(l.ctf_res, 2), abs=0.006)
+
+
 def test_cli_single_micrograph(gpu_lib, tmp_path):
     img = _img(1024, 1024, 1.0, (22000.0, 22600.0), -30.0, 510)
     path = str(tmp_path / "mic.mrc")

@@ -72,3 +72,36 @@ def test_learned_search_needs_weights(gpu_lib):
     with pytest.raises(G.GcfError):
         ctx.run_batch([img], [1.35], G.make_optics(), mode=G.GCF_SEARCH_LEARNED)
     ctx.close()
+
+
+def test_trained_network_gain_on_held_out_spectra(gpu_lib):
+    """The trained weights shipped with the package (written by
+    `python -m gctffind_b200.train_init`) on 1024 held-out synthetic spectra
+    (a generator seed never trained on), each searched three ways: the plain
+    FP32 exhaustive search, the BF16 contraction search without the network
+    and the learned window search.  Bar: the learned search lands within one
+    search step of the plain one for >= 99 % of the spectra with a median
+    |d defocus| <= 20 A, falls back to the full search for at most 5 %, and
+    scores fewer than half the table candidates of the search without the
+    network -- what the network gains."""
+    from gctffind_b200 import train_init as TI
+    G = gpu_lib
+    assert G.learned_available(), "trained weights missing: run python -m gctffind_b200.train_init"
+    ctx = G.Context(0, 512, 0)
+    op = G.make_optics()
+    G.load_learned(ctx)
+    n = 1024
+    plain, prm = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_PLAIN)
+    bf16, _ = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_BF16)
+    cb = ctx.fast_counts()
+    learned, _ = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_LEARNED)
+    cl = ctx.fast_counts()
+    ctx.close()
+    med_b, frac_b, _ = TI.compare(bf16, plain)
+    med_l, frac_l, _ = TI.compare(learned, plain)
+    assert frac_b >= 0.99 and med_b <= 20.0, (frac_b, med_b)
+    assert frac_l >= 0.99 and med_l <= 20.0, (frac_l, med_l)
+    assert cl["fallbacks"] <= 0.05 * n, cl
+    assert cl["table_cand"] < 0.5 * cb["table_cand"], (cl, cb)
+    # both stay as close to the generator's truth as the plain search
+    assert TI.truth_error(learned, prm) <= TI.truth_error(plain, prm) + 20.0

@@ -144,6 +144,25 @@ def test_ctf_file_format_matches_csavectfresults(tmp_path):
     assert not os.path.exists(str(tmp_path / "one_Imod.txt"))
 
 
+def test_ctf_file_resolution_column_is_opt_in(tmp_path):
+    """gcf_write_ctf_file_ex: flags 0 writes the reference's file byte for
+    byte; GCF_CTF_COLUMN_RES appends the spectral-CC resolution after the
+    file name, so the reference's columns keep their positions."""
+    rs = [_res(29700.12, 30301.5, -38.89, 0.0, 0.84431), _res(29000.0, 29500.25, 12.5, 0.0, 0.5)]
+    rs[0].ctf_res, rs[1].ctf_res = 4.21, 11.5
+    a, b = str(tmp_path / "a.txt"), str(tmp_path / "b.txt")
+    G.write_ctf_file(a, rs, tilts=[0.0, -3.0], names=["ts.mrc", "ts.mrc"], is_tomo=True)
+    G.write_ctf_file(b, rs, tilts=[0.0, -3.0], names=["ts.mrc", "ts.mrc"], is_tomo=True, ctf_res=True)
+    la, lb = open(a).read().splitlines(), open(b).read().splitlines()
+    assert lb[0] == la[0] + "  ctfRes"
+    assert lb[1] == la[1] + "     4.21"
+    assert lb[2] == la[2] + "    11.50"
+    # the Imod file does not change
+    assert open(str(tmp_path / "a_Imod.txt")).read() == open(str(tmp_path / "b_Imod.txt")).read()
+    L = G.load_library()
+    assert L.gcf_write_ctf_file_ex(b.encode(), (G.Result * 1)(rs[0]), None, None, 1, 0, 2) == 1
+
+
 def test_series_order_zero_tilt_first():
     # CInputFolder::FindZeroTilt + CLoadImages::mReadTomo
     so = G.series_order([-6, -3, 0.0, 3, 6])
