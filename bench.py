@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--mode", default="auto", choices=["auto", "bf16", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel from the host")
+    ap.add_argument("--no-autotune", action="store_true", help="default shapes instead of the autotuner's")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the tilt-series and 1.0 A/px single-micrograph figures")
     ap.add_argument("--shrink", type=int, default=1,
@@ -447,7 +448,7 @@ def main():
     op = G.make_optics()
     # the project's autotuner picks the tile-kernel shape and the contraction
     # tile; repeated batch calls run as captured CUDA graphs
-    tuning = ctx.autotune()
+    tuning = None if args.no_autotune else ctx.autotune()
     ctx.set_graphs(not args.no_graphs)
     specs, imgs = make_batch(rank, args.batch, f"cuda:{local}", args.shrink)
     pxs = [s.pixel_size for s in specs]

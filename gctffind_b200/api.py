@@ -86,12 +86,12 @@ class CtfParam(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("fused_shape", C.c_int), ("gemm_tile_n", C.c_int), ("gemm_stages", C.c_int),
-                ("fused_ms", C.c_float * 3), ("gemm_ms", C.c_float * 6)]
+                ("fused_ms", C.c_float * 4), ("gemm_ms", C.c_float * 6)]
 
     def as_dict(self):
         return {"fused_shape": self.fused_shape, "gemm_tile_n": self.gemm_tile_n,
                 "gemm_stages": self.gemm_stages,
-                "fused_ms": dict(zip(["8", "816", "16"], [round(x, 4) for x in self.fused_ms])),
+                "fused_ms": dict(zip(["8", "816", "16", "162"], [round(x, 4) for x in self.fused_ms])),
                 "gemm_ms": dict(zip(["256x2", "256x3", "256x4", "128x4", "128x6", "64x4"],
                                     [round(x, 4) for x in self.gemm_ms]))}
 
@@ -434,9 +434,11 @@ class Context:
     def graph_info(self):
         """(graph launches of the last batch call, nodes and library kernels
         of the cached graph) -- gcf_get_graph_info."""
-        c = (C.c_longlong * 3)()
+        c = (C.c_longlong * 4)()
         _check(self.L.gcf_get_graph_info(self._h, c), self._h)
-        return dict(zip(["graph_launches", "nodes", "kernels"], list(c)))
+        d = dict(zip(["graph_launches", "nodes", "kernels", "capture_fail"], list(c)))
+        d["detail"] = self.L.gcf_last_error(self._h).decode()
+        return d
 
     def fast_counts(self):
         """Contraction work of the last batched call (gcf_get_fast_counts)."""

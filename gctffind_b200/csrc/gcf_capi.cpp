@@ -96,11 +96,31 @@ struct HostArena {
         for (Block& b : blocks) b.used = 0;
         cur = 0;
     }
+    bool frozen = false;   // no new blocks (inside a stream capture)
+    size_t used_bytes() const
+    {
+        size_t u = 0;
+        for (const Block& b : blocks) u += b.used;
+        return u;
+    }
+    // One free block of at least `bytes` (blocks allocated now, not during a
+    // capture, where a page-locked allocation would end the capture).
+    bool reserve(size_t bytes)
+    {
+        for (const Block& b : blocks)
+            if (b.cap >= bytes) return true;
+        release();
+        Block b{nullptr, std::max<size_t>(bytes, (size_t)1 << 20), 0};
+        if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) return false;
+        blocks.push_back(b);
+        return true;
+    }
     void* put(const void* src, size_t bytes)
     {
         const size_t need = (bytes + 255) & ~(size_t)255;
         while (cur < blocks.size() && blocks[cur].cap - blocks[cur].used < need) ++cur;
         if (cur == blocks.size()) {
+            if (frozen) return nullptr;
             Block b{nullptr, std::max<size_t>(need, (size_t)1 << 20), 0};
             if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
             blocks.push_back(b);
@@ -279,6 +299,7 @@ struct gcf_ctx {
     BatchGraph bgraph;
     cudaEvent_t fork_ev = nullptr;    // dependency-only fork of st_copy from st
     long long graph_launches = 0;     // graph launches of the last batch call
+    int graph_fail = 0;               // why the last capture gave no graph (0: it did)
 };
 
 namespace {
@@ -1520,6 +1541,10 @@ gcf_status stage_image(gcf_ctx* ctx, const float* dimg, int w, int h, float px, 
     return GCF_OK;
 }
 
+// Images packed in one staging buffer start on 256-byte boundaries (cuFFT
+// and the vector loads of the tile kernels want aligned rows).
+size_t align_floats(size_t n) { return (n + 63) / 64 * 64; }
+
 // Uploads (host inputs), rescales and produces the spectra of n images.
 // Host inputs are uploaded in chunks on a copy stream so that the upload of
 // chunk c+1 overlaps the rescale and spectrum of chunk c.
@@ -1532,9 +1557,9 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
         int nw, nh;
         float pn;
         gcf_rescale_dims(ws[i], hs[i], pxs[i], &nw, &nh, &pn);
-        tot_raw += (size_t)ws[i] * hs[i];
+        tot_raw += align_floats((size_t)ws[i] * hs[i]);
         float bin = 1.2f / pxs[i];
-        if (bin > 1) tot_new += (size_t)nw * nh;
+        if (bin > 1) tot_new += align_floats((size_t)nw * nh);
     }
     CKS(spectra_alloc(ctx, n));
     if (tot_new) CK(ctx->rescaled.ensure(tot_new));
@@ -1563,7 +1588,7 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
                 CK(cudaMemcpyAsync(ctx->images.p + roff, images[i], cnt * sizeof(float),
                                    cudaMemcpyHostToDevice, ctx->st_copy));
                 dimg[i - i0] = ctx->images.p + roff;
-                roff += cnt;
+                roff += align_floats(cnt);
             }
             // the timing record first: in a capture, the chunk event joins
             // everything on the copy stream back into st
@@ -1578,7 +1603,7 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
             size_t used = 0;
             float* dst = tot_new ? ctx->rescaled.p + roff_new : nullptr;
             CKS(stage_image(ctx, dimg[i - i0], ws[i], hs[i], pxs[i], dst, mics[i], &used));
-            roff_new += used;
+            roff_new += align_floats(used);
         }
         CKS(spectra_chunk(ctx, mics, i0, i1 - i0));
     }
@@ -1889,7 +1914,7 @@ gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int w, int h, float px, i
 
 gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape)
 {
-    if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16)) return GCF_ERR_INVALID_ARG;
+    if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16 && shape != 162)) return GCF_ERR_INVALID_ARG;
     ctx->fused_shape_req = shape;
     ctx->fused_clusters = 0;   // recomputed at the next launch
     ctx->solo_n = -1;
@@ -2565,33 +2590,54 @@ bool batch_capture(gcf_ctx* ctx, unsigned long long key, const std::vector<const
                    int on_device, const gcf_optics& op, int mode)
 {
     BatchGraph& G = ctx->bgraph;
+    // the graph's arena holds all of the call's uploads in one block, sized
+    // from the eager call before (with room to spare)
+    if (!G.arena.reserve(2 * ctx->arena.used_bytes() + ((size_t)1 << 20))) {
+        ctx->graph_fail = 1;
+        return false;
+    }
     G.arena.reset();
+    G.arena.frozen = true;
     std::swap(ctx->arena, G.arena);   // this capture's uploads go to the graph's arena
     const unsigned long long ep0 = device_alloc_epoch();
     const unsigned long long mv0 = ctx->model_version;
-    const long long launches0 = ctx->launches;
+    ctx->kev_used = 0;   // only this attempt's timing events and launches count
+    ctx->launches = 0;
+    const long long launches0 = 0;
     SearchPending pend;
     std::vector<float> pxn;
     cudaGraph_t g = nullptr;
     gcf_status st = GCF_ERR_CUDA;
-    if (cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+    ctx->graph_fail = 2;
+    cudaError_t ce = cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeRelaxed);
+    if (ce == cudaSuccess) {
         ctx->capturing = true;
         t_capturing = true;
         st = batch_enqueue(ctx, imgs, ws, hs, pxs, on_device, op, mode, pend, pxn);
         ctx->capturing = false;
         t_capturing = false;
-        if (cudaStreamEndCapture(ctx->st, &g) != cudaSuccess) g = nullptr;
+        ce = cudaStreamEndCapture(ctx->st, &g);
+        if (ce != cudaSuccess) g = nullptr;
+        ctx->graph_fail = st != GCF_OK ? 3 : (!g ? 4 : 0);
     }
+    if (ctx->graph_fail && ce != cudaSuccess) ctx->err = std::string("graph capture: ") + cudaGetErrorString(ce);
     std::swap(ctx->arena, G.arena);
+    G.arena.frozen = false;
     cudaGetLastError();
     bool ok = st == GCF_OK && g && device_alloc_epoch() == ep0;
+    if (!ctx->graph_fail && !ok) ctx->graph_fail = 5;
     if (ok) {
         cudaGraphExecUpdateResultInfo info;
         if (!(G.exec && cudaGraphExecUpdate(G.exec, g, &info) == cudaSuccess)) {
             cudaGetLastError();
             if (G.exec) cudaGraphExecDestroy(G.exec);
             G.exec = nullptr;
-            ok = cudaGraphInstantiate(&G.exec, g, 0) == cudaSuccess;
+            ce = cudaGraphInstantiate(&G.exec, g, 0);
+            ok = ce == cudaSuccess;
+            if (!ok) {
+                ctx->graph_fail = 6;
+                ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
+            }
         }
     }
     if (ok) {
@@ -2651,8 +2697,15 @@ gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, 
     const unsigned long long key = graphable ? batch_key(ctx, items, n, on_device, *optics, mode) : 0;
     bool replay = graphable && G.exec && G.key == key && G.epoch == device_alloc_epoch() &&
                   G.model_version == ctx->model_version;
-    if (!replay && graphable && G.key == key && G.seen >= 1)
-        replay = batch_capture(ctx, key, imgs, ws, hs, pxs, on_device, *optics, mode);
+    if (!replay && graphable && G.key == key && G.seen >= 1) {
+        // a second attempt within the call: a library may initialise
+        // something on the first captured use of an object
+        for (int attempt = 0; attempt < 2 && !replay; ++attempt) {
+            G.key = key;
+            G.seen = 1;
+            replay = batch_capture(ctx, key, imgs, ws, hs, pxs, on_device, *optics, mode);
+        }
+    }
     SearchPending pend;
     std::vector<float> pxn;
     gcf_status st = GCF_OK;
@@ -2732,7 +2785,7 @@ struct TuneCache {
 };
 std::mutex g_tune_mu;
 TuneCache g_tune[64];
-constexpr int kTuneShapes[3] = {8, 816, 16};
+constexpr int kTuneShapes[4] = {8, 816, 16, 162};
 constexpr int kTuneGemm[6][2] = {{256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {64, 4}};
 
 // Best of three timed runs after one warm-up of `run` on ctx->st, in ms.
@@ -2766,7 +2819,7 @@ gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b
         for (int i = 0; i < nm; ++i) mics[i] = MicImage{img.p + (size_t)i * W * H, W, H, W, 1.35f};
         CKS(spectra_alloc(ctx, nm));
         float best = 1e30f;
-        for (int si = 0; si < 3; ++si) {
+        for (int si = 0; si < 4; ++si) {
             int ncl = 0;
             if (fused_clusters_of(kTuneShapes[si], &ncl) != cudaSuccess || ncl <= 0) {
                 cudaGetLastError();
@@ -2945,12 +2998,13 @@ gcf_status gcf_set_graphs(gcf_ctx* ctx, int on)
     return GCF_OK;
 }
 
-gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[3])
+gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[4])
 {
     if (!ctx || !info) return GCF_ERR_INVALID_ARG;
     info[0] = ctx->graph_launches;
     info[1] = ctx->bgraph.exec ? ctx->bgraph.nodes : 0;
     info[2] = ctx->bgraph.exec ? ctx->bgraph.launches : 0;
+    info[3] = ctx->graph_fail;
     return GCF_OK;
 }
 

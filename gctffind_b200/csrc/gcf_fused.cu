@@ -254,12 +254,13 @@ __device__ __forceinline__ int take_back(unsigned long long* q, int nitems, int 
 }
 
 // Compile-time shape of one cluster configuration.
-template <int CL_, int NW_, bool DB_, bool PF_ = true>
+template <int CL_, int NW_, bool DB_, bool PF_ = true, int MINB_ = 1>
 struct FusedShape {
     static constexpr int CL = CL_;                   // CTAs per cluster
     static constexpr int NW = NW_;                   // warps per CTA
     static constexpr bool DB = DB_;                  // double-buffered column buffer
     static constexpr bool PF = PF_;                  // register prefetch of the next row pair
+    static constexpr int MINB = MINB_;               // CTAs per SM the registers are sized for
     static constexpr int THR = NW * 32;
     static constexpr int R = FT / CL;                // tile rows per CTA
     static constexpr int C = FT / 2 / CL;            // frequency columns per CTA
@@ -276,9 +277,13 @@ struct FusedShape {
 using Shape16 = FusedShape<16, 16, true>;         // 16-CTA clusters, 512 threads
 using Shape8 = FusedShape<8, 8, false>;           // 8-CTA clusters, 256 threads
 using Shape8W16 = FusedShape<8, 16, false, false>;  // 8-CTA clusters, 512 threads, 128 registers
+// 16-CTA clusters of 256 threads at <= 128 registers and 107 KB of shared
+// memory: two CTAs (of different clusters, or of one) per SM, so one CTA's
+// cluster barrier or DSMEM exchange overlaps the other's FFTs
+using Shape16x2 = FusedShape<16, 8, false, false, 2>;
 
 template <class S>
-__global__ void __launch_bounds__(S::THR, 1)
+__global__ void __launch_bounds__(S::THR, S::MINB)
 k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ items, int nitems,
                  const float* __restrict__ taper, const float2* __restrict__ twg,
                  float* __restrict__ partial, unsigned long long* __restrict__ next_item)
@@ -725,7 +730,8 @@ cudaError_t fused_max_clusters(int* n, int* shape)
 }
 
 // Co-resident clusters of one shape: 8 (8 CTAs x 8 warps), 816 (8 CTAs x 16
-// warps, 128 registers), 16 (16 CTAs x 16 warps, double buffered).
+// warps, 128 registers), 16 (16 CTAs x 16 warps, double buffered), 162 (16
+// CTAs x 8 warps, two CTAs per SM).
 cudaError_t fused_clusters_of(int shape, int* n)
 {
     *n = 0;
@@ -733,6 +739,7 @@ cudaError_t fused_clusters_of(int shape, int* n)
     case 8: return max_clusters<Shape8>(n);
     case 816: return max_clusters<Shape8W16>(n);
     case 16: return max_clusters<Shape16>(n);
+    case 162: return max_clusters<Shape16x2>(n);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -765,6 +772,11 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
         cudaLaunchConfig_t cfg = fused_cfg<Shape16>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16>, reinterpret_cast<const FusedTab*>(descs), items,
                                nitems, taper, tw, partial, next_item);
+    } else if (shape == 162) {
+        if ((e = prepare_kernel<Shape16x2>()) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = fused_cfg<Shape16x2>(nclusters, st, attr);
+        e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16x2>, reinterpret_cast<const FusedTab*>(descs),
+                               items, nitems, taper, tw, partial, next_item);
     } else if (shape == 816) {
         if ((e = prepare_kernel<Shape8W16>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape8W16>(nclusters, st, attr);

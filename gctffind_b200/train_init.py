@@ -4,7 +4,8 @@
     python -m gctffind_b200.train_init [--samples 1048576] [--batch 256]
 
 Training data: `samples` synthetic (256-bin rotational profile, 256 x 256
-polar half spectrum) pairs that the library itself generates on the GPU
+polar half spectrum) pairs, visited `epochs` times, that the library itself
+generates on the GPU
 (gcf_nn_train): the expected averaged spectrum of the micrograph model --
 white object, CTF with the parameter draw of the uneven batch (mean defocus
 5000-40000 A, astigmatism 0-1000 A at a uniform angle, pixel size
@@ -90,6 +91,8 @@ def main(argv=None):
     ap.add_argument("--samples", type=int, default=1 << 20)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--epochs", type=int, default=4,
+                    help="passes over the same samples; each pass decays from half the previous pass's rate")
     ap.add_argument("--init-seed", type=int, default=7)
     ap.add_argument("--eval", type=int, default=10000)
     ap.add_argument("--out", default=None, help="weights file (default: the package's weights/ctf_init.bin)")
@@ -103,13 +106,16 @@ def main(argv=None):
     ctx.nn_init(a.init_seed)
     steps = max(1, a.samples // a.batch)
     t0 = time.perf_counter()
-    losses = ctx.nn_train(op, steps=steps, batch=a.batch, seed=TRAIN_SEED, first=0, lr=a.lr)
+    losses = np.concatenate([ctx.nn_train(op, steps=steps, batch=a.batch, seed=TRAIN_SEED, first=0,
+                                          lr=a.lr * 0.5 ** e) for e in range(a.epochs)])
     train_s = time.perf_counter() - t0
     if not np.all(np.isfinite(losses)):
         raise RuntimeError("training diverged")
     ctx.save_weights(out)
-    summary = {"training": {"pairs": steps * a.batch, "batch": a.batch, "steps": steps, "lr": a.lr,
-                            "schedule": "Adam, cosine decay to 5 % of lr", "generator_seed": TRAIN_SEED,
+    summary = {"training": {"pairs": steps * a.batch, "batch": a.batch, "epochs": a.epochs,
+                            "steps": steps * a.epochs, "lr": a.lr,
+                            "schedule": "Adam; per epoch a cosine decay to 5 % of that epoch's rate, "
+                                        "the rate halved from epoch to epoch", "generator_seed": TRAIN_SEED,
                             "init_seed": a.init_seed, "seconds": round(train_s, 2),
                             "loss_first_100": round(float(losses[:100].mean()), 5),
                             "loss_last_100": round(float(losses[-100:].mean()), 5)}}

@@ -81,7 +81,8 @@ const char* gcf_last_error(gcf_ctx* ctx);
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
 /* Cluster shape of the fused tile kernel: 0 = the shape that keeps the most
  * SMs busy (default), 8 = 8 CTAs x 8 warps, 816 = 8 CTAs x 16 warps,
- * 16 = 16 CTAs x 16 warps.  For tuning; results do not depend on it. */
+ * 16 = 16 CTAs x 16 warps, 162 = 16 CTAs x 8 warps with two CTAs per SM.
+ * For tuning (gcf_autotune picks one by timing); results do not depend on it. */
 gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape);
 
 /* ---------------------------------------------------------------------- */
@@ -305,17 +306,21 @@ gcf_status gcf_set_graphs(gcf_ctx* ctx, int on);
  * not depend on the choice, only speed.  No counterpart in the reference,
  * whose kernels have fixed launch shapes. */
 typedef struct {
-    int fused_shape;     /* tile-kernel cluster shape picked: 8, 816 or 16 */
+    int fused_shape;     /* tile-kernel cluster shape picked: 8, 816, 16 or 162 */
     int gemm_tile_n;     /* contraction product tile picked: 128 x gemm_tile_n */
     int gemm_stages;     /* its load-pipeline depth */
-    float fused_ms[3];   /* trial ms of shapes 8, 816, 16 (-1: cannot be resident) */
+    float fused_ms[4];   /* trial ms of shapes 8, 816, 16, 162 (-1: cannot be resident) */
     float gemm_ms[6];    /* trial ms of (256,2) (256,3) (256,4) (128,4) (128,6) (64,4) */
 } gcf_tuning;
 gcf_status gcf_autotune(gcf_ctx* ctx, int force, gcf_tuning* out);
 
 /* [0] graph launches of the last batch call (0: it ran eagerly), [1] nodes
- * of the cached graph, [2] kernels of this library captured in it. */
-gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[3]);
+ * of the cached graph, [2] kernels of this library captured in it, [3] why
+ * the last capture gave no graph (0: it did; 1 staging memory, 2 capture
+ * could not begin, 3 an enqueued step failed, 4 capture could not end,
+ * 5 a buffer was reallocated during it, 6 instantiation failed; the
+ * detail is in gcf_last_error). */
+gcf_status gcf_get_graph_info(gcf_ctx* ctx, long long info[4]);
 
 /* Refined CC below which a learned search falls back to the full search
  * (default 0.1); a result at the edge of its window always falls back. */

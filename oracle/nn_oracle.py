@@ -17,7 +17,12 @@ Loss: mean over the batch and the 3 outputs of (pred - target)^2.
 
 The library multiplies BF16 copies of the weights; pass bf16_weights=True
 (the default) to use the same rounded values here, so the comparison
-isolates the rounding of the activations.
+isolates the rounding of the activations.  emulate_bf16=True also rounds to
+BF16 wherever the library stores BF16 (gctffind_b200/csrc/gcf_learned.cpp
+nn_forward / nn_backward): every ReLU output, the loss gradient dpred, and
+each layer's masked input gradient (after the col2im sums for the
+convolutions); products and sums stay FP64, so what remains is the
+library's FP32 accumulation.
 """
 from __future__ import annotations
 
@@ -71,9 +76,10 @@ def _col2im3(dcols, H, W, C):
     return dxp[:, 1:H + 1, 1:W + 1, :]
 
 
-def forward_backward(params, x1, x2, target, bf16_weights=True):
+def forward_backward(params, x1, x2, target, bf16_weights=True, emulate_bf16=False):
     """Returns (loss, flat gradients, predictions)."""
     P = unpack(params, bf16_weights)
+    q = bf16 if emulate_bf16 else (lambda v: v)
     x1 = np.asarray(x1, np.float64)
     x2 = np.asarray(x2, np.float64)
     t = np.asarray(target, np.float64)
@@ -81,16 +87,16 @@ def forward_backward(params, x1, x2, target, bf16_weights=True):
     relu = lambda z: np.maximum(z, 0.0)
     # conv1: 4x4 stride-4 patches
     c1 = x2.reshape(B, 64, 4, 64, 4).transpose(0, 1, 3, 2, 4).reshape(B, 64, 64, 16)
-    y1 = relu(c1 @ P[0][0].T + P[0][1])
+    y1 = q(relu(c1 @ P[0][0].T + P[0][1]))
     c2 = _im2col3(y1)
-    y2 = relu(c2 @ P[1][0].T + P[1][1])
+    y2 = q(relu(c2 @ P[1][0].T + P[1][1]))
     c3 = _im2col3(y2)
-    y3 = relu(c3 @ P[2][0].T + P[2][1])
+    y3 = q(relu(c3 @ P[2][0].T + P[2][1]))
     c4 = _im2col3(y3)
-    y4 = relu(c4 @ P[3][0].T + P[3][1])
+    y4 = q(relu(c4 @ P[3][0].T + P[3][1]))
     h0 = np.concatenate([x1, y4.reshape(B, 2048)], axis=1)
-    h1 = relu(h0 @ P[4][0].T + P[4][1])
-    h2 = relu(h1 @ P[5][0].T + P[5][1])
+    h1 = q(relu(h0 @ P[4][0].T + P[4][1]))
+    h2 = q(relu(h1 @ P[5][0].T + P[5][1]))
     pred = h2 @ P[6][0].T + P[6][1]
     d = pred - t
     loss = float((d * d).mean())
@@ -100,17 +106,17 @@ def forward_backward(params, x1, x2, target, bf16_weights=True):
         g[k] = (dz.reshape(-1, dz.shape[-1]).T @ x.reshape(-1, x.shape[-1]), dz.reshape(-1, dz.shape[-1]).sum(0))
         return dz @ P[k][0]
 
-    dz = 2.0 * d / (3.0 * B)
-    dh2 = lin_grad(6, dz, h2) * (h2 > 0)
-    dh1 = lin_grad(5, dh2, h1) * (h1 > 0)
+    dz = q(2.0 * d / (3.0 * B))
+    dh2 = q(lin_grad(6, dz, h2) * (h2 > 0))
+    dh1 = q(lin_grad(5, dh2, h1) * (h1 > 0))
     dh0 = lin_grad(4, dh1, h0)
-    dy4 = dh0[:, 256:].reshape(B, 8, 8, 32) * (y4 > 0)
+    dy4 = q(dh0[:, 256:].reshape(B, 8, 8, 32) * (y4 > 0))
     dc4 = lin_grad(3, dy4, c4)
-    dy3 = _col2im3(dc4, 16, 16, 32) * (y3 > 0)
+    dy3 = q(_col2im3(dc4, 16, 16, 32) * (y3 > 0))
     dc3 = lin_grad(2, dy3, c3)
-    dy2 = _col2im3(dc3, 32, 32, 32) * (y2 > 0)
+    dy2 = q(_col2im3(dc3, 32, 32, 32) * (y2 > 0))
     dc2 = lin_grad(1, dy2, c2)
-    dy1 = _col2im3(dc2, 64, 64, 16) * (y1 > 0)
+    dy1 = q(_col2im3(dc2, 64, 64, 16) * (y1 > 0))
     lin_grad(0, dy1, c1)
     flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in g])
     return loss, flat, pred

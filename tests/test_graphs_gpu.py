@@ -49,7 +49,7 @@ def test_graph_replay_matches_eager(gpu_lib, mode_name):
         assert _same(res, eager)
         seen.append(ctx.graph_info()["graph_launches"])
     # first call eager, then captured and replayed
-    assert seen == [0, 1, 1, 1]
+    assert seen == [0, 1, 1, 1], ctx.graph_info()
     info = ctx.graph_info()
     assert info["nodes"] > 0 and info["kernels"] == eager_launches
     assert ctx.stage_times()["total"] > 0
@@ -80,7 +80,7 @@ def test_graph_pinned_host_inputs(gpu_lib):
     ctx.set_graphs(True)
     for k in range(3):
         assert _same(ctx.run_batch(host, pxs, op, mode=G.GCF_SEARCH_BF16), ref)
-        assert ctx.graph_info()["graph_launches"] == (0 if k == 0 else 1)
+        assert ctx.graph_info()["graph_launches"] == (0 if k == 0 else 1), ctx.graph_info()
     # pageable host memory never takes a graph
     pageable = [h.clone().numpy() for h in host]
     for _ in range(2):

@@ -2,12 +2,16 @@
 against the FP64 oracle (oracle/nn_oracle.py), training by the library's
 own kernels, and the learned window search against the plain search.
 
-Gradient check bar: the library stores activations and gradients in BF16
-(8 significant bits) between layers and multiplies BF16 operands with FP32
-accumulation; the oracle uses the same BF16-rounded weights in FP64 with
-unrounded activations.  So per layer the gradient must agree to a relative
-L2 error of 5e-2 with cosine similarity above 0.998, the loss to 2e-2
-relative and the predictions to 2e-2 of their spread.
+Gradient check bars.  The library stores activations and gradients in
+BF16 (8 significant bits) between layers and multiplies BF16 operands with
+FP32 accumulation.  (1) Against the oracle that rounds to BF16 at the same
+points (products and sums in FP64): per layer a relative L2 error <= 1e-2
+and cosine similarity >= 0.9999 -- what remains is FP32 accumulation and
+the rare ReLU input that lands on the other side of zero.  (2) Against the
+plain FP64 oracle (BF16 weights, unrounded activations), the cost of the
+BF16 storage itself: loss within 2e-2 relative, predictions within 2e-2 of
+their spread, each layer's gradient within a relative L2 error of 0.15 and
+cosine similarity >= 0.99.
 """
 import numpy as np
 import pytest
@@ -30,20 +34,21 @@ def test_gradients_match_oracle(gpu_lib):
     loss, grads, pred = ctx.nn_forward_backward(x1, x2, t)
     ctx.close()
     # the oracle sees the BF16-rounded inputs the library used
-    oloss, ograds, opred = N.forward_backward(params, N.bf16(x1), N.bf16(x2), t)
-    assert abs(loss - oloss) <= 2e-2 * abs(oloss), (loss, oloss)
-    assert np.abs(pred - opred).max() <= 2e-2 * (np.abs(opred).max() + 1e-3), (pred, opred)
-    for k, ((gw, gb), (ow, ob)) in enumerate(zip(N.split(grads), N.split(ograds))):
-        for a, b in ((gw, ow), (gb, ob)):
-            a = a.ravel().astype(np.float64)
-            b = b.ravel()
-            nb = np.linalg.norm(b)
-            if nb == 0:
-                assert np.linalg.norm(a) == 0
-                continue
-            rel = np.linalg.norm(a - b) / nb
-            cos = float(a @ b / (np.linalg.norm(a) * nb + 1e-300))
-            assert rel <= 5e-2 and cos >= 0.998, (k, rel, cos)
+    for emulate, rel_bar, cos_bar in ((True, 1e-2, 0.9999), (False, 0.15, 0.99)):
+        oloss, ograds, opred = N.forward_backward(params, N.bf16(x1), N.bf16(x2), t, emulate_bf16=emulate)
+        assert abs(loss - oloss) <= 2e-2 * abs(oloss), (emulate, loss, oloss)
+        assert np.abs(pred - opred).max() <= 2e-2 * (np.abs(opred).max() + 1e-3), (emulate, pred, opred)
+        for k, ((gw, gb), (ow, ob)) in enumerate(zip(N.split(grads), N.split(ograds))):
+            for a, b in ((gw, ow), (gb, ob)):
+                a = a.ravel().astype(np.float64)
+                b = b.ravel()
+                nb = np.linalg.norm(b)
+                if nb == 0:
+                    assert np.linalg.norm(a) == 0
+                    continue
+                rel = np.linalg.norm(a - b) / nb
+                cos = float(a @ b / (np.linalg.norm(a) * nb + 1e-300))
+                assert rel <= rel_bar and cos >= cos_bar, (emulate, k, rel, cos)
 
 
 def test_training_lowers_the_loss_and_weights_round_trip(gpu_lib, tmp_path):
@@ -81,7 +86,8 @@ def test_trained_network_gain_on_held_out_spectra(gpu_lib):
     FP32 exhaustive search, the BF16 contraction search without the network
     and the learned window search.  Bar: the learned search lands within one
     search step of the plain one for >= 99 % of the spectra with a median
-    |d defocus| <= 20 A, falls back to the full search for at most 5 %, and
+    |d defocus| <= 20 A, falls back to the full search for at most 3 % beyond
+    the spectra whose CC is below the threshold anyway, and
     scores fewer than half the table candidates of the search without the
     network -- what the network gains."""
     from gctffind_b200 import train_init as TI
@@ -101,7 +107,10 @@ def test_trained_network_gain_on_held_out_spectra(gpu_lib):
     med_l, frac_l, _ = TI.compare(learned, plain)
     assert frac_b >= 0.99 and med_b <= 20.0, (frac_b, med_b)
     assert frac_l >= 0.99 and med_l <= 20.0, (frac_l, med_l)
-    assert cl["fallbacks"] <= 0.05 * n, cl
+    # fallbacks: the refined CC below the threshold (low-dose spectra, where
+    # the full search finds no better) or an optimum at the window's edge
+    low_cc = sum(r.score < 0.1 for r in bf16)
+    assert cl["fallbacks"] <= low_cc + 0.03 * n, (cl, low_cc)
     assert cl["table_cand"] < 0.5 * cb["table_cand"], (cl, cb)
     # both stay as close to the generator's truth as the plain search
     assert TI.truth_error(learned, prm) <= TI.truth_error(plain, prm) + 20.0
