@@ -49,9 +49,14 @@ N_BATCH = 256
 METRIC = "4096^2 micrographs/s, learned+batched+BF16 vs plain GPU path; defocus error (A)"
 SERIES_PX = 1.35
 # DRAM bytes (read + write) of k_fused_spectrum per algorithmic byte (the
-# image read once), from ncu dram__bytes_read.sum + dram__bytes_write.sum on
-# a 3-micrograph capture of the same kernel
-TILE_KERNEL_TRAFFIC_RATIO = (262_052_608 + 11_340_544) / (3 * 67_108_864)
+# images read once), from ncu dram__bytes_read.sum + dram__bytes_write.sum of
+# the first tile launch of `bench.py --batch 16 --steps 1 --warmup 3
+# --no-secondary --no-cpu-baseline --no-autotune --no-graphs --mode bf16`
+# (16 micrographs of this workload, 904.6 MB of algorithmic bytes)
+TILE_KERNEL_TRAFFIC_RATIO = (1_028_731_000 + 62_378_752) / 904_559_168
+TILE_KERNEL_TRAFFIC_CAPTURE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the first k_fused_spectrum launch "
+                               "of bench.py --batch 16 (16 micrographs of this workload), per algorithmic byte, "
+                               "scaled by this launch's algorithmic bytes")
 
 
 def parse():
@@ -352,6 +357,21 @@ def single_1p0(ctx, G, steps):
             "result": {"df_min": round(r.df_min, 1), "df_max": round(r.df_max, 1), "azimuth": round(r.azimuth, 2)}}
 
 
+def h2d_rate(src, device):
+    """Host -> device copy rate of this box (GB/s): one pinned micrograph
+    copied 8 times, CUDA events around the copies."""
+    import torch
+    dst = torch.empty(src.shape, dtype=src.dtype, device=f"cuda:{device}")
+    dst.copy_(src, non_blocking=True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(8):
+        dst.copy_(src, non_blocking=True)
+    b.record()
+    b.synchronize()
+    return round(8 * src.numel() * 4 / (a.elapsed_time(b) / 1000.0) / 1e9, 1)
+
+
 def tile_kernel_roofline(stage, imgs_dims, pk):
     """k_fused_spectrum (+ its cluster-less companion) over every tile of the
     batch: algorithmic bytes = each (rescaled) image the kernel reads, read
@@ -364,8 +384,7 @@ def tile_kernel_roofline(stage, imgs_dims, pk):
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": "fallback" if pk.get("_fallback") else "measured",
             "traffic": int(algo * TILE_KERNEL_TRAFFIC_RATIO),
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per image byte on a 3 x 4096^2 "
-                              "capture of k_fused_spectrum, scaled by the batch's image bytes",
+            "traffic_source": TILE_KERNEL_TRAFFIC_CAPTURE,
             "algorithmic_bytes_per_launch": algo, "launch_ms": round(ms, 3)}
 
 
@@ -476,11 +495,16 @@ def main():
         ctx.run_batch(host, pxs, op, mode=fast_mode)
     barrier(world)
     e2e_wall = 0.0
+    e2e_stage = {}
     for _ in range(args.steps):
         t0 = time.perf_counter()
         ctx.run_batch(host, pxs, op, mode=fast_mode)
         e2e_wall += time.perf_counter() - t0
+        for k, v in ctx.stage_times().items():
+            e2e_stage[k] = e2e_stage.get(k, 0.0) + v / args.steps
+    e2e_graph = ctx.graph_info()
     e2e_ms = max_over_ranks(e2e_wall / args.steps * 1000.0, world)
+    pcie = h2d_rate(host[0], local)
     clocks = clk.stop()
     n = args.batch
     value = world * n / (fast["ms"] / 1000.0)
@@ -516,7 +540,11 @@ def main():
             "e2e": {"value": round(world * n / (e2e_ms / 1000.0), 2), "unit": "micrographs/s",
                     "h2d_bytes_per_step": sum(4 * s.width * s.height for s in specs),
                     "d2h_bytes_per_step": n * 40, "ms_per_step": round(e2e_ms, 3),
-                    "timing": "host clock around gcf_run_batch_mode (pinned host images)"},
+                    "timing": "host clock around gcf_run_batch_mode (pinned host images)",
+                    "stage_ms": {k: round(v, 3) for k, v in e2e_stage.items()},
+                    "graph_launches": e2e_graph["graph_launches"],
+                    "pcie_h2d_gbs": pcie,
+                    "pcie_bound_ms": round(sum(4 * s.width * s.height for s in specs) / pcie / 1e6, 1)},
             "gpu_launches": fast["launches"],
             "cuda_graphs": {"graph_launches_per_step": fast["graph_launches_per_step"],
                             "graph_nodes": fast["graph"]["nodes"],

@@ -143,8 +143,9 @@ struct HostArena {
 // graphs on): the graph of its device work, keyed by everything the work
 // depends on, and what the host needs to read its results back.
 struct BatchGraph {
-    unsigned long long key = 0;
-    int seen = 0;                      // eager calls with this key so far
+    unsigned long long key = 0;        // key of the call that `exec` replays
+    unsigned long long want = 0;       // key of the latest eager call
+    int seen = 0;                      // eager calls in a row with key `want`
     cudaGraphExec_t exec = nullptr;
     unsigned long long epoch = 0;      // device-allocation epoch at capture
     unsigned long long model_version = 0;   // contraction model rows it read
@@ -661,17 +662,24 @@ gcf_status spectrum_cufft(gcf_ctx* ctx, const MicImage& m, float* raw_out)
 // micrograph's tiles form runs of at most 24 (an item's |F| sums live in
 // registers until it ends); the split depends on the micrograph alone, so
 // its spectrum does not depend on the batch or chunk it is in.
+// The tile kernel's cluster shape and resident cluster count (chosen once,
+// again after gcf_set_fused_shape / gcf_autotune).
+gcf_status ensure_fused_shape(gcf_ctx* ctx)
+{
+    if (ctx->fused_clusters > 0) return GCF_OK;
+    int n = 0, shape = ctx->fused_shape_req;
+    if (shape) CK(fused_clusters_of(shape, &n));
+    else CK(fused_max_clusters(&n, &shape));
+    if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
+    ctx->fused_clusters = n;
+    ctx->fused_shape = shape;
+    return GCF_OK;
+}
+
 gcf_status fused_plan(gcf_ctx* ctx, const std::vector<MicImage>& mics)
 {
     const int T = ctx->tile, cx = T / 2 + 1, nm = (int)mics.size();
-    if (ctx->fused_clusters <= 0) {
-        int n = 0, shape = ctx->fused_shape_req;
-        if (shape) CK(fused_clusters_of(shape, &n));
-        else CK(fused_max_clusters(&n, &shape));
-        if (n <= 0) return fail(ctx, GCF_ERR_CUDA, "fused spectrum kernel cannot be resident");
-        ctx->fused_clusters = n;
-        ctx->fused_shape = shape;
-    }
+    CKS(ensure_fused_shape(ctx));
     // 24 rather than 32: the cluster-less CTAs then finish their last items
     // sooner and may keep taking items longer (a 41-tilt series step 12.43
     // -> 12.21 ms; the spectra change only in the grouping of the sums)
@@ -2657,7 +2665,6 @@ bool batch_capture(gcf_ctx* ctx, unsigned long long key, const std::vector<const
         if (G.exec) cudaGraphExecDestroy(G.exec);
         G.exec = nullptr;
         G.key = 0;
-        G.seen = 0;
     }
     if (g) cudaGraphDestroy(g);
     return ok;
@@ -2694,17 +2701,22 @@ gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, 
     CK(cudaEventRecord(t0, ctx->st));
     BatchGraph& G = ctx->bgraph;
     const bool graphable = ctx->graphs && (on_device || all_pinned(imgs.data(), n));
+    if (graphable && ctx->impl == GCF_SPECT_FUSED && fused_tile_supported(ctx->tile)) {
+        gcf_status fs = ensure_fused_shape(ctx);   // part of the key
+        if (fs != GCF_OK) {
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            return fs;
+        }
+    }
     const unsigned long long key = graphable ? batch_key(ctx, items, n, on_device, *optics, mode) : 0;
     bool replay = graphable && G.exec && G.key == key && G.epoch == device_alloc_epoch() &&
                   G.model_version == ctx->model_version;
-    if (!replay && graphable && G.key == key && G.seen >= 1) {
+    if (!replay && graphable && G.want == key && G.seen >= 1) {
         // a second attempt within the call: a library may initialise
         // something on the first captured use of an object
-        for (int attempt = 0; attempt < 2 && !replay; ++attempt) {
-            G.key = key;
-            G.seen = 1;
+        for (int attempt = 0; attempt < 2 && !replay; ++attempt)
             replay = batch_capture(ctx, key, imgs, ws, hs, pxs, on_device, *optics, mode);
-        }
     }
     SearchPending pend;
     std::vector<float> pxn;
@@ -2723,8 +2735,8 @@ gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, 
         ctx->arena.reset();   // every earlier call has completed
         st = batch_enqueue(ctx, imgs, ws, hs, pxs, on_device, *optics, mode, pend, pxn);
         if (graphable) {
-            if (G.key != key) {
-                G.key = key;
+            if (G.want != key) {
+                G.want = key;
                 G.seen = 0;
             }
             G.seen += 1;

@@ -63,7 +63,18 @@ def test_graph_replay_matches_eager(gpu_lib, mode_name):
     # another batch: eager again, its own graph from its second call on
     res2 = ctx.run_batch(imgs[:3], pxs[:3], op, mode=mode)
     assert ctx.graph_info()["graph_launches"] == 0
-    assert _same(res2, eager_ctx.run_batch(imgs[:3], pxs[:3], op, mode=mode))
+    ref2 = eager_ctx.run_batch(imgs[:3], pxs[:3], op, mode=mode)
+    assert _same(res2, ref2)
+    # calls that alternate between batches and methods never replay another
+    # call's graph
+    ref1 = eager_ctx.run_batch(imgs, pxs, op, mode=mode)
+    other = G.GCF_SEARCH_BF16 if mode == G.GCF_SEARCH_PLAIN else G.GCF_SEARCH_PLAIN
+    ref3 = eager_ctx.run_batch(imgs[:3], pxs[:3], op, mode=other)
+    for args, ref in [((imgs[:3], pxs[:3], mode), ref2), ((imgs[:3], pxs[:3], mode), ref2),
+                      ((imgs, pxs, mode), ref1), ((imgs[:3], pxs[:3], other), ref3),
+                      ((imgs[:3], pxs[:3], other), ref3), ((imgs[:3], pxs[:3], mode), ref2),
+                      ((imgs, pxs, mode), ref1)]:
+        assert _same(ctx.run_batch(args[0], args[1], op, mode=args[2]), ref), ctx.graph_info()
     ctx.close()
     eager_ctx.close()
 
