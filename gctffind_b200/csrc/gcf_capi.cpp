@@ -76,18 +76,20 @@ struct BandHost {
 
 struct FftPlan {
     cufftHandle h = 0;
+    unsigned long long used = 0;   // last use (the context's plan clock)
 };
 
-// Pinned host staging of the small host -> device uploads of one call
-// (job tables, work items, descriptors): the asynchronous copies read from
-// here, so the host vectors they came from may go away, and a CUDA graph
-// captured from the call keeps valid sources for its copy nodes (a graph
-// owns the arena it was captured with).  Blocks never move; reset() reuses
-// them once the copies of the previous call are complete.
+// Mapped page-locked host staging of the small host -> device uploads of
+// one call (job tables, work items, descriptors): the copy kernels read
+// from here, so the host vectors they came from may go away, and a CUDA
+// graph captured from the call keeps valid sources for its copy nodes (a
+// graph owns the arena it was captured with).  Blocks never move; reset()
+// reuses them once the copies of the previous call are complete.
 struct HostArena {
     struct Block {
         char* p;
         size_t cap, used;
+        char* dev;   // the block's address on the device (mapped memory)
     };
     std::vector<Block> blocks;
     size_t cur = 0;
@@ -110,26 +112,38 @@ struct HostArena {
         for (const Block& b : blocks)
             if (b.cap >= bytes) return true;
         release();
-        Block b{nullptr, std::max<size_t>(bytes, (size_t)1 << 20), 0};
-        if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) return false;
+        Block b{nullptr, std::max<size_t>(bytes, (size_t)1 << 20), 0, nullptr};
+        if (!alloc(b)) return false;
         blocks.push_back(b);
         return true;
     }
+    static bool alloc(Block& b)
+    {
+        if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+            return false;
+        if (cudaHostGetDevicePointer((void**)&b.dev, b.p, 0) != cudaSuccess) {
+            cudaFreeHost(b.p);
+            b.p = nullptr;
+            return false;
+        }
+        return true;
+    }
+    // Copies src into the arena; returns the copy's device-side address.
     void* put(const void* src, size_t bytes)
     {
         const size_t need = (bytes + 255) & ~(size_t)255;
         while (cur < blocks.size() && blocks[cur].cap - blocks[cur].used < need) ++cur;
         if (cur == blocks.size()) {
             if (frozen) return nullptr;
-            Block b{nullptr, std::max<size_t>(need, (size_t)1 << 20), 0};
-            if (cudaHostAlloc((void**)&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+            Block b{nullptr, std::max<size_t>(need, (size_t)1 << 20), 0, nullptr};
+            if (!alloc(b)) return nullptr;
             blocks.push_back(b);
         }
         Block& b = blocks[cur];
-        void* dst = b.p + b.used;
-        std::memcpy(dst, src, bytes);
+        std::memcpy(b.p + b.used, src, bytes);
+        void* dev = b.dev + b.used;
         b.used += need;
-        return dst;
+        return dev;
     }
     void release()
     {
@@ -217,6 +231,8 @@ struct gcf_ctx {
     DBuf<PixOptics> d_optics;
 
     std::map<std::tuple<int, int, int>, FftPlan> plans;   // (kind, a, b)
+    unsigned long long plan_clock = 0;
+    DBuf<char> fft_work;   // work area shared by the rescale plans (one stream)
 
     // fused spectrum
     DBuf<float2> tw512;
@@ -306,8 +322,11 @@ struct gcf_ctx {
 namespace {
 
 // Host -> device upload of `bytes` from a transient host buffer, staged
-// through the context's pinned arena.  Outside a capture, an arena that has
-// grown past 64 MB is recycled once the context's streams are idle.
+// through the context's pinned arena and copied by a kernel on `st` (not a
+// copy-engine transfer: those queue behind the bulk image uploads of the
+// copy stream, which would hold the compute stream until every image had
+// landed).  Outside a capture, an arena that has grown past 64 MB is
+// recycled once the context's streams are idle.
 cudaError_t h2d(gcf_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st)
 {
     if (bytes == 0) return cudaSuccess;
@@ -325,7 +344,7 @@ cudaError_t h2d(gcf_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStre
     }
     void* h = ctx->arena.put(src, bytes);
     if (!h) return cudaErrorMemoryAllocation;
-    return cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, st);
+    return launch_copy_from_host(dst, h, bytes, st);
 }
 
 gcf_status fail(gcf_ctx* c, gcf_status s, const char* what)
@@ -580,16 +599,58 @@ gcf_status upload_bands(gcf_ctx* ctx)
     return GCF_OK;
 }
 
+// Rescale plans (kinds 1, 2) kept at most: a batch of micrographs at
+// continuously varying pixel sizes needs a new C2R size per micrograph, so
+// the least recently used plans are destroyed beyond this count (more than
+// one 256-micrograph batch needs, so a repeated batch finds all its plans).
+constexpr size_t kMaxRescalePlans = 640;
+
 gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
 {
     auto key = std::make_tuple(kind, a, b);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) {
+        it->second.used = ++ctx->plan_clock;
         *out = it->second.h;
         return GCF_OK;
     }
     cufftHandle h;
     cufftResult r;
+    if (kind == 1 || kind == 2) {
+        // rescale plans run one after another on ctx->st: they share one
+        // work area instead of each holding its own
+        size_t n_rescale = 0;
+        for (auto& kv : ctx->plans) n_rescale += (std::get<0>(kv.first) == 1 || std::get<0>(kv.first) == 2);
+        while (n_rescale >= kMaxRescalePlans) {
+            auto lru = ctx->plans.end();
+            for (auto q = ctx->plans.begin(); q != ctx->plans.end(); ++q)
+                if ((std::get<0>(q->first) == 1 || std::get<0>(q->first) == 2) &&
+                    (lru == ctx->plans.end() || q->second.used < lru->second.used))
+                    lru = q;
+            CK(cudaStreamSynchronize(ctx->st));
+            cufftDestroy(lru->second.h);
+            ctx->plans.erase(lru);
+            note_device_alloc();   // a captured graph may hold the destroyed plan
+            --n_rescale;
+        }
+        size_t ws = 0;
+        r = cufftCreate(&h);
+        if (r == CUFFT_SUCCESS) r = cufftSetAutoAllocation(h, 0);
+        if (r == CUFFT_SUCCESS) r = cufftMakePlan2d(h, a, b, kind == 1 ? CUFFT_R2C : CUFFT_C2R, &ws);
+        if (r == CUFFT_SUCCESS && ws > ctx->fft_work.n) {
+            CK(cudaStreamSynchronize(ctx->st));
+            CK(ctx->fft_work.ensure(ws));
+            for (auto& kv : ctx->plans)
+                if (std::get<0>(kv.first) == 1 || std::get<0>(kv.first) == 2)
+                    cufftSetWorkArea(kv.second.h, ctx->fft_work.p);
+        }
+        if (r == CUFFT_SUCCESS) r = cufftSetWorkArea(h, ctx->fft_work.p);
+        if (r != CUFFT_SUCCESS) {
+            cufftDestroy(h);
+            ctx->err = "cufft plan creation failed (" + std::to_string((int)r) + ")";
+            return r == CUFFT_ALLOC_FAILED ? GCF_ERR_NO_MEMORY : GCF_ERR_CUFFT;
+        }
+    }
     if (kind == 0) {   // batched tile R2C: a = tile, b = batch
         int n[2] = {a, a};
         r = cufftPlanMany(&h, 2, n, nullptr, 1, a * a, nullptr, 1, (a / 2 + 1) * a, CUFFT_R2C, b);
@@ -599,11 +660,7 @@ gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
             r = cufftPlanMany(&h, 2, n, nullptr, 1, a * a, nullptr, 1, (a / 2 + 1) * a, CUFFT_R2C, b);
         else
             r = cufftPlanMany(&h, 2, n, nullptr, 1, (a / 2 + 1) * a, nullptr, 1, a * a, CUFFT_C2R, b);
-    } else if (kind == 1) {   // image R2C: a = height, b = width
-        r = cufftPlan2d(&h, a, b, CUFFT_R2C);
-    } else {   // image C2R: a = height, b = width
-        r = cufftPlan2d(&h, a, b, CUFFT_C2R);
-    }
+    }   // kinds 1 and 2 (image R2C / C2R: a = height, b = width) above
     if (r != CUFFT_SUCCESS) {
         ctx->err = "cufft plan creation failed (" + std::to_string((int)r) + ")";
         return r == CUFFT_ALLOC_FAILED ? GCF_ERR_NO_MEMORY : GCF_ERR_CUFFT;
@@ -613,6 +670,7 @@ gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
         return fail(ctx, GCF_ERR_CUFFT, "cufftSetStream failed");
     }
     ctx->plans[key].h = h;
+    ctx->plans[key].used = ++ctx->plan_clock;
     *out = h;
     return GCF_OK;
 }
@@ -1759,6 +1817,7 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->st_solo) cudaStreamSynchronize(ctx->st_solo);
     if (ctx->st_tile) cudaStreamSynchronize(ctx->st_tile);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
+    ctx->fft_work.release();
     for (auto* b : ctx->bands) {
         b->idx.release();
         b->a.release();

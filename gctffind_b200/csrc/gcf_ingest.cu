@@ -1,4 +1,5 @@
-// gcf_ingest.cu -- MRC section bytes to float on the GPU.
+// gcf_ingest.cu -- MRC section bytes to float on the GPU, and the copy
+// kernel of the context's small uploads.
 //
 // CLoadImages::mToFloat (MrcUtil/CLoadImages.cpp:146-181) converts each
 // section on the host after reading it; here the raw bytes cross PCIe as
@@ -84,6 +85,36 @@ __global__ void k_mrc_to_float(const unsigned char* __restrict__ raw, int mode, 
 }
 
 }  // namespace
+
+namespace {
+
+// dst[0, bytes) = src[0, bytes) with src in mapped page-locked host memory:
+// 16-byte words where both sides allow, bytes at the ends.
+__global__ void k_copy_from_host(unsigned char* __restrict__ dst, const unsigned char* __restrict__ src,
+                                 size_t bytes, int vec)
+{
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nth = (size_t)gridDim.x * blockDim.x;
+    size_t done = 0;
+    if (vec) {
+        const size_t words = bytes / 16;
+        for (size_t i = tid; i < words; i += nth)
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+        done = words * 16;
+    }
+    for (size_t i = done + tid; i < bytes; i += nth) dst[i] = src[i];
+}
+
+}  // namespace
+
+cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st)
+{
+    if (bytes == 0) return cudaSuccess;
+    const int vec = (((uintptr_t)dst | (uintptr_t)src_mapped) % 16) == 0;
+    const int blocks = (int)std::min<size_t>((bytes / 16 + 255) / 256 + 1, 148);
+    k_copy_from_host<<<blocks, 256, 0, st>>>(static_cast<unsigned char*>(dst),
+                                             static_cast<const unsigned char*>(src_mapped), bytes, vec);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mrc_to_float(const void* raw, int mode, int swap, size_t npx, float* out, cudaStream_t st)
 {

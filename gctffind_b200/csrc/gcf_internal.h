@@ -36,6 +36,11 @@ int mrc_mode_bytes(int mode);
 // gcf_ingest.cu: raw MRC section bytes (mode 0/5 unsigned char, 1 short,
 // 6 unsigned short, 2 float; `swap`: big-endian file) to float.
 cudaError_t launch_mrc_to_float(const void* raw, int mode, int swap, size_t npx, float* out, cudaStream_t st);
+// dst (device) = bytes read by a kernel from mapped page-locked host memory
+// (src_mapped: its device-side address).  Small uploads take this route
+// instead of a copy-engine transfer, so they never queue behind the bulk
+// image uploads on the copy engines.
+cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st);
 
 constexpr int kMaxCand = 2624;        // >= 51 * 51 astigmatism grid
 constexpr int kEvalThreads = 256;     // threads of the candidate kernel
