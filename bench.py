@@ -230,6 +230,7 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
     dev_ms, launches, stage, ftimes, fcounts = 0.0, 0, {}, {}, {}
     graph_launches = 0
     res = None
+    torch.cuda.nvtx.range_push(f"timed_mode{mode}")
     for _ in range(steps):
         res = ctx.run_batch(imgs, pxs, op, mode=mode)
         st = ctx.stage_times()
@@ -242,6 +243,7 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
             for k, v in ctx.fast_times().items():
                 ftimes[k] = ftimes.get(k, 0.0) + v / steps
             fcounts = ctx.fast_counts()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(world)
     return {"ms": max_over_ranks(dev_ms / steps, world), "results": res, "stage": stage,
