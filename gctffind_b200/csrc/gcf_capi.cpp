@@ -916,8 +916,20 @@ gcf_status spectra_post(gcf_ctx* ctx, int nm, int first = 0)
     launch_moments(ctx->ctf0.p + o, (int)cmp_n, nm, ctx->moments.p + 2 * (size_t)first, ctx->st);
     CKL();
     // CFindCtfBase::mLowpass (FindCTF/CFindCtfBase.cpp:191-219): full
-    // spectrum, R2C, B-factor 10 (normalised), C2R, half back.
+    // spectrum, R2C, B-factor 10 (normalised), C2R, half back.  Tile 512
+    // with the hand-written spectrum path: the separable filter on the warp
+    // FFT (launch_lowpass512); otherwise (and for the cuFFT comparison
+    // variant) batched cuFFT.
     CK(ctx->lpfull.ensure((size_t)nm * T * T));
+    if (ctx->impl == GCF_SPECT_FUSED && fused_tile_supported(T)) {
+        CK(launch_lowpass512(ctx->ctf0.p + o, ctx->tw512.p, 10.0, nm, ctx->moments.p + 2 * (size_t)first,
+                             ctx->lpfull.p, ctx->ctf.p + o, ctx->lowpassed.p + first, ctx->st));
+        launch_radial(ctx->ctf.p + o, T, nm, ctx->rad_off.p, ctx->rad_pix.p, ctx->radial.p + (size_t)first * cx,
+                      ctx->st);
+        CKL();
+        ctx->launches += 6;
+        return GCF_OK;
+    }
     CK(ctx->lpcmp.ensure((size_t)nm * cx * T));
     launch_lp_full(ctx->ctf0.p + o, T, nm, ctx->lpfull.p, ctx->st);
     CKL();

@@ -704,9 +704,182 @@ cudaError_t max_clusters(int* n)
     return cudaOccupancyMaxActiveClusters(n, (void*)k_fused_spectrum<S>, &cfg);
 }
 
+// ---- B-factor lowpass of 512 x 512 spectra with the warp FFT ----------------
+// CFindCtfBase::mLowpass (FindCTF/CFindCtfBase.cpp:191-219) filters the full
+// spectrum F (512 x 512 real, DC at column 256) by a forward R2C, the
+// factor exp(-B (kx^2 + ky^2) / (2 N^2)) / N^2 (GLowpass2D::DoBFactor,
+// FindCTF/GLowpass2D.cu:9-23) and a C2R.  The factor is a product of one
+// real, even function per axis, so the filter is separable: rows first,
+// then columns, each  r' = IDFT(g DFT(r)) / N  with g(k) = exp(-B k^2 / (2 N^2))
+// (k wrapped to -N/2 .. N/2).  Because g is real and even it keeps real
+// signals real, so two rows (columns) a, b go through one complex FFT as
+// a + i b and come back as a' + i b' with no split; the inverse is the
+// forward FFT of the conjugate.
+constexpr int kLpWarps = 8;
+
+// Filter values g(K) / N for the output layout of fft512_warp: lane 2m+p
+// holds bin K = m + 16k + 256p in v[P16(k)].
+__device__ __forceinline__ void lp_filter_pass(float2 (&v)[16], float2* scr, const float2* twl, const float* gk,
+                                               int lane)
+{
+    const int m = lane >> 1, p = lane & 1;
+    fft512_warp(v, scr, twl, lane);
+    // multiply, conjugate and put the spectrum back into natural order
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int K = m + 16 * k + 256 * p;
+        const float g = gk[K];
+        scr[sslot(K)] = make_float2(v[P16(k)].x * g, -v[P16(k)].y * g);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = scr[sslot(32 * j + lane)];
+    __syncwarp();
+    fft512_warp(v, scr, twl, lane);   // conj(result) = the filtered pair, bin order
+}
+
+__device__ __forceinline__ void lp_setup(float2* twl, float* gk, const float2* twg, double bfactor)
+{
+    for (int i = threadIdx.x; i < 16 * 32; i += blockDim.x) twl[i] = twg[((i & 31) * (i >> 5)) & (FT - 1)];
+    const double scale = -bfactor / (2.0 * (double)FT * FT);
+    for (int k = threadIdx.x; k < FT; k += blockDim.x) {
+        const int kw = k <= FT / 2 ? k : k - FT;
+        gk[k] = (float)(exp(scale * (double)kw * kw) / (double)FT);
+    }
+    __syncthreads();
+}
+
+// Rows: one warp per row pair of the full spectrum built from the half
+// spectrum (GCalcSpectrum::GenFullSpect's mirror, DC at column 256);
+// filtered rows to rowf [m][512][512].
+__global__ void __launch_bounds__(kLpWarps * 32)
+k_lowpass_rows(const float* __restrict__ ctf0, const float2* __restrict__ twg, double bfactor,
+               float* __restrict__ rowf)
+{
+    __shared__ float2 s_twl[16 * 32];
+    __shared__ float s_g[FT];
+    __shared__ float2 s_scr[kLpWarps][FSCR];
+    lp_setup(s_twl, s_g, twg, bfactor);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = blockIdx.y, y0 = 2 * (blockIdx.x * kLpWarps + warp);
+    const float* half = ctf0 + (size_t)m * FCX * FT;
+    float2 v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int X = 32 * j + lane, xd = X - (FCX - 1);
+        float a, b;
+        if (xd >= 0) {
+            a = half[(size_t)y0 * FCX + xd];
+            b = half[(size_t)(y0 + 1) * FCX + xd];
+        } else {
+            const int ya = (FT - y0) & (FT - 1), yb = (FT - y0 - 1) & (FT - 1);
+            a = half[(size_t)ya * FCX - xd];
+            b = half[(size_t)yb * FCX - xd];
+        }
+        v[j] = make_float2(a, b);
+    }
+    float2* scr = s_scr[warp];
+    lp_filter_pass(v, scr, s_twl, s_g, lane);
+    // the pair leaves through the scratch in bin order: coalesced rows
+    const int mm = lane >> 1, p = lane & 1;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) scr[sslot(mm + 16 * k + 256 * p)] = v[P16(k)];
+    __syncwarp();
+    float* ra = rowf + ((size_t)m * FT + y0) * FT;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float2 z = scr[sslot(32 * j + lane)];
+        ra[32 * j + lane] = z.x;          // conjugate: a' = Re, b' = -Im
+        ra[FT + 32 * j + lane] = -z.y;
+    }
+}
+
+// Columns: a CTA takes 32 adjacent columns of the row-filtered spectrum
+// (a 512 x 32 block through shared memory, 128-byte rows), each warp two
+// column pairs; only the columns of the half spectrum are kept: out[y][x] =
+// filtered[y][x + 256] (x < 256) and out[y][256] = filtered[y][0]
+// (CFindCtfBase.cpp:212-218).  Spectra whose background-removed variance is
+// below 1 keep ctf0 (the variance gate of mRemoveBackground,
+// FindCTF/CFindCtfBase.cpp:169-174).
+__global__ void __launch_bounds__(kLpWarps * 32)
+k_lowpass_cols(const float* __restrict__ rowf, const float* __restrict__ ctf0, const float2* __restrict__ twg,
+               double bfactor, const double* __restrict__ mom, float* __restrict__ out, int* __restrict__ lowpassed)
+{
+    extern __shared__ float s_blk[];   // [512][33]
+    __shared__ float2 s_twl[16 * 32];
+    __shared__ float s_g[FT];
+    __shared__ float2 s_scr[kLpWarps][FSCR];
+    const int m = blockIdx.y;
+    // blocks 0..7: columns 256 + 32 b ..; block 8: columns 0 .. 31 (column 0 kept)
+    const int c0 = blockIdx.x < 8 ? FT / 2 + 32 * blockIdx.x : 0;
+    const double mean = mom[2 * m], var = mom[2 * m + 1] - mean * mean;
+    const bool run = !(var < 1.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) lowpassed[m] = run ? 1 : 0;
+    float* o = out + (size_t)m * FCX * FT;
+    const float* h0 = ctf0 + (size_t)m * FCX * FT;
+    if (!run) {
+        for (int i = threadIdx.x; i < FT * 32; i += blockDim.x) {
+            const int y = i >> 5, X = c0 + (i & 31);
+            const int x = X >= FT / 2 ? X - FT / 2 : (X == 0 ? FT / 2 : -1);
+            if (x >= 0) o[(size_t)y * FCX + x] = h0[(size_t)y * FCX + x];
+        }
+        return;
+    }
+    lp_setup(s_twl, s_g, twg, bfactor);
+    const float* src = rowf + (size_t)m * FT * FT + c0;
+    for (int i = threadIdx.x; i < FT * 32; i += blockDim.x) {
+        const int y = i >> 5, c = i & 31;
+        s_blk[y * 33 + c] = src[(size_t)y * FT + c];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2* scr = s_scr[warp];
+    const int npairs = c0 == 0 ? 1 : 2;   // block 8 needs columns 0 and 1 only
+    for (int q = 0; q < npairs; ++q) {
+        const int cl = 2 * (2 * warp + q);   // local column of a; b = cl + 1
+        if (c0 == 0 && warp != 0) break;
+        float2 v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int y = 32 * j + lane;
+            v[j] = make_float2(s_blk[y * 33 + cl], s_blk[y * 33 + cl + 1]);
+        }
+        lp_filter_pass(v, scr, s_twl, s_g, lane);
+        const int mm = lane >> 1, p = lane & 1;
+        const int Xa = c0 + cl;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int y = mm + 16 * k + 256 * p;
+            const float2 z = v[P16(k)];
+            if (Xa >= FT / 2) {
+                o[(size_t)y * FCX + (Xa - FT / 2)] = z.x;
+                o[(size_t)y * FCX + (Xa + 1 - FT / 2)] = -z.y;
+            } else {   // Xa == 0: column 0 becomes the last half-spectrum column
+                o[(size_t)y * FCX + FT / 2] = z.x;
+            }
+        }
+    }
+}
+
 }  // namespace
 
 int fused_tile_supported(int tile) { return tile == FT ? 1 : 0; }
+
+cudaError_t launch_lowpass512(const float* ctf0, const float2* tw, double bfactor, int nmic, const double* moments,
+                              float* rowf, float* out, int* lowpassed, cudaStream_t st)
+{
+    if (nmic <= 0) return cudaSuccess;
+    cudaError_t e = init_constants();
+    if (e != cudaSuccess) return e;
+    k_lowpass_rows<<<dim3(FT / 2 / kLpWarps, nmic), kLpWarps * 32, 0, st>>>(ctf0, tw, bfactor, rowf);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const size_t sm = (size_t)FT * 33 * sizeof(float);
+    if ((e = cudaFuncSetAttribute(k_lowpass_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) !=
+        cudaSuccess)
+        return e;
+    k_lowpass_cols<<<dim3(9, nmic), kLpWarps * 32, sm, st>>>(rowf, ctf0, tw, bfactor, moments, out, lowpassed);
+    return cudaGetLastError();
+}
 
 // Picks the cluster shape that covers the most SMs: 16-CTA clusters (double
 // buffered) when the device can co-schedule them, else 8-CTA clusters.

@@ -209,6 +209,11 @@ void launch_bg_vertical(const float* raw, const double* hsum, int tile, int nmic
 void launch_moments(const float* spect, int n, int nmic, double* out2, cudaStream_t st);
 // lowpass of CFindCtfBase::mLowpass around a batched R2C / C2R pair
 void launch_lp_full(const float* ctf0, int tile, int nmic, float* full, cudaStream_t st);
+// gcf_fused.cu: the whole lowpass of 512 x 512 spectra (ctf0 -> out, the
+// variance gate included) with the warp FFT; rowf: 512 x 512 floats per
+// spectrum of scratch; tw: exp(-2 pi i k / 512), k < 512.
+cudaError_t launch_lowpass512(const float* ctf0, const float2* tw, double bfactor, int nmic, const double* moments,
+                              float* rowf, float* out, int* lowpassed, cudaStream_t st);
 void launch_lp_table(double* g, int tile, double bfactor, cudaStream_t st);
 void launch_lp_filter(float2* cmp, int tile, int nmic, const double* g, cudaStream_t st);
 void launch_lp_extract(const float* ctf0, const float* full, int tile, int nmic, const double* moments,

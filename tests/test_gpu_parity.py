@@ -71,6 +71,41 @@ def test_ctf_spectrum_matches_oracle_given_gpu_raw(case, oracle):
     assert np.max(np.abs(g - octf)) <= 1e-4 * rms
 
 
+def test_lowpass512_matches_oracle_and_cufft_variant(gpu_lib, oracle):
+    """Tile 512: the separable warp-FFT lowpass (rows, then columns, each
+    pair of real lines as one complex FFT) against the oracle's background
+    removal + FP64 lowpass of the same raw spectrum, and against the
+    batched-cuFFT comparison variant (2D R2C / C2R), both within 1e-4 of the
+    rms per pixel; the variance gate (faint image) keeps the unfiltered
+    spectrum in both variants."""
+    G = gpu_lib
+    img = _img(seed=17, w=1536, h=1536)
+    out = {}
+    for impl in (G.GCF_SPECT_FUSED, G.GCF_SPECT_CUFFT):
+        ctx = G.Context(0, 512, 0)
+        ctx.set_spectrum_impl(impl)
+        ctx.setup(G.make_optics(pixel_size=PX), 1536, 1536)
+        ctx.gen_half_spectrum(img)
+        graw = ctx.half_spectrum(raw=True).astype(np.float64)
+        g = ctx.half_spectrum(raw=False).astype(np.float64)
+        octf, lp = oracle.ctf_spectrum(graw, 0)
+        assert lp == 1
+        rms = np.sqrt(np.mean(octf ** 2))
+        assert np.max(np.abs(g - octf)) <= 1e-4 * rms, impl
+        out[impl] = g
+        # the variance gate: a faint image keeps the background-removed spectrum
+        faint = img * np.float32(1e-4)
+        ctx.gen_half_spectrum(faint)
+        fraw = ctx.half_spectrum(raw=True).astype(np.float64)
+        fctf, flp = oracle.ctf_spectrum(fraw, 0)
+        assert flp == 0
+        f = ctx.half_spectrum(raw=False).astype(np.float64)
+        assert np.max(np.abs(f - fctf)) <= 1e-4 * np.sqrt(np.mean(fctf ** 2)), impl
+        ctx.close()
+    a, b = out[G.GCF_SPECT_FUSED], out[G.GCF_SPECT_CUFFT]
+    assert np.max(np.abs(a - b)) <= 1e-4 * np.sqrt(np.mean(b ** 2))
+
+
 def test_radial_average_matches_oracle(case, oracle):
     g_ctf = case["ctx"].half_spectrum(raw=False).astype(np.float64)
     orad = oracle.radial_average(g_ctf)
