@@ -15,7 +15,6 @@
 #include <cstring>
 #include <map>
 #include <mutex>
-#include <thread>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -1620,70 +1619,6 @@ gcf_status stage_image(gcf_ctx* ctx, const float* dimg, int w, int h, float px, 
     return GCF_OK;
 }
 
-// The rescale plans a batch will need and does not have yet, made on host
-// threads at once before the batch is enqueued (a batch at continuously
-// varying pixel sizes needs a new C2R size for almost every micrograph, and
-// making a plan is mostly host work).  Not during a capture: the plans of a
-// captured call exist already.
-gcf_status prefetch_rescale_plans(gcf_ctx* ctx, const int* ws, const int* hs, const float* pxs, int n)
-{
-    if (ctx->capturing) return GCF_OK;
-    std::vector<std::tuple<int, int, int>> need;
-    for (int i = 0; i < n; ++i) {
-        if (!(1.2f / pxs[i] > 1)) continue;
-        int nw, nh;
-        float pn;
-        gcf_rescale_dims(ws[i], hs[i], pxs[i], &nw, &nh, &pn);
-        for (auto k : {std::make_tuple(1, hs[i], ws[i]), std::make_tuple(2, nh, nw)})
-            if (!ctx->plans.count(k) && std::find(need.begin(), need.end(), k) == need.end()) need.push_back(k);
-    }
-    size_t have = 0;
-    for (auto& kv : ctx->plans) have += (std::get<0>(kv.first) == 1 || std::get<0>(kv.first) == 2);
-    if (need.size() < 4 || have + need.size() > kMaxRescalePlans) return GCF_OK;   // get_plan makes them
-    std::vector<cufftHandle> h(need.size(), 0);
-    std::vector<size_t> wsz(need.size(), 0);
-    std::vector<int> ok(need.size(), 0);
-    const int nthreads = (int)std::min<size_t>(need.size(), 8);
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthreads; ++t)
-        pool.emplace_back([&, t] {
-            if (cudaSetDevice(ctx->dev) != cudaSuccess) return;
-            for (size_t q = t; q < need.size(); q += nthreads) {
-                const int kind = std::get<0>(need[q]), a = std::get<1>(need[q]), b = std::get<2>(need[q]);
-                cufftHandle hh;
-                if (cufftCreate(&hh) != CUFFT_SUCCESS) continue;
-                if (cufftSetAutoAllocation(hh, 0) == CUFFT_SUCCESS &&
-                    cufftMakePlan2d(hh, a, b, kind == 1 ? CUFFT_R2C : CUFFT_C2R, &wsz[q]) == CUFFT_SUCCESS) {
-                    h[q] = hh;
-                    ok[q] = 1;
-                } else {
-                    cufftDestroy(hh);
-                }
-            }
-        });
-    for (auto& th : pool) th.join();
-    size_t wmax = 0;
-    for (size_t q = 0; q < need.size(); ++q)
-        if (ok[q]) wmax = std::max(wmax, wsz[q]);
-    if (wmax > ctx->fft_work.n) {
-        CK(cudaStreamSynchronize(ctx->st));
-        CK(ctx->fft_work.ensure(wmax));
-        for (auto& kv : ctx->plans)
-            if (std::get<0>(kv.first) == 1 || std::get<0>(kv.first) == 2) cufftSetWorkArea(kv.second.h, ctx->fft_work.p);
-    }
-    for (size_t q = 0; q < need.size(); ++q) {
-        if (!ok[q]) continue;   // get_plan makes it (and reports its error) when it is used
-        if (cufftSetWorkArea(h[q], ctx->fft_work.p) != CUFFT_SUCCESS || cufftSetStream(h[q], ctx->st) != CUFFT_SUCCESS) {
-            cufftDestroy(h[q]);
-            continue;
-        }
-        FftPlan& fp = ctx->plans[need[q]];
-        fp.h = h[q];
-        fp.used = ++ctx->plan_clock;
-    }
-    return GCF_OK;
-}
-
 // Images packed in one staging buffer start on 256-byte boundaries (cuFFT
 // and the vector loads of the tile kernels want aligned rows).
 size_t align_floats(size_t n) { return (n + 63) / 64 * 64; }
@@ -1707,7 +1642,6 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
     CKS(spectra_alloc(ctx, n));
     if (tot_new) CK(ctx->rescaled.ensure(tot_new));
     if (!on_device) CK(ctx->images.ensure(tot_raw));
-    if (tot_new) CKS(prefetch_rescale_plans(ctx, ws, hs, pxs, n));
     const int kChunk = on_device ? n : 8;
     const int nchunks = (n + kChunk - 1) / kChunk;
     while ((int)ctx->chunk_ev.size() < nchunks) {
