@@ -43,7 +43,7 @@ EXPORTS = [
     "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs",
     "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
     "gcf_write_ctf_file", "gcf_write_ctf_file_ex", "gcf_set_package_callback", "gcf_set_graphs",
-    "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load", "gcf_set_overlap",
+    "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load",
     "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
     "gcf_ctf_phase_shift", "gcf_ctf_defocus", "gcf_ctf_frequency", "gcf_ctf_nth_zero",
@@ -175,7 +175,6 @@ def load_library(path: str = LIB_PATH):
     L.gcf_write_ctf_file_ex.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i, i]
     L.gcf_set_package_callback.argtypes = [vp, PACKAGE_FN, vp]
     L.gcf_set_graphs.argtypes = [vp, i]
-    L.gcf_set_overlap.argtypes = [vp, i]
     L.gcf_mrc_load.argtypes = [vp, C.c_char_p, i, i, C.POINTER(vp)]
     L.gcf_autotune.argtypes = [vp, i, C.POINTER(Tuning)]
     L.gcf_get_graph_info.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -427,10 +426,6 @@ class Context:
         t = Tuning()
         _check(self.L.gcf_autotune(self._h, 1 if force else 0, C.byref(t)), self._h)
         return t.as_dict()
-
-    def set_overlap(self, clusters: int = -1):
-        """Rescale beside the tile spectra (gcf_set_overlap): -1 auto, 0 off."""
-        _check(self.L.gcf_set_overlap(self._h, int(clusters)), self._h)
 
     def set_graphs(self, on: bool = True):
         """CUDA graphs for repeated batch calls (gcf_set_graphs)."""

@@ -190,13 +190,6 @@ struct gcf_ctx {
     // device series alternate between `st` and `st_tile`, so a chunk's
     // clusters start while the previous chunk's last items finish.
     cudaStream_t st_tile = nullptr;
-    // Rescales of a device-resident batch run here, beside the tile kernel
-    // (which then holds only overlap_clusters clusters and no cluster-less
-    // CTAs): cuFFT's transforms are memory-bound and the tile FFTs are not,
-    // so they share the SMs better than they take turns.
-    cudaStream_t st_rescale = nullptr;
-    int overlap_clusters = -1;        // -1: two thirds of the resident clusters; 0: off
-    std::vector<cudaEvent_t> rs_ev;   // rescale chunk done (dependency only)
     std::vector<cudaEvent_t> chunk_ev;
     std::string err;
     long long launches = 0;
@@ -635,7 +628,6 @@ gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
                     (lru == ctx->plans.end() || q->second.used < lru->second.used))
                     lru = q;
             CK(cudaStreamSynchronize(ctx->st));
-            CK(cudaStreamSynchronize(ctx->st_rescale));
             cufftDestroy(lru->second.h);
             ctx->plans.erase(lru);
             note_device_alloc();   // a captured graph may hold the destroyed plan
@@ -647,7 +639,6 @@ gcf_status get_plan(gcf_ctx* ctx, int kind, int a, int b, cufftHandle* out)
         if (r == CUFFT_SUCCESS) r = cufftMakePlan2d(h, a, b, kind == 1 ? CUFFT_R2C : CUFFT_C2R, &ws);
         if (r == CUFFT_SUCCESS && ws > ctx->fft_work.n) {
             CK(cudaStreamSynchronize(ctx->st));
-            CK(cudaStreamSynchronize(ctx->st_rescale));
             CK(ctx->fft_work.ensure(ws));
             for (auto& kv : ctx->plans)
                 if (std::get<0>(kv.first) == 1 || std::get<0>(kv.first) == 2)
@@ -847,8 +838,7 @@ gcf_status solo_setup(gcf_ctx* ctx, SoloLaunch* sl)
     return GCF_OK;
 }
 
-gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream_t st, bool solo = true,
-                        int cap = 0)
+gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream_t st, bool solo = true)
 {
     const std::vector<int>& first = ctx->f_first_h;
     if (m0 < 0 || m1 > (int)first.size() - 1 || m0 >= m1) return fail(ctx, GCF_ERR_STATE, "tile-spectrum range outside the plan");
@@ -856,7 +846,6 @@ gcf_status fused_launch(gcf_ctx* ctx, int m0, int m1, float* raw_out, cudaStream
     int max_blocks = 0;
     for (int i = m0; i < m1; ++i) max_blocks = std::max(max_blocks, ctx->f_blocks_h[i]);
     int ncl = std::min(ctx->fused_clusters, ni);
-    if (cap > 0) ncl = std::min(ncl, cap);
     if (ctx->kev_used > 256) ctx->kev_used = 0;   // calls that never read their stage times
     while ((int)ctx->kev.size() < ctx->kev_used + 2) {
         cudaEvent_t e;
@@ -1565,10 +1554,8 @@ gcf_status set_device(gcf_ctx* ctx)
 // CRescaleImage::DoIt on the device: returns a dense new_w x new_h image
 // (FindCTF/CRescaleImage.cpp:68-99).
 gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px, float* out,
-                          int* nw_out, int* nh_out, float* px_out, bool* copied, cudaStream_t rs_st = nullptr,
-                          bool enqueue = true)
+                          int* nw_out, int* nh_out, float* px_out, bool* copied)
 {
-    if (!rs_st) rs_st = ctx->st;
     int nw, nh;
     float pxn;
     gcf_rescale_dims(w, h, px, &nw, &nh, &pxn);
@@ -1582,19 +1569,15 @@ gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px
         return GCF_OK;
     }
     *copied = true;
-    if (!enqueue) return GCF_OK;
     int cxi = w / 2 + 1, cxo = nw / 2 + 1;
     CK(ctx->rs_cmp.ensure((size_t)cxi * h));
     CK(ctx->rs_crop.ensure((size_t)cxo * nh));
     cufftHandle p1, p2;
     CKS(get_plan(ctx, 1, h, w, &p1));
     CKS(get_plan(ctx, 2, nh, nw, &p2));
-    // every rescale of a call runs on one stream (they share the scratch)
-    if (cufftSetStream(p1, rs_st) != CUFFT_SUCCESS || cufftSetStream(p2, rs_st) != CUFFT_SUCCESS)
-        return fail(ctx, GCF_ERR_CUFFT, "cufftSetStream (rescale) failed");
     if (cufftExecR2C(p1, (cufftReal*)img, (cufftComplex*)ctx->rs_cmp.p) != CUFFT_SUCCESS)
         return fail(ctx, GCF_ERR_CUFFT, "cufftExecR2C (rescale) failed");
-    launch_fourier_crop(ctx->rs_cmp.p, cxi, h, ctx->rs_crop.p, cxo, nh, rs_st);
+    launch_fourier_crop(ctx->rs_cmp.p, cxi, h, ctx->rs_crop.p, cxo, nh, ctx->st);
     CKL();
     ctx->launches += 1;
     if (cufftExecC2R(p2, (cufftComplex*)ctx->rs_crop.p, (cufftReal*)out) != CUFFT_SUCCESS)
@@ -1612,12 +1595,12 @@ bool valid_optics(const gcf_optics* o)
 // One image through CRescaleImage (FindCTF/CRescaleImage.cpp:47-99) to the
 // MicImage the spectrum stage reads.
 gcf_status stage_image(gcf_ctx* ctx, const float* dimg, int w, int h, float px, float* rescale_dst,
-                       MicImage& m, size_t* used, cudaStream_t rs_st = nullptr, bool enqueue = true)
+                       MicImage& m, size_t* used)
 {
     bool copied = false;
     int nw, nh;
     float pn;
-    CKS(rescale_device(ctx, dimg, w, h, px, rescale_dst, &nw, &nh, &pn, &copied, rs_st, enqueue));
+    CKS(rescale_device(ctx, dimg, w, h, px, rescale_dst, &nw, &nh, &pn, &copied));
     *used = 0;
     if (copied) {
         m.img = rescale_dst;
@@ -1640,72 +1623,6 @@ gcf_status stage_image(gcf_ctx* ctx, const float* dimg, int w, int h, float px, 
 // and the vector loads of the tile kernels want aligned rows).
 size_t align_floats(size_t n) { return (n + 63) / 64 * 64; }
 
-// Device images with some to rescale, fused spectrum path: the rescales run
-// on st_rescale in chunks of 16 while the tile kernel, held to `cap`
-// clusters and without its cluster-less CTAs, works through the images that
-// need no rescale and then each rescaled chunk as it lands (the SMs the
-// clusters leave run cuFFT's transforms).  The spectra are those of the
-// plain order: work items depend on the micrograph alone.
-gcf_status prepare_overlapped(gcf_ctx* ctx, const float* const* images, const int* ws, const int* hs,
-                              const float* pxs, int n, std::vector<MicImage>& mics)
-{
-    const size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
-    std::vector<size_t> dst_off(n, 0);
-    std::vector<char> rescaled(n, 0);
-    size_t roff_new = 0;
-    for (int i = 0; i < n; ++i) {   // describe only: nothing enqueued
-        size_t used = 0;
-        dst_off[i] = roff_new;
-        CKS(stage_image(ctx, images[i], ws[i], hs[i], pxs[i], ctx->rescaled.p + roff_new, mics[i], &used, nullptr,
-                        false));
-        rescaled[i] = used > 0;
-        roff_new += align_floats(used);
-    }
-    int na = 0;   // the leading run of images that need no rescale
-    while (na < n && !rescaled[na]) ++na;
-    CK(record_timing(ctx->ev[0], ctx->st));
-    CK(record_timing(ctx->ev[1], ctx->st));
-    CK(record_timing(ctx->ev[2], ctx->st));
-    CKS(fused_plan(ctx, mics));
-    if (!ctx->fork_ev) CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ctx->fork_ev, ctx->st));
-    CK(cudaStreamWaitEvent(ctx->st_rescale, ctx->fork_ev, 0));
-    const int cap = ctx->overlap_clusters > 0 ? ctx->overlap_clusters : std::max(1, ctx->fused_clusters * 2 / 3);
-    const int kRsChunk = 16;
-    const int nch = (n - na + kRsChunk - 1) / kRsChunk;
-    while ((int)ctx->rs_ev.size() < nch) {
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        ctx->rs_ev.push_back(e);
-    }
-    for (int c = 0; c < nch; ++c) {
-        const int i0 = na + c * kRsChunk, i1 = std::min(n, i0 + kRsChunk);
-        for (int i = i0; i < i1; ++i) {
-            if (!rescaled[i]) continue;
-            size_t used = 0;
-            CKS(stage_image(ctx, images[i], ws[i], hs[i], pxs[i], ctx->rescaled.p + dst_off[i], mics[i], &used,
-                            ctx->st_rescale, true));
-        }
-        CK(cudaEventRecord(ctx->rs_ev[c], ctx->st_rescale));
-    }
-    if (na > 0) CKS(fused_launch(ctx, 0, na, ctx->raw.p, ctx->st, false, cap));
-    for (int c = 0; c < nch; ++c) {
-        const int i0 = na + c * kRsChunk, i1 = std::min(n, i0 + kRsChunk);
-        CK(cudaStreamWaitEvent(ctx->st, ctx->rs_ev[c], 0));
-        CKS(fused_launch(ctx, i0, i1, ctx->raw.p + cmp_n * i0, ctx->st, false, cap));
-    }
-    CK(record_timing(ctx->ev[3], ctx->st));
-    CKS(spectra_post(ctx, n));
-    CK(record_timing(ctx->ev[4], ctx->st));
-    return GCF_OK;
-}
-
-bool overlap_applies(const gcf_ctx* ctx, int on_device, int n)
-{
-    return on_device && n > 1 && ctx->overlap_clusters != 0 && ctx->impl == GCF_SPECT_FUSED &&
-           fused_tile_supported(ctx->tile);
-}
-
 // Uploads (host inputs), rescales and produces the spectra of n images.
 // Host inputs are uploaded in chunks on a copy stream so that the upload of
 // chunk c+1 overlaps the rescale and spectrum of chunk c.
@@ -1725,7 +1642,6 @@ gcf_status prepare_images(gcf_ctx* ctx, const float* const* images, const int* w
     CKS(spectra_alloc(ctx, n));
     if (tot_new) CK(ctx->rescaled.ensure(tot_new));
     if (!on_device) CK(ctx->images.ensure(tot_raw));
-    if (tot_new && overlap_applies(ctx, on_device, n)) return prepare_overlapped(ctx, images, ws, hs, pxs, n, mics);
     const int kChunk = on_device ? n : 8;
     const int nchunks = (n + kChunk - 1) / kChunk;
     while ((int)ctx->chunk_ev.size() < nchunks) {
@@ -1889,7 +1805,6 @@ gcf_status gcf_create(int gpu, int tile_size, int log_spect, gcf_ctx** out)
         cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->st_search, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->st_tile, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->st_rescale, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->st_copy, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return GCF_ERR_CUDA;
@@ -1913,7 +1828,6 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->st_search) cudaStreamSynchronize(ctx->st_search);
     if (ctx->st_solo) cudaStreamSynchronize(ctx->st_solo);
     if (ctx->st_tile) cudaStreamSynchronize(ctx->st_tile);
-    if (ctx->st_rescale) cudaStreamSynchronize(ctx->st_rescale);
     for (auto& kv : ctx->plans) cufftDestroy(kv.second.h);
     ctx->fft_work.release();
     for (auto* b : ctx->bands) {
@@ -2016,8 +1930,6 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->solo_fork) cudaEventDestroy(ctx->solo_fork);
     if (ctx->solo_join) cudaEventDestroy(ctx->solo_join);
     if (ctx->st_tile) cudaStreamDestroy(ctx->st_tile);
-    if (ctx->st_rescale) cudaStreamDestroy(ctx->st_rescale);
-    for (auto& ev : ctx->rs_ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -2711,7 +2623,6 @@ unsigned long long batch_key(const gcf_ctx* ctx, const gcf_item* items, int n, i
     k.v(ctx->log_spect);
     k.v(ctx->fused_shape);
     k.v(ctx->fused_clusters);
-    k.v(ctx->overlap_clusters);
     k.v(ctx->gemm_bn);
     k.v(ctx->gemm_stages);
     k.v(ctx->contract_dz);
@@ -2847,27 +2758,6 @@ gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, 
         hs[i] = items[i].height;
         pxs[i] = items[i].pixel_size;
     }
-    // the overlapped spectrum path wants the images that need no rescale
-    // first: slot j holds image perm[j] (results are per micrograph and do
-    // not depend on the order)
-    std::vector<int> perm(n);
-    for (int i = 0; i < n; ++i) perm[i] = i;
-    if (overlap_applies(ctx, on_device, n)) {
-        std::stable_partition(perm.begin(), perm.end(), [&](int i) { return !(1.2f / pxs[i] > 1); });
-        std::vector<const float*> i2(n);
-        std::vector<int> w2(n), h2(n);
-        std::vector<float> p2(n);
-        for (int j = 0; j < n; ++j) {
-            i2[j] = imgs[perm[j]];
-            w2[j] = ws[perm[j]];
-            h2[j] = hs[perm[j]];
-            p2[j] = pxs[perm[j]];
-        }
-        imgs.swap(i2);
-        ws.swap(w2);
-        hs.swap(h2);
-        pxs.swap(p2);
-    }
     CKS(set_device(ctx));
     for (float& t : ctx->stage_ms) t = 0.0f;
     for (long long& c : ctx->search_counts) c = 0;
@@ -2927,7 +2817,7 @@ gcf_status batch_run(gcf_ctx* ctx, const gcf_item* items, int n, int on_device, 
         std::vector<gcf_result> r;
         st = search_collect(ctx, pxn, mode == GCF_SEARCH_PLAIN ? pxs.data() : nullptr, *optics, mode, pend, r);
         if (st == GCF_OK)
-            for (int j = 0; j < n; ++j) results[perm[j]] = r[j];
+            for (int i = 0; i < n; ++i) results[i] = r[i];
     }
     cudaEventRecord(t1, ctx->st);
     cudaEventSynchronize(t1);
@@ -3182,13 +3072,6 @@ gcf_status gcf_mrc_load(gcf_ctx* ctx, const char* path, int z0, int n, const flo
     cudaError_t e = cudaStreamSynchronize(ctx->st);
     if (st == GCF_OK && e != cudaSuccess) st = cuda_fail(ctx, e, "mrc load");
     return st;
-}
-
-gcf_status gcf_set_overlap(gcf_ctx* ctx, int clusters)
-{
-    if (!ctx || clusters < -1) return GCF_ERR_INVALID_ARG;
-    ctx->overlap_clusters = clusters;
-    return GCF_OK;
 }
 
 gcf_status gcf_set_graphs(gcf_ctx* ctx, int on)

@@ -287,16 +287,6 @@ gcf_status gcf_nn_get_params(gcf_ctx* ctx, float* params, size_t n);
 /* Weights file: 8-byte tag "GCFNN001", the count (uint64), FP32 params. */
 gcf_status gcf_nn_save(gcf_ctx* ctx, const char* path);
 gcf_status gcf_nn_load(gcf_ctx* ctx, const char* path);
-/* Rescale beside the tile spectra in batch calls with device images: the
- * micrographs below 1.2 A/px are rescaled (cuFFT) on a second stream while
- * the fused tile kernel, held to `clusters` thread-block clusters, works
- * through the others and then each rescaled group as it lands.  -1 (the
- * default): two thirds of the clusters the device holds; 0: off (all
- * rescales first, then one tile launch on the whole GPU).  Results do not
- * depend on it.  No counterpart in the reference, which rescales and
- * transforms one micrograph at a time (CFindSeriesCtfs.cpp:62-92). */
-gcf_status gcf_set_overlap(gcf_ctx* ctx, int clusters);
-
 /* CUDA graphs for batch calls (gcf_run_batch, gcf_run_batch_mode), off by
  * default.  With graphs on, a call that repeats an earlier call's inputs
  * (the same image buffers, sizes, pixel sizes, optics and method; device

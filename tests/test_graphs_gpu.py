@@ -136,28 +136,3 @@ def test_autotune_picks_the_fastest_trial_and_keeps_results(gpu_lib):
         assert abs(x.score - y.score) <= 2e-3
     ctx.close()
     ref_ctx.close()
-
-
-def test_overlapped_rescale_gives_the_serial_results(gpu_lib):
-    """gcf_set_overlap: rescaling on a second stream beside a tile kernel held
-    to fewer clusters (default, and 4 clusters) gives the results of the
-    serial order (all rescales, then one tile launch) bit for bit and in the
-    caller's order, for the plain and the BF16 search, eager and replayed."""
-    G = gpu_lib
-    specs = _specs(9, 61)
-    pxs = [s.pixel_size for s in specs]
-    assert any(p < 1.2 for p in pxs) and any(p >= 1.2 for p in pxs)
-    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
-    op = G.make_optics()
-    ref_ctx = G.Context(0, 512, 0)
-    ref_ctx.set_overlap(0)
-    for mode in (G.GCF_SEARCH_PLAIN, G.GCF_SEARCH_BF16):
-        ref = ref_ctx.run_batch(imgs, pxs, op, mode=mode)
-        for clusters in (-1, 4):
-            ctx = G.Context(0, 512, 0)
-            ctx.set_overlap(clusters)
-            ctx.set_graphs(True)
-            for _ in range(3):   # eager, captured, replayed
-                assert _same(ctx.run_batch(imgs, pxs, op, mode=mode), ref), (mode, clusters)
-            ctx.close()
-    ref_ctx.close()
