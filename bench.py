@@ -558,6 +558,9 @@ def main():
     torch.cuda.nvtx.range_pop()
     # ---- plain FP32 search: batched, and single-file mode ----
     plain = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_PLAIN, args.steps, min(args.warmup, 2), world)
+    # ---- the contraction search without the network (what the network saves) ----
+    nonet = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_BF16, args.steps, min(args.warmup, 2), world) \
+        if learned else None
     single_ms, single_wall = timed_single_file(ctx, imgs, pxs, op, max(1, min(args.steps, 2)), world)
     # ---- end to end: pinned host inputs, host clock around the call ----
     host = [im.cpu().pin_memory() for im in imgs]
@@ -604,6 +607,13 @@ def main():
                                               "device time summed over the calls"}},
             "speedup": {"vs_plain_single_file": round(single_ms / fast["ms"], 3),
                         "vs_plain_batched": round(plain["ms"] / fast["ms"], 3)},
+            "bf16_without_network": None if nonet is None else {
+                "value": round(world * n / (nonet["ms"] / 1000.0), 2), "ms_per_step": round(nonet["ms"], 3),
+                "search_ms": round(nonet["stage"].get("search1d", 0.0) + nonet["stage"].get("search2d", 0.0), 3),
+                "table_candidates": nonet["fast_counts"].get("table_cand"),
+                "tensor_macs": nonet["fast_counts"].get("tensor_macs"),
+                "note": "the same batch through the contraction search without the learned window; the "
+                        "headline's own search_ms is search1d + search2d of stage_ms_per_step"},
             "defocus_error": defocus_error(fast["results"], plain["results"], specs),
             "stage_ms_per_step": {k: round(v, 3) for k, v in fast["stage"].items()},
             "contraction": {"stage_ms": {k: round(v, 3) for k, v in ft.items()}, "counts": fc,

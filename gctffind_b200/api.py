@@ -43,7 +43,7 @@ EXPORTS = [
     "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs",
     "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
     "gcf_write_ctf_file", "gcf_write_ctf_file_ex", "gcf_set_package_callback", "gcf_set_graphs",
-    "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load",
+    "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load", "gcf_gemm_bf16_ex",
     "gcf_ctf_setup", "gcf_ctf_set_ext_phase", "gcf_ctf_get_ext_phase", "gcf_ctf_set_defocus",
     "gcf_ctf_set_defocus_px", "gcf_ctf_change_pixel_size", "gcf_ctf_evaluate",
     "gcf_ctf_phase_shift", "gcf_ctf_defocus", "gcf_ctf_frequency", "gcf_ctf_nth_zero",
@@ -86,14 +86,14 @@ class CtfParam(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("fused_shape", C.c_int), ("gemm_tile_n", C.c_int), ("gemm_stages", C.c_int),
-                ("fused_ms", C.c_float * 4), ("gemm_ms", C.c_float * 6)]
+                ("gemm_persistent", C.c_int), ("fused_ms", C.c_float * 4), ("gemm_ms", C.c_float * 10)]
 
     def as_dict(self):
         return {"fused_shape": self.fused_shape, "gemm_tile_n": self.gemm_tile_n,
-                "gemm_stages": self.gemm_stages,
+                "gemm_stages": self.gemm_stages, "gemm_persistent": self.gemm_persistent,
                 "fused_ms": dict(zip(["8", "816", "16", "162"], [round(x, 4) for x in self.fused_ms])),
-                "gemm_ms": dict(zip(["256x2", "256x3", "256x4", "128x4", "128x6", "64x4"],
-                                    [round(x, 4) for x in self.gemm_ms]))}
+                "gemm_ms": dict(zip(["256x2", "256x3", "256x4", "128x4", "128x6", "64x4", "p256x3", "p256x4",
+                                     "p128x4", "p128x6"], [round(x, 4) for x in self.gemm_ms]))}
 
 
 class Item(C.Structure):
@@ -155,6 +155,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_avg_spectrum_noalloc.argtypes = [vp, i, i, i, vp, vp]
     ll = C.c_longlong
     L.gcf_gemm_bf16.argtypes = [vp, ll, vp, ll, i, i, i, vp, ll, i, i, vp]
+    L.gcf_gemm_bf16_ex.argtypes = [vp, ll, vp, ll, i, i, i, vp, ll, i, i, i, vp]
     L.gcf_run_batch_mode.argtypes = [vp, C.POINTER(Item), i, i, C.POINTER(Optics), i, C.POINTER(Result)]
     L.gcf_get_fast_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gcf_get_fast_times.argtypes = [vp, C.POINTER(f)]

@@ -282,6 +282,7 @@ struct gcf_ctx {
     DBuf<int> cNtiles, cErr;
     DBuf<float4> cPrior;
     int gemm_bn = 256, gemm_stages = 4;     // tile of the P product (tuned)
+    int gemm_persistent = 0;                // P product by the persistent kernel (tuned)
     float contract_dz = 10.0f;              // defocus row step, Angstrom
     int contract_ns = 512, contract_nth = 64;
     // [0] candidates scored on the table, [1] tensor-core multiply-adds,
@@ -1320,7 +1321,11 @@ gcf_status run_fast_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, con
     ga.tiles = ctx->cTiles.p;
     ga.ntiles = ctx->cNtiles.p;
     ga.err = ctx->cErr.p;
-    CK(launch_umma_gemm(ctx->cA.p, g.ns, ctx->cB.p, g.ns, ga, bn, ctx->gemm_stages, max_tiles, ctx->st));
+    if (ctx->gemm_persistent)
+        CK(launch_umma_gemm_persistent(ctx->cA.p, g.ns, ctx->cB.p, g.ns, ga, bn, ctx->gemm_stages, max_tiles,
+                                       ctx->st));
+    else
+        CK(launch_umma_gemm(ctx->cA.p, g.ns, ctx->cB.p, g.ns, ga, bn, ctx->gemm_stages, max_tiles, ctx->st));
     GemmArgs gd;
     gd.M = nj;
     gd.N = g.nz;
@@ -2625,6 +2630,7 @@ unsigned long long batch_key(const gcf_ctx* ctx, const gcf_item* items, int n, i
     k.v(ctx->fused_clusters);
     k.v(ctx->gemm_bn);
     k.v(ctx->gemm_stages);
+    k.v(ctx->gemm_persistent);
     k.v(ctx->contract_dz);
     k.v(ctx->contract_ns);
     k.v(ctx->contract_nth);
@@ -2869,7 +2875,9 @@ struct TuneCache {
 std::mutex g_tune_mu;
 TuneCache g_tune[64];
 constexpr int kTuneShapes[4] = {8, 816, 16, 162};
-constexpr int kTuneGemm[6][2] = {{256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {64, 4}};
+// (tile N, stages, persistent)
+constexpr int kTuneGemm[10][3] = {{256, 2, 0}, {256, 3, 0}, {256, 4, 0}, {128, 4, 0}, {128, 6, 0},
+                                  {64, 4, 0},  {256, 3, 1}, {256, 4, 1}, {128, 4, 1}, {128, 6, 1}};
 
 // Best of three timed runs after one warm-up of `run` on ctx->st, in ms.
 template <class F>
@@ -2940,8 +2948,8 @@ gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b
         CKL();
         CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->st));
         float best = 1e30f;
-        for (int q = 0; q < 6; ++q) {
-            const int bn = kTuneGemm[q][0], stages = kTuneGemm[q][1];
+        for (int q = 0; q < 10; ++q) {
+            const int bn = kTuneGemm[q][0], stages = kTuneGemm[q][1], pers = kTuneGemm[q][2];
             if (bn < ctx->contract_nth || bn % ctx->contract_nth) {
                 t.gemm_ms[q] = -1.0f;
                 continue;
@@ -2955,7 +2963,8 @@ gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b
             g.err = err.p;
             float ms = 0.0f;
             CKS(time_trial(ctx, a, b, [&]() -> gcf_status {
-                CK(launch_umma_gemm(A.p, K, B.p, K, g, bn, stages, 0, ctx->st));
+                if (pers) CK(launch_umma_gemm_persistent(A.p, K, B.p, K, g, bn, stages, 0, ctx->st));
+                else CK(launch_umma_gemm(A.p, K, B.p, K, g, bn, stages, 0, ctx->st));
                 return GCF_OK;
             }, &ms));
             t.gemm_ms[q] = ms;
@@ -2963,6 +2972,7 @@ gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b
                 best = ms;
                 t.gemm_tile_n = bn;
                 t.gemm_stages = stages;
+                t.gemm_persistent = pers;
             }
         }
         int h = 0;
@@ -3004,6 +3014,7 @@ gcf_status gcf_autotune(gcf_ctx* ctx, int force, gcf_tuning* out)
     if (C.t.gemm_tile_n) {
         ctx->gemm_bn = C.t.gemm_tile_n;
         ctx->gemm_stages = C.t.gemm_stages;
+        ctx->gemm_persistent = C.t.gemm_persistent;
     }
     if (out) *out = C.t;
     return GCF_OK;

@@ -262,6 +262,11 @@ struct GemmArgs {
 int umma_tile_n_supported(int bn);
 cudaError_t launch_umma_gemm(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B, long long ldb,
                              GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st);
+// The same product by one persistent CTA per SM over all tiles, the
+// accumulator double-buffered in tensor memory (pairs 256 x 3/4, 128 x 4/6,
+// 64 x 4, 32 x 4).
+cudaError_t launch_umma_gemm_persistent(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B,
+                                        long long ldb, GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st);
 
 // gcf_contract.cu: the BF16 candidate contraction.
 // Common polar grid of a batch: ns bins uniform in s^2 (1/A^2) over the

@@ -17,6 +17,10 @@
 // a swizzled shared-memory stage into coalesced global stores, with an
 // optional bias, ReLU, BF16 conversion and transposed copy.
 //
+// k_umma_gemm_persistent (below) is the same product for many tiles: one CTA
+// per SM walks the tile list, with the accumulator double-buffered in tensor
+// memory so that each tile's epilogue overlaps the next tile's MMAs.
+//
 // Every wait is bounded (about one second of global timer): a wait that runs
 // out records an error code in *err, the roles stop issuing work, the
 // producer waits (bounded) for the loads it has in flight, and the CTA frees
@@ -153,6 +157,88 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// One warp's 32 rows of a 128 x BN accumulator in tensor memory (columns
+// from tacc, the warp's lane quarter q) to global memory: bias, ReLU, and any
+// of the FP32 (through a swizzled 4 KB shared-memory stage, 4 rows x 128 B
+// per store), BF16 and transposed BF16 outputs.  write = false only drains
+// the tensor-memory loads.
+template <int BN>
+__device__ __forceinline__ void store_accumulator(const GemmArgs& g, uint32_t tacc, int q, int lane, int m0, int n0,
+                                                  unsigned char* sb, bool write)
+{
+    const int row0 = m0 + 32 * q;
+#pragma unroll 1
+    for (int c = 0; c < BN / 32; ++c) {
+        uint32_t v[32];
+        tmem_ld32(tacc + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
+        if (!write) continue;
+        const int col0 = n0 + 32 * c;
+        float f[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            float x = __uint_as_float(v[i]);
+            if (g.bias) {
+                const int n = col0 + i;
+                x += (n < g.N) ? g.bias[n] : 0.0f;
+            }
+            if (g.relu) x = fmaxf(x, 0.0f);
+            f[i] = x;
+        }
+        const int myrow = row0 + lane;
+        if (g.Dt) {
+            // transposed BF16 copy: Dt[n][m]; lanes are consecutive m
+            if (myrow < g.M) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int n = col0 + i;
+                    if (n < g.N) g.Dt[(size_t)n * g.ldt + myrow] = __float2bfloat16_rn(f[i]);
+                }
+            }
+        }
+        if (g.Db) {
+            // BF16 row-major copy
+            if (myrow < g.M) {
+                __nv_bfloat16* dst = g.Db + (size_t)myrow * g.ldd + col0;
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (col0 + i < g.N) dst[i] = __float2bfloat16_rn(f[i]);
+            }
+        }
+        if (g.D) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float4 t = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                *reinterpret_cast<float4*>(sb + lane * 128 + ((j ^ (lane & 7)) << 4)) = t;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int r = 4 * i + (lane >> 3), j = lane & 7;
+                float4 t = *reinterpret_cast<const float4*>(sb + r * 128 + ((j ^ (r & 7)) << 4));
+                const int m = row0 + r, n = col0 + 4 * j;
+                if (m < g.M) {
+                    float* dst = g.D + (size_t)m * g.ldd + n;
+                    if (n + 3 < g.N && g.vec4) {
+                        if (g.accumulate) {
+                            float4 o = *reinterpret_cast<float4*>(dst);
+                            t.x += o.x;
+                            t.y += o.y;
+                            t.z += o.z;
+                            t.w += o.w;
+                        }
+                        *reinterpret_cast<float4*>(dst) = t;
+                    } else {
+                        const float e[4] = {t.x, t.y, t.z, t.w};
+                        for (int u = 0; u < 4; ++u)
+                            if (n + u < g.N) dst[u] = g.accumulate ? dst[u] + e[u] : e[u];
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 template <int BN, int STAGES>
 struct GemmSmem {
     static constexpr int kA = kBM * kBK * 2;       // 16 KB per stage
@@ -258,90 +344,187 @@ k_umma_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
     }
     __syncwarp();
 
-    // epilogue: all four warps
-    const bool ok = mbar_wait(done_bar, 0);
-    if (!ok) atomicExch(g.err, 3);
+    // epilogue: all four warps (the tensor-memory loads are warp-wide
+    // .sync.aligned instructions: every decision before them is made
+    // uniform across the warp)
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(done_bar, 0));
+    if (!ok && lane == 0) atomicExch(g.err, 3);
     tc_fence_after();
     __syncthreads();   // every role is past its loop: the ring's shared memory is free
-    const bool write = ok && !*(volatile int*)s_abort;
-    float* stage = reinterpret_cast<float*>(smem + warp * 4096);   // 32 rows x 128 B per warp
-    const int row0 = m0 + 32 * warp;
-#pragma unroll 1
-    for (int c = 0; c < BN / 32; ++c) {
-        uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * c), v);
-        if (!write) continue;
-        const int col0 = n0 + 32 * c;
-        float f[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-            float x = __uint_as_float(v[i]);
-            if (g.bias) {
-                const int n = col0 + i;
-                x += (n < g.N) ? g.bias[n] : 0.0f;
-            }
-            if (g.relu) x = fmaxf(x, 0.0f);
-            f[i] = x;
-        }
-        const int myrow = row0 + lane;
-        if (g.Dt) {
-            // transposed BF16 copy: Dt[n][m]; lanes are consecutive m
-            if (myrow < g.M) {
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int n = col0 + i;
-                    if (n < g.N) g.Dt[(size_t)n * g.ldt + myrow] = __float2bfloat16_rn(f[i]);
-                }
-            }
-        }
-        if (g.Db) {
-            // BF16 row-major copy
-            if (myrow < g.M) {
-                __nv_bfloat16* dst = g.Db + (size_t)myrow * g.ldd + col0;
-#pragma unroll
-                for (int i = 0; i < 32; ++i)
-                    if (col0 + i < g.N) dst[i] = __float2bfloat16_rn(f[i]);
-            }
-        }
-        if (g.D) {
-            // FP32: swizzled shared-memory stage, then 4 rows x 128 B per store
-            unsigned char* sb = reinterpret_cast<unsigned char*>(stage);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                float4 q = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
-                *reinterpret_cast<float4*>(sb + lane * 128 + ((j ^ (lane & 7)) << 4)) = q;
-            }
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int r = 4 * i + (lane >> 3), j = lane & 7;
-                float4 q = *reinterpret_cast<const float4*>(sb + r * 128 + ((j ^ (r & 7)) << 4));
-                const int m = row0 + r, n = col0 + 4 * j;
-                if (m < g.M) {
-                    float* dst = g.D + (size_t)m * g.ldd + n;
-                    if (n + 3 < g.N && g.vec4) {
-                        if (g.accumulate) {
-                            float4 o = *reinterpret_cast<float4*>(dst);
-                            q.x += o.x;
-                            q.y += o.y;
-                            q.z += o.z;
-                            q.w += o.w;
-                        }
-                        *reinterpret_cast<float4*>(dst) = q;
-                    } else {
-                        const float e[4] = {q.x, q.y, q.z, q.w};
-                        for (int u = 0; u < 4; ++u)
-                            if (n + u < g.N) dst[u] = g.accumulate ? dst[u] + e[u] : e[u];
-                    }
-                }
-            }
-            __syncwarp();
-        }
-    }
+    const bool write = __all_sync(0xffffffffu, ok && !*(volatile int*)s_abort);
+    store_accumulator<BN>(g, tmem, warp, lane, m0, n0, smem + warp * 4096, write);
     tc_fence_before();
     __syncthreads();
     if (warp == 2)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Persistent variant for products of many tiles (the contraction table): one
+// CTA per SM walks the tile list with a stride of the grid, and the
+// accumulator is double-buffered in tensor memory (2 x BN columns), so the
+// epilogue of one tile overlaps the MMAs of the next and the TMA loads of
+// the one after.  Six warps: warp 0 lane 0 the TMA producer (one ring of K
+// slices across all of the CTA's tiles), warp 1 the tensor-memory
+// allocation and lane 0 of it the MMA issuer, warps 2-5 the epilogue (warp w
+// reads tensor-memory lanes 32 (w mod 4) .. +31, i.e. those rows of the tile).
+// Hand-offs: full/empty per ring slot, acc_full/acc_empty per accumulator
+// buffer; every wait bounded as in k_umma_gemm.
+constexpr int kPThreads = 192;
+
+template <int BN, int STAGES>
+struct PGemmSmem {
+    static constexpr int kA = kBM * kBK * 2;
+    static constexpr int kB = BN * kBK * 2;
+    static constexpr int kStage = kA + kB;
+    static constexpr int kEpi = 4 * 4096;          // four epilogue warps' stages
+    static constexpr int kBars = 1024;
+    static constexpr int kBytes = 1024 + STAGES * kStage + kEpi + kBars;
+};
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(kPThreads, 1)
+k_umma_gemm_persistent(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g,
+                       int ntiles_grid)
+{
+    using L = PGemmSmem<BN, STAGES>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + STAGES * L::kA;
+    unsigned char* sEpi = smem + STAGES * L::kStage;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sEpi + L::kEpi);
+    // [0, S): slice loaded; [S, 2S): slice consumed; 2S, 2S+1: accumulator b
+    // full; 2S+2, 2S+3: accumulator b drained
+    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
+    int* s_abort = reinterpret_cast<int*>(s_taddr + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = g.ntiles ? *g.ntiles : ntiles_grid;
+    const int gn = (g.N + BN - 1) / BN;   // column tiles of the whole grid
+    const int nkb = (g.K + kBK - 1) / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2 * STAGES + 2; ++i) mbar_init(smem_u32(bars + i), 1);
+        mbar_init(smem_u32(bars + 2 * STAGES + 2), 4);
+        mbar_init(smem_u32(bars + 2 * STAGES + 3), 4);
+        *s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_taddr)),
+                     "r"(2 * BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_taddr;
+    volatile int* abort_flag = s_abort;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+            int m0, n0;
+            if (g.tiles) {
+                const int2 tt = g.tiles[t];
+                m0 = tt.x;
+                n0 = tt.y;
+            } else {
+                m0 = (t / gn) * kBM;
+                n0 = (t % gn) * BN;
+            }
+            for (int kb = 0; kb < nkb; ++kb, ++it) {
+                const int s = it % STAGES;
+                if (it >= STAGES && !mbar_wait(smem_u32(bars + STAGES + s), ((it / STAGES) & 1) ^ 1)) {
+                    atomicExch(g.err, 1);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                const uint32_t fb = smem_u32(bars + s);
+                mbar_expect_tx(fb, L::kStage);
+                tma_load_2d(smem_u32(sA + s * L::kA), &ta, fb, kb * kBK, m0);
+                tma_load_2d(smem_u32(sB + s * L::kB), &tb, fb, kb * kBK, n0);
+            }
+        }
+        // on an abort, the loads still in flight land before the CTA exits
+        if (*abort_flag)
+            for (int j = (it > STAGES ? it - STAGES : 0); j < it; ++j)
+                mbar_wait(smem_u32(bars + (j % STAGES)), (j / STAGES) & 1);
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        constexpr uint32_t idesc = idesc_bf16(BN);
+        int it = 0, i = 0;
+        for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++i) {
+            const int b = i & 1, use = i >> 1;
+            if (use > 0 && !mbar_wait(smem_u32(bars + 2 * STAGES + 2 + b), (use - 1) & 1)) {
+                atomicExch(g.err, 4);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t tacc = tmem + (uint32_t)(b * BN);
+            bool bad = false;
+            for (int kb = 0; kb < nkb; ++kb, ++it) {
+                const int s = it % STAGES;
+                if (!mbar_wait(smem_u32(bars + s), (it / STAGES) & 1)) {
+                    atomicExch(g.err, 2);
+                    *abort_flag = 1;
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t da = desc_k128(smem_u32(sA + s * L::kA));
+                const uint64_t db = desc_k128(smem_u32(sB + s * L::kB));
+#pragma unroll
+                for (int k = 0; k < kBK / kUK; ++k)
+                    umma(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb > 0 || k > 0) ? 1u : 0u);
+                umma_commit(smem_u32(bars + STAGES + s));
+            }
+            umma_commit(smem_u32(bars + 2 * STAGES + b));   // accumulator b complete (or abandoned)
+            if (bad) break;
+        }
+    } else if (warp >= 2) {
+        // epilogue warps
+        const int q = warp & 3;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            // warp-uniform decisions: the tensor-memory loads are .sync.aligned
+            if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
+            const int b = i & 1, use = i >> 1;
+            if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(bars + 2 * STAGES + b), use & 1))) {
+                if (lane == 0) {
+                    atomicExch(g.err, 3);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            int m0, n0;
+            if (g.tiles) {
+                const int2 tt = g.tiles[t];
+                m0 = tt.x;
+                n0 = tt.y;
+            } else {
+                m0 = (t / gn) * kBM;
+                n0 = (t % gn) * BN;
+            }
+            const bool wr = !__any_sync(0xffffffffu, *abort_flag != 0);
+            store_accumulator<BN>(g, tmem + (uint32_t)(b * BN), q, lane, m0, n0, sEpi + (warp - 2) * 4096, wr);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bars + 2 * STAGES + 2 + b))
+                                        : "memory");
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -397,9 +580,54 @@ cudaError_t launch_bn(const CUtensorMap& ta, const CUtensorMap& tb, const GemmAr
     return cudaGetLastError();
 }
 
+template <int BN, int STAGES>
+cudaError_t launch_pbn(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int ntiles, cudaStream_t st)
+{
+    using L = PGemmSmem<BN, STAGES>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(k_umma_gemm_persistent<BN, STAGES>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int grid_tiles = ((g.M + kBM - 1) / kBM) * ((g.N + BN - 1) / BN);
+    const int total = g.tiles ? ntiles : grid_tiles;   // an upper bound with a device tile count
+    const int grid = std::max(1, std::min(total, sms));
+    k_umma_gemm_persistent<BN, STAGES><<<grid, kPThreads, L::kBytes, st>>>(ta, tb, g, grid_tiles);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int umma_tile_n_supported(int bn) { return bn == 32 || bn == 64 || bn == 128 || bn == 256; }
+
+cudaError_t launch_umma_gemm_persistent(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B,
+                                        long long ldb, GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st)
+{
+    if (!umma_tile_n_supported(bn) || g.M <= 0 || g.N <= 0 || g.K <= 0 || !g.err) return cudaErrorInvalidValue;
+    if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (lda * 2) % 16 || (ldb * 2) % 16 || lda < g.K || ldb < g.K)
+        return cudaErrorInvalidValue;
+    if (g.tiles && ntiles <= 0) return cudaSuccess;
+    g.vec4 = (g.D && ((uintptr_t)g.D & 15) == 0 && g.ldd % 4 == 0) ? 1 : 0;
+    CUtensorMap ta, tb;
+    cudaError_t e;
+    if ((e = make_map(&ta, A, g.M, g.K, lda, kBM)) != cudaSuccess) return e;
+    if ((e = make_map(&tb, B, g.N, g.K, ldb, bn)) != cudaSuccess) return e;
+    switch (bn * 10 + stages) {
+    case 2563: return launch_pbn<256, 3>(ta, tb, g, ntiles, st);
+    case 2564: return launch_pbn<256, 4>(ta, tb, g, ntiles, st);
+    case 1284: return launch_pbn<128, 4>(ta, tb, g, ntiles, st);
+    case 1286: return launch_pbn<128, 6>(ta, tb, g, ntiles, st);
+    case 644: return launch_pbn<64, 4>(ta, tb, g, ntiles, st);
+    case 324: return launch_pbn<32, 4>(ta, tb, g, ntiles, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_umma_gemm(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B, long long ldb,
                              GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st)
@@ -437,8 +665,9 @@ namespace {
 __device__ int g_umma_err_flag;
 }
 
-extern "C" gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b, long long ldb, int m, int n,
-                                    int k, float* d, long long ldd, int tile_n, int stages, void* cuda_stream)
+extern "C" gcf_status gcf_gemm_bf16_ex(const void* a, long long lda, const void* b, long long ldb, int m, int n,
+                                       int k, float* d, long long ldd, int tile_n, int stages, int persistent,
+                                       void* cuda_stream)
 {
     using namespace gcf;
     if (!a || !b || !d || m <= 0 || n <= 0 || k <= 0 || ldd < n) return GCF_ERR_INVALID_ARG;
@@ -453,8 +682,11 @@ extern "C" gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b,
     g.D = d;
     g.ldd = ldd;
     g.err = flag;
-    cudaError_t e = launch_umma_gemm(static_cast<const __nv_bfloat16*>(a), lda, static_cast<const __nv_bfloat16*>(b),
-                                     ldb, g, tile_n, stages, 0, st);
+    cudaError_t e = persistent ? launch_umma_gemm_persistent(static_cast<const __nv_bfloat16*>(a), lda,
+                                                             static_cast<const __nv_bfloat16*>(b), ldb, g, tile_n,
+                                                             stages, 0, st)
+                               : launch_umma_gemm(static_cast<const __nv_bfloat16*>(a), lda,
+                                                  static_cast<const __nv_bfloat16*>(b), ldb, g, tile_n, stages, 0, st);
     if (e == cudaErrorInvalidValue) return GCF_ERR_INVALID_ARG;
     if (e != cudaSuccess) return GCF_ERR_CUDA;
     int hflag = 0;
@@ -462,4 +694,10 @@ extern "C" gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b,
         cudaStreamSynchronize(st) != cudaSuccess)
         return GCF_ERR_CUDA;
     return hflag ? GCF_ERR_TIMEOUT : GCF_OK;
+}
+
+extern "C" gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b, long long ldb, int m, int n,
+                                    int k, float* d, long long ldd, int tile_n, int stages, void* cuda_stream)
+{
+    return gcf_gemm_bf16_ex(a, lda, b, ldb, m, n, k, d, ldd, tile_n, stages, 0, cuda_stream);
 }

@@ -309,8 +309,10 @@ typedef struct {
     int fused_shape;     /* tile-kernel cluster shape picked: 8, 816, 16 or 162 */
     int gemm_tile_n;     /* contraction product tile picked: 128 x gemm_tile_n */
     int gemm_stages;     /* its load-pipeline depth */
+    int gemm_persistent; /* 1: the persistent product (gcf_gemm_bf16_ex) */
     float fused_ms[4];   /* trial ms of shapes 8, 816, 16, 162 (-1: cannot be resident) */
-    float gemm_ms[6];    /* trial ms of (256,2) (256,3) (256,4) (128,4) (128,6) (64,4) */
+    float gemm_ms[10];   /* trial ms of (256,2) (256,3) (256,4) (128,4) (128,6) (64,4) one tile per
+                            CTA, then (256,3) (256,4) (128,4) (128,6) persistent */
 } gcf_tuning;
 gcf_status gcf_autotune(gcf_ctx* ctx, int force, gcf_tuning* out);
 
@@ -411,6 +413,12 @@ gcf_status gcf_write_ctf_file_ex(const char* path, const gcf_result* results, co
  * device and waits for it; GCF_ERR_TIMEOUT if a bounded device wait gave up. */
 gcf_status gcf_gemm_bf16(const void* a, long long lda, const void* b, long long ldb, int m, int n, int k,
                          float* d, long long ldd, int tile_n, int stages, void* cuda_stream);
+/* gcf_gemm_bf16 with persistent = 1: one CTA per SM walks all output tiles
+ * and double-buffers the accumulator in tensor memory, so each tile's
+ * epilogue overlaps the next tile's MMAs (pairs 256 x 3/4, 128 x 4/6,
+ * 64 x 4, 32 x 4).  Same results as persistent = 0. */
+gcf_status gcf_gemm_bf16_ex(const void* a, long long lda, const void* b, long long ldb, int m, int n, int k,
+                            float* d, long long ldd, int tile_n, int stages, int persistent, void* cuda_stream);
 
 /* ---------------------------------------------------------------------- */
 /* Allocation-free spectrum.  No counterpart in the reference.              */

@@ -73,3 +73,36 @@ def test_gemm_rejects_unaligned(gpu_lib):
     assert L.gcf_gemm_bf16(p, 70, p, 72, 128, 128, 70, C.c_void_p(d.data_ptr()), 128, 128, 2, None) == 1
     # unsupported tile width
     assert L.gcf_gemm_bf16(p, 72, p, 72, 128, 128, 64, C.c_void_p(d.data_ptr()), 128, 96, 2, None) == 1
+
+
+PCONFIGS = [(256, 3), (256, 4), (128, 4), (128, 6), (64, 4), (32, 4)]
+
+
+def _run_ex(L, a, b, tile_n, stages, persistent):
+    import torch
+    m, k = a.shape
+    n = b.shape[0]
+    d = torch.full((m, n), float("nan"), dtype=torch.float32, device="cuda")
+    st = L.gcf_gemm_bf16_ex(C.c_void_p(a.data_ptr()), a.stride(0), C.c_void_p(b.data_ptr()), b.stride(0),
+                            m, n, k, C.c_void_p(d.data_ptr()), d.stride(0), tile_n, stages, persistent, None)
+    assert st == 0, L.gcf_strerror(st)
+    return d
+
+
+@pytest.mark.parametrize("tile_n,stages", PCONFIGS)
+def test_persistent_gemm_matches_fp32_and_one_tile_per_cta(gpu_lib, tile_n, stages):
+    """The persistent variant (one CTA per SM over all tiles, accumulator
+    double-buffered in tensor memory) against the FP32 reference, on shapes
+    with fewer tiles than SMs, with several tiles per CTA (both accumulator
+    buffers reused) and ragged edges; it equals the one-tile-per-CTA kernel
+    bit for bit (same MMAs, same accumulation order)."""
+    import torch
+    L = gpu_lib.load_library()
+    g = torch.Generator(device="cuda").manual_seed(tile_n + stages)
+    for (m, n, k) in [(256, 512, 512), (300, 200, 72), (2048, 4096, 512), (1100, 1000, 264)]:
+        a = torch.randn((m, k), generator=g, device="cuda").to(torch.bfloat16)
+        b = torch.randn((n, k), generator=g, device="cuda").to(torch.bfloat16)
+        dp = _run_ex(L, a, b, tile_n, stages, 1)
+        _check(a, b, dp)
+        if (tile_n, stages) in CONFIGS:
+            assert torch.equal(dp, _run(L, a, b, tile_n, stages))
