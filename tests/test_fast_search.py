@@ -4,7 +4,7 @@ the plain FP32 search (GCF_SEARCH_PLAIN) of the same batch.
 The contraction scores every candidate of every micrograph on a BF16
 tensor-core table, so its optimum may sit a little off the plain search's;
 the FP32 re-score and local passes then refine on each micrograph's own
-band.  Accuracy bar (the north star's): defocus within one search step of the
+band.  Accuracy bar: defocus within one search step of the
 plain path's last mean-defocus line search (max(20 A, 0.105 * mean / 31))
 for at least 99 % of micrographs -- here every one of the batch -- with a
 median |d defocus| <= 20 A; azimuth within 2 degrees (mod 180) where the

@@ -1,7 +1,7 @@
 """CPU: the FP64 restatement of the learned initialiser's network
 (oracle/nn_oracle.py) against central finite differences of its own loss,
 on a small batch with unrounded weights -- the check that pins the oracle
-before it judges the library's BF16 training kernels."""
+before it checks the library's BF16 training kernels."""
 import numpy as np
 
 from oracle import nn_oracle as N
