@@ -40,7 +40,7 @@ EXPORTS = [
     "gcf_get_stage_times", "gcf_get_launch_count", "gcf_get_search_counts", "gcf_avg_spectrum_noalloc",
     "gcf_gemm_bf16", "gcf_run_batch_mode", "gcf_get_fast_counts", "gcf_get_fast_times",
     "gcf_nn_param_count", "gcf_nn_init", "gcf_nn_set_params", "gcf_nn_get_params", "gcf_nn_save",
-    "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs",
+    "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs", "gcf_nn_inputs",
     "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
     "gcf_write_ctf_file", "gcf_write_ctf_file_ex", "gcf_set_package_callback", "gcf_set_graphs",
     "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load", "gcf_gemm_bf16_ex",
@@ -86,12 +86,12 @@ class CtfParam(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("fused_shape", C.c_int), ("gemm_tile_n", C.c_int), ("gemm_stages", C.c_int),
-                ("gemm_persistent", C.c_int), ("fused_ms", C.c_float * 4), ("gemm_ms", C.c_float * 10)]
+                ("gemm_persistent", C.c_int), ("fused_ms", C.c_float * 5), ("gemm_ms", C.c_float * 10)]
 
     def as_dict(self):
         return {"fused_shape": self.fused_shape, "gemm_tile_n": self.gemm_tile_n,
                 "gemm_stages": self.gemm_stages, "gemm_persistent": self.gemm_persistent,
-                "fused_ms": dict(zip(["8", "816", "16", "162"], [round(x, 4) for x in self.fused_ms])),
+                "fused_ms": dict(zip(["8", "816", "16", "162", "168"], [round(x, 4) for x in self.fused_ms])),
                 "gemm_ms": dict(zip(["256x2", "256x3", "256x4", "128x4", "128x6", "64x4", "p256x3", "p256x4",
                                      "p128x4", "p128x6"], [round(x, 4) for x in self.gemm_ms]))}
 
@@ -170,6 +170,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_set_learned_threshold.argtypes = [vp, f]
     L.gcf_nn_train.argtypes = [vp, C.POINTER(Optics), i, i, ull, ull, f, vp]
     L.gcf_nn_synth_inputs.argtypes = [vp, C.POINTER(Optics), ull, ull, i, vp, vp, vp, vp]
+    L.gcf_nn_inputs.argtypes = [vp, vp, vp, i, vp, vp]
     L.gcf_nn_forward_backward.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
     L.gcf_nn_eval_synthetic.argtypes = [vp, C.POINTER(Optics), ull, ull, i, i, C.POINTER(Result), vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
@@ -270,7 +271,7 @@ class Context:
         _check(self.L.gcf_set_spectrum_impl(self._h, impl), self._h)
 
     def set_fused_shape(self, shape: int):
-        """0 (auto), 8, 816 or 16: cluster shape of the fused tile kernel."""
+        """0 (auto), 8, 816, 16, 162 or 168: cluster shape of the fused tile kernel."""
         _check(self.L.gcf_set_fused_shape(self._h, shape), self._h)
 
     # -- CFindCtf2D shape ------------------------------------------------------
@@ -484,6 +485,20 @@ class Context:
         _check(self.L.gcf_nn_synth_inputs(self._h, C.byref(optics), seed, first, n, x1.ctypes.data,
                                           x2.ctypes.data, t.ctypes.data, p.ctypes.data), self._h)
         return x1, x2, t, p
+
+    def nn_inputs(self, spectra, pixel_sizes):
+        """Network inputs (x1 n x 256, x2 n x 256 x 256) of background-removed
+        half spectra (n x tile x tile/2+1, or one spectrum) of the given pixel sizes."""
+        s = np.ascontiguousarray(spectra, np.float32)
+        if s.ndim == 2:
+            s = s[None]
+        n = s.shape[0]
+        px = np.ascontiguousarray(np.broadcast_to(np.asarray(pixel_sizes, np.float32), (n,)))
+        x1 = np.zeros((n, 256), np.float32)
+        x2 = np.zeros((n, 256, 256), np.float32)
+        _check(self.L.gcf_nn_inputs(self._h, s.ctypes.data, px.ctypes.data, n, x1.ctypes.data, x2.ctypes.data),
+               self._h)
+        return x1, x2
 
     def nn_forward_backward(self, x1, x2, target):
         x1 = np.ascontiguousarray(x1, np.float32)

@@ -813,7 +813,7 @@ gcf_status solo_setup(gcf_ctx* ctx, SoloLaunch* sl)
     if (ctx->solo_n < 0) {
         int sms = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->dev));
-        const int per_cluster = ctx->fused_shape == 16 ? 16 : 8;
+        const int per_cluster = (ctx->fused_shape == 16 || ctx->fused_shape == 168) ? 16 : 8;
         ctx->solo_n = std::max(0, sms - ctx->fused_clusters * per_cluster);
         if (ctx->solo_n > 0 && !ctx->st_solo) {
             int lo = 0, hi = 0;
@@ -1998,7 +1998,8 @@ gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int w, int h, float px, i
 
 gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape)
 {
-    if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16 && shape != 162)) return GCF_ERR_INVALID_ARG;
+    if (!ctx || (shape != 0 && shape != 8 && shape != 816 && shape != 16 && shape != 162 && shape != 168))
+        return GCF_ERR_INVALID_ARG;
     ctx->fused_shape_req = shape;
     ctx->fused_clusters = 0;   // recomputed at the next launch
     ctx->solo_n = -1;
@@ -2874,7 +2875,7 @@ struct TuneCache {
 };
 std::mutex g_tune_mu;
 TuneCache g_tune[64];
-constexpr int kTuneShapes[4] = {8, 816, 16, 162};
+constexpr int kTuneShapes[5] = {8, 816, 16, 162, 168};
 // (tile N, stages, persistent)
 constexpr int kTuneGemm[10][3] = {{256, 2, 0}, {256, 3, 0}, {256, 4, 0}, {128, 4, 0}, {128, 6, 0},
                                   {64, 4, 0},  {256, 3, 1}, {256, 4, 1}, {128, 4, 1}, {128, 6, 1}};
@@ -2910,7 +2911,7 @@ gcf_status tune_device(gcf_ctx* ctx, gcf_tuning& t, cudaEvent_t a, cudaEvent_t b
         for (int i = 0; i < nm; ++i) mics[i] = MicImage{img.p + (size_t)i * W * H, W, H, W, 1.35f};
         CKS(spectra_alloc(ctx, nm));
         float best = 1e30f;
-        for (int si = 0; si < 4; ++si) {
+        for (int si = 0; si < 5; ++si) {
             int ncl = 0;
             if (fused_clusters_of(kTuneShapes[si], &ncl) != cudaSuccess || ncl <= 0) {
                 cudaGetLastError();
@@ -3209,6 +3210,36 @@ gcf_status gcf_nn_train(gcf_ctx* ctx, const gcf_optics* optics, int steps, int b
     if (losses) CK(cudaMemcpyAsync(losses, ctx->nloss.p, steps * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     if (err) return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core product: a bounded wait gave up");
+    return GCF_OK;
+}
+
+gcf_status gcf_nn_inputs(gcf_ctx* ctx, const float* spectra, const float* px, int n, float* x1, float* x2)
+{
+    if (!ctx || !spectra || !px || n <= 0 || n > kNnChunk) return GCF_ERR_INVALID_ARG;
+    CKS(set_device(ctx));
+    const size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
+    DBuf<float> ds, dp;
+    DBuf<__nv_bfloat16> d1, d2;
+    std::vector<__nv_bfloat16> h1((size_t)n * kNnProfile), h2((size_t)n * kNnMap * kNnMap);
+    cudaError_t e = ds.ensure(cmp_n * n);
+    if (e == cudaSuccess) e = dp.ensure(n);
+    if (e == cudaSuccess) e = d1.ensure(h1.size());
+    if (e == cudaSuccess) e = d2.ensure(h2.size());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds.p, spectra, cmp_n * n * sizeof(float), cudaMemcpyHostToDevice, ctx->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dp.p, px, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st);
+    if (e == cudaSuccess) e = launch_nn_input(ds.p, ctx->tile, dp.p, 1, n, d1.p, d2.p, ctx->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h1.data(), d1.p, h1.size() * 2, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h2.data(), d2.p, h2.size() * 2, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    ds.release();
+    dp.release();
+    d1.release();
+    d2.release();
+    CK(e);
+    if (x1)
+        for (size_t i = 0; i < h1.size(); ++i) x1[i] = __bfloat162float(h1[i]);
+    if (x2)
+        for (size_t i = 0; i < h2.size(); ++i) x2[i] = __bfloat162float(h2[i]);
     return GCF_OK;
 }
 

@@ -281,6 +281,9 @@ using Shape8W16 = FusedShape<8, 16, false, false>;  // 8-CTA clusters, 512 threa
 // memory: two CTAs (of different clusters, or of one) per SM, so one CTA's
 // cluster barrier or DSMEM exchange overlaps the other's FFTs
 using Shape16x2 = FusedShape<16, 8, false, false, 2>;
+// 16-CTA clusters of 8 warps with the column buffer double-buffered (one
+// cluster barrier per tile) and half the per-warp accumulators of Shape8
+using Shape16W8 = FusedShape<16, 8, true>;
 
 template <class S>
 __global__ void __launch_bounds__(S::THR, S::MINB)
@@ -904,7 +907,7 @@ cudaError_t fused_max_clusters(int* n, int* shape)
 
 // Co-resident clusters of one shape: 8 (8 CTAs x 8 warps), 816 (8 CTAs x 16
 // warps, 128 registers), 16 (16 CTAs x 16 warps, double buffered), 162 (16
-// CTAs x 8 warps, two CTAs per SM).
+// CTAs x 8 warps, two CTAs per SM), 168 (16 CTAs x 8 warps, double buffered).
 cudaError_t fused_clusters_of(int shape, int* n)
 {
     *n = 0;
@@ -913,6 +916,7 @@ cudaError_t fused_clusters_of(int shape, int* n)
     case 816: return max_clusters<Shape8W16>(n);
     case 16: return max_clusters<Shape16>(n);
     case 162: return max_clusters<Shape16x2>(n);
+    case 168: return max_clusters<Shape16W8>(n);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -945,6 +949,11 @@ cudaError_t launch_fused(const void* descs, double* const* bsum_out, int max_blo
         cudaLaunchConfig_t cfg = fused_cfg<Shape16>(nclusters, st, attr);
         e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16>, reinterpret_cast<const FusedTab*>(descs), items,
                                nitems, taper, tw, partial, next_item);
+    } else if (shape == 168) {
+        if ((e = prepare_kernel<Shape16W8>()) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = fused_cfg<Shape16W8>(nclusters, st, attr);
+        e = cudaLaunchKernelEx(&cfg, k_fused_spectrum<Shape16W8>, reinterpret_cast<const FusedTab*>(descs),
+                               items, nitems, taper, tw, partial, next_item);
     } else if (shape == 162) {
         if ((e = prepare_kernel<Shape16x2>()) != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = fused_cfg<Shape16x2>(nclusters, st, attr);

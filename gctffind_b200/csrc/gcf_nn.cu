@@ -65,7 +65,10 @@ __device__ __forceinline__ float gauss(uint64_t seed, uint64_t stream, uint64_t 
 // bins (x2, angle rows) and 256 s^2 bins over all angles (x1); each is then
 // standardised over its non-empty cells (empty cells 0).  One CTA per job;
 // the angle bins are done in two halves of 128 so the sums fit in shared
-// memory.
+// memory.  Angle bin t = (atan2(fy, fx) + pi/2) * 256 / pi: rows above the
+// DC row (fy < 0, |angle| >= atan(1/256) off the axis) fall in t < 128 and
+// the others in t >= 128, so each half visits only its own rows, one warp
+// per row over the row's in-band column interval.
 __global__ void __launch_bounds__(1024)
 k_nn_input(const float* __restrict__ ctf, int tile, const float* __restrict__ px_of, int px_stride,
            __nv_bfloat16* __restrict__ x1, __nv_bfloat16* __restrict__ x2)
@@ -83,6 +86,7 @@ k_nn_input(const float* __restrict__ ctf, int tile, const float* __restrict__ px
     const float s2lo = 1.0f / 1600.0f, s2hi = 1.0f / 12.25f;
     const float ds2 = (s2hi - s2lo) / 256.0f;
     const float inv_px2 = 1.0f / (px * px);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         s_prof[i] = 0.0f;
         s_pcnt[i] = 0;
@@ -94,23 +98,29 @@ k_nn_input(const float* __restrict__ ctf, int tile, const float* __restrict__ px
             cnt[i] = 0;
         }
         __syncthreads();
-        for (int p = threadIdx.x; p < cx * cy; p += blockDim.x) {
-            const int y = p / cx, x = p - y * cx;
-            const float fx = (float)x / (float)tile, fy = (float)(y - cy / 2) / (float)tile;
-            const float s2 = (fx * fx + fy * fy) * inv_px2;
-            if (s2 < s2lo || s2 >= s2hi) continue;
-            const int k = min(max((int)((s2 - s2lo) / ds2), 0), 255);
-            const int t = min(max((int)((atan2f(fy, fx) + 0.5f * kPiF) * (256.0f / kPiF)), 0), 255);
-            const float v = S[p];
-            if (half == 0) {
+        for (int yr = warp; yr < cy / 2; yr += nwarps) {
+            const int y = half * (cy / 2) + yr;
+            const float fy = (float)(y - cy / 2) / (float)tile;
+            // columns whose s^2 can fall in [s2lo, s2hi), one column of slack on
+            // each side; the exact test below decides
+            const float alo = s2lo * px * px - fy * fy, ahi = s2hi * px * px - fy * fy;
+            const int xlo = alo > 0.0f ? max((int)(sqrtf(alo) * (float)tile) - 1, 0) : 0;
+            const int xhi = min(ahi > 0.0f ? (int)(sqrtf(ahi) * (float)tile) + 2 : 2, cx);
+            for (int x = xlo + lane; x < xhi; x += 32) {
+                const float fx = (float)x / (float)tile;
+                const float s2 = (fx * fx + fy * fy) * inv_px2;
+                if (s2 < s2lo || s2 >= s2hi) continue;
+                const int k = min(max((int)((s2 - s2lo) / ds2), 0), 255);
+                const int t = min(max((int)((atan2f(fy, fx) + 0.5f * kPiF) * (256.0f / kPiF)), 0), 255);
+                const float v = S[(size_t)y * cx + x];
                 atomicAdd(&s_prof[k], v);
                 atomicAdd(&s_pcnt[k], 1);
+                if ((t >> 7) != half) continue;
+                const int c = (t & 127) * 256 + k;
+                atomicAdd(&sum[c], v);
+                // counts stay below 65536: at most a few hundred pixels per cell
+                atomicAdd(reinterpret_cast<unsigned int*>(&cnt[c & ~1]), (c & 1) ? 65536u : 1u);
             }
-            if ((t >> 7) != half) continue;
-            const int c = (t & 127) * 256 + k;
-            atomicAdd(&sum[c], v);
-            // counts stay below 65536: at most a few hundred pixels per cell
-            atomicAdd(reinterpret_cast<unsigned int*>(&cnt[c & ~1]), (c & 1) ? 65536u : 1u);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < 128 * 256; i += blockDim.x) {
@@ -135,11 +145,10 @@ k_nn_input(const float* __restrict__ ctf, int tile, const float* __restrict__ px
         q2 += __shfl_xor_sync(0xffffffffu, q2, o);
         n2 += __shfl_xor_sync(0xffffffffu, n2, o);
     }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        s_red[0][w] = m2;
-        s_red[1][w] = q2;
-        s_red[2][w] = n2;
+    if (lane == 0) {
+        s_red[0][warp] = m2;
+        s_red[1][warp] = q2;
+        s_red[2][warp] = n2;
     }
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -277,35 +286,46 @@ __global__ void k_synth_raw(unsigned long long seed, unsigned long long first, c
 
 // ---------------------------------------------------------------------------
 // im2col of the 4 x 4 stride-4 first layer on the 256 x 256 x 1 input:
-// row (b, oy, ox) = the 16 pixels of patch (oy, ox), (ky, kx) order.
+// row (b, oy, ox) = the 16 pixels of patch (oy, ox), (ky, kx) order.  One
+// thread per (row, ky): 4 contiguous BF16 (8 bytes) in and out.
 __global__ void k_im2col_p4(const __nv_bfloat16* __restrict__ x, int B, __nv_bfloat16* __restrict__ cols)
 {
-    const long long n = (long long)B * 4096 * 16;
+    const long long n = (long long)B * 4096 * 4;
+    const uint2* __restrict__ xv = reinterpret_cast<const uint2*>(x);
+    uint2* __restrict__ cv = reinterpret_cast<uint2*>(cols);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int kk = (int)(i & 15);
-        const long long r = i >> 4;
-        const int b = (int)(r >> 12), oy = (int)((r >> 6) & 63), ox = (int)(r & 63);
-        const int yy = oy * 4 + (kk >> 2), xx = ox * 4 + (kk & 3);
-        cols[i] = x[(size_t)b * 65536 + yy * 256 + xx];
+        const int ky = (int)(i & 3);
+        const long long r = i >> 2;
+        const int ox = (int)(r & 63), oy = (int)((r >> 6) & 63);
+        const long long b = r >> 12;
+        // x row (oy * 4 + ky), columns ox * 4 .. ox * 4 + 3: uint2 index / 4 pixels
+        cv[i] = xv[(size_t)b * 16384 + (oy * 4 + ky) * 64 + ox];
     }
 }
 
 // im2col of a 3 x 3 stride-2 pad-1 layer on channel-last [B][H][W][C]:
-// row (b, oy, ox), column (ky * 3 + kx) * C + c.
+// row (b, oy, ox), column (ky * 3 + kx) * C + c.  One thread per (row, tap,
+// 8 channels): 16 bytes in and out (C a multiple of 8).
 __global__ void k_im2col_3s2(const __nv_bfloat16* __restrict__ x, int B, int H, int W, int C,
                              __nv_bfloat16* __restrict__ cols)
 {
-    const int OH = H / 2, OW = W / 2, K = 9 * C;
-    const long long n = (long long)B * OH * OW * K;
+    const int OH = H / 2, OW = W / 2, C8 = C / 8, K8 = 9 * C8;
+    const long long n = (long long)B * OH * OW * K8;
+    const uint4* __restrict__ xv = reinterpret_cast<const uint4*>(x);
+    uint4* __restrict__ cv = reinterpret_cast<uint4*>(cols);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int col = (int)(i % K);
-        const long long r = i / K;
-        const int ox = (int)(r % OW), oy = (int)((r / OW) % OH), b = (int)(r / ((long long)OW * OH));
-        const int c = col % C, kk = col / C, ky = kk / 3, kx = kk - 3 * ky;
+        const long long r = i / K8;
+        const int col8 = (int)(i - r * K8);
+        const int kk = col8 / C8, c8 = col8 - kk * C8;
+        const int ky = kk / 3, kx = kk - 3 * ky;
+        const int ox = (int)(r % OW);
+        const long long r2 = r / OW;
+        const int oy = (int)(r2 % OH);
+        const long long b = r2 / OH;
         const int yy = 2 * oy - 1 + ky, xx = 2 * ox - 1 + kx;
-        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
-        if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = x[(((size_t)b * H + yy) * W + xx) * C + c];
-        cols[i] = v;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);   // BF16 zero is all-zero bits
+        if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = xv[((b * H + yy) * W + xx) * C8 + c8];
+        cv[i] = v;
     }
 }
 
@@ -501,12 +521,13 @@ void launch_synth_raw(unsigned long long seed, unsigned long long first, const f
 
 void launch_im2col_p4(const __nv_bfloat16* x, int B, __nv_bfloat16* cols, cudaStream_t st)
 {
-    k_im2col_p4<<<grid_for((long long)B * 65536, 256), 256, 0, st>>>(x, B, cols);
+    k_im2col_p4<<<grid_for((long long)B * 4096 * 4, 256), 256, 0, st>>>(x, B, cols);
 }
 
 void launch_im2col_3s2(const __nv_bfloat16* x, int B, int H, int W, int C, __nv_bfloat16* cols, cudaStream_t st)
 {
-    k_im2col_3s2<<<grid_for((long long)B * (H / 2) * (W / 2) * 9 * C, 256), 256, 0, st>>>(x, B, H, W, C, cols);
+    // C is 16 or 32 here: 16-byte channel groups, buffers 256-byte aligned
+    k_im2col_3s2<<<grid_for((long long)B * (H / 2) * (W / 2) * 9 * (C / 8), 256), 256, 0, st>>>(x, B, H, W, C, cols);
 }
 
 void launch_col2im_3s2_relu(const float* dcols, const __nv_bfloat16* y, int B, int H, int W, int C,

@@ -81,7 +81,8 @@ const char* gcf_last_error(gcf_ctx* ctx);
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
 /* Cluster shape of the fused tile kernel: 0 = the shape that keeps the most
  * SMs busy (default), 8 = 8 CTAs x 8 warps, 816 = 8 CTAs x 16 warps,
- * 16 = 16 CTAs x 16 warps, 162 = 16 CTAs x 8 warps with two CTAs per SM.
+ * 16 = 16 CTAs x 16 warps, 162 = 16 CTAs x 8 warps with two CTAs per SM,
+ * 168 = 16 CTAs x 8 warps with a double-buffered column buffer.
  * For tuning (gcf_autotune picks one by timing); results do not depend on it. */
 gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape);
 
@@ -306,11 +307,11 @@ gcf_status gcf_set_graphs(gcf_ctx* ctx, int on);
  * not depend on the choice, only speed.  No counterpart in the reference,
  * whose kernels have fixed launch shapes. */
 typedef struct {
-    int fused_shape;     /* tile-kernel cluster shape picked: 8, 816, 16 or 162 */
+    int fused_shape;     /* tile-kernel cluster shape picked: 8, 816, 16, 162 or 168 */
     int gemm_tile_n;     /* contraction product tile picked: 128 x gemm_tile_n */
     int gemm_stages;     /* its load-pipeline depth */
     int gemm_persistent; /* 1: the persistent product (gcf_gemm_bf16_ex) */
-    float fused_ms[4];   /* trial ms of shapes 8, 816, 16, 162 (-1: cannot be resident) */
+    float fused_ms[5];   /* trial ms of shapes 8, 816, 16, 162, 168 (-1: cannot be resident) */
     float gemm_ms[10];   /* trial ms of (256,2) (256,3) (256,4) (128,4) (128,6) (64,4) one tile per
                             CTA, then (256,3) (256,4) (128,4) (128,6) persistent */
 } gcf_tuning;
@@ -343,6 +344,12 @@ gcf_status gcf_nn_train(gcf_ctx* ctx, const gcf_optics* optics, int steps, int b
 gcf_status gcf_nn_synth_inputs(gcf_ctx* ctx, const gcf_optics* optics, unsigned long long seed,
                                unsigned long long first, int n, float* x1, float* x2, float* target,
                                float* params);
+/* The network inputs of n <= 512 given background-removed half spectra
+ * (host, n x tile x (tile/2+1) floats in the layout of
+ * gcf_get_half_spectrum) of pixel sizes px[n]: x1 n x 256 (s^2 profile),
+ * x2 n x 256 x 256 (angle rows x s^2 bins), as host floats (the BF16 values
+ * the network reads); each output nullable. */
+gcf_status gcf_nn_inputs(gcf_ctx* ctx, const float* spectra, const float* px, int n, float* x1, float* x2);
 /* One forward and backward pass on given inputs (rounded to BF16): loss,
  * the FP32 gradient of every parameter (gcf_nn_param_count floats) and the
  * predictions (n x 3); outputs nullable.  For gradient checks. */

@@ -129,3 +129,47 @@ def split(flat):
         out.append((flat[off: off + o * i].reshape(o, i), flat[off + o * i: off + o * i + o]))
         off += o * i + o
     return out
+
+
+def polar_inputs(half, px):
+    """The network inputs of one background-removed half spectrum
+    `half` [tile][tile/2+1] (DC at (0, tile/2)) of pixel size px, as the
+    library bins them (gctffind_b200/csrc/gcf_nn.cu k_nn_input): pixels with
+    s^2 in [1/1600, 1/12.25) 1/A^2 go to s^2 bin k (256 uniform bins) and
+    angle bin t = (atan2(fy, fx) + pi/2) * 256 / pi; x2[t][k] and x1[k] are
+    the bins' means, standardised (population variance) over non-empty bins,
+    empty bins 0.  Bin indices are computed in float32 like the library's;
+    x2's means are rounded to BF16 before standardisation, as the library
+    stores them.  Returns (x1 [256], x2 [256][256]) in float64."""
+    half = np.asarray(half)
+    cy, cx = half.shape
+    tile = cy
+    f32 = np.float32
+    y, x = np.mgrid[0:cy, 0:cx]
+    fx = x.astype(f32) / f32(tile)
+    fy = (y - cy // 2).astype(f32) / f32(tile)
+    inv_px2 = f32(1.0) / (f32(px) * f32(px))
+    s2 = (fx * fx + fy * fy) * inv_px2
+    s2lo, s2hi = f32(1.0) / f32(1600.0), f32(1.0) / f32(12.25)
+    ds2 = (s2hi - s2lo) / f32(256.0)
+    m = (s2 >= s2lo) & (s2 < s2hi)
+    k = np.clip(((s2 - s2lo) / ds2).astype(np.int64), 0, 255)[m]
+    ang = np.arctan2(fy.astype(np.float64), fx.astype(np.float64)) + 0.5 * np.pi
+    t = np.clip((ang * (256.0 / np.pi)).astype(np.int64), 0, 255)[m]
+    v = half.astype(np.float64)[m]
+
+    def standardise(s, c, rounded):
+        mean = np.where(c > 0, s / np.maximum(c, 1), 0.0)
+        nz = c > 0
+        mu = mean[nz].mean() if nz.any() else 0.0
+        var = (mean[nz] ** 2).mean() - mu * mu if nz.any() else 0.0
+        inv = 1.0 / np.sqrt(var) if var > 1e-30 else 0.0
+        base = bf16(mean) if rounded else mean
+        return np.where(nz, (base - mu) * inv, 0.0)
+
+    c1 = np.bincount(k, minlength=256).astype(np.float64)
+    s1 = np.bincount(k, weights=v, minlength=256)
+    cell = t * 256 + k
+    c2 = np.bincount(cell, minlength=65536).astype(np.float64)
+    s2m = np.bincount(cell, weights=v, minlength=65536)
+    return standardise(s1, c1, False), standardise(s2m, c2, True).reshape(256, 256)

@@ -305,6 +305,25 @@ def test_fused_batch_deterministic(gpu_lib):
         assert x.as_dict() == y.as_dict()
 
 
+def test_every_cluster_shape_gives_the_same_spectrum(gpu_lib):
+    """The tile kernel's cluster shapes (8, 816, 16, 162, 168) split a tile's
+    rows and columns differently over CTAs and warps, but every FFT and every
+    sum runs in the same order: the averaged spectrum is bit-identical."""
+    G = gpu_lib
+    img = _img(seed=44, w=2560, h=2048, df=(16800.0, 17300.0), az=25.0)
+    op = G.make_optics(pixel_size=PX)
+    out = {}
+    for shape in (8, 816, 16, 162, 168):
+        ctx = G.Context(0, 512, 0)
+        ctx.set_fused_shape(shape)
+        ctx.setup(op, 2560, 2048)
+        ctx.gen_half_spectrum(img)
+        out[shape] = ctx.half_spectrum(raw=True)
+        ctx.close()
+    for shape, g in out.items():
+        assert np.array_equal(g, out[8]), shape
+
+
 def test_cluster_less_ctas_do_not_change_spectra(gpu_lib):
     """Twelve 4096 x 4096 micrographs (10 work items each) through one
     gcf_run_batch call: with 120 items in one launch the cluster-less tile

@@ -51,6 +51,33 @@ def test_gradients_match_oracle(gpu_lib):
                 assert rel <= rel_bar and cos >= cos_bar, (emulate, k, rel, cos)
 
 
+@pytest.mark.parametrize("px", [1.2, 1.35, 1.5])
+def test_network_inputs_match_oracle(gpu_lib, px):
+    """The polar binning of a background-removed half spectrum (k_nn_input)
+    against oracle/nn_oracle.py polar_inputs.  Both round the bin indices in
+    float32, but the library's atan2f and fused multiply-adds may move a
+    pixel that sits on a bin edge to the neighbouring bin: at most 0.5 % of
+    the bins may differ by more than the BF16 rounding of the output
+    (2^-7 relative + 0.02), and the empty bins must be the same up to 0.5 %."""
+    from gctffind_b200 import synth
+    G = gpu_lib
+    spec = synth.MicrographSpec(width=2048, height=2048, pixel_size=px, df_min=17800.0, df_max=18300.0,
+                                azimuth_deg=30.0, seed=5)
+    img = synth.make_micrograph(spec).numpy()
+    ctx = G.Context(0, 512, 0)
+    ctx.setup(G.make_optics(pixel_size=px), 2048, 2048)
+    ctx.gen_half_spectrum(img)
+    half = ctx.half_spectrum(raw=False)
+    x1, x2 = ctx.nn_inputs(half, px)
+    ctx.close()
+    o1, o2 = N.polar_inputs(half, px)
+    for g, o in ((x1[0], o1), (x2[0], o2)):
+        bad = np.abs(g - o) > 2.0 ** -7 * np.abs(o) + 0.02
+        assert bad.mean() <= 5e-3, (px, int(bad.sum()), g.size)
+        assert abs(int((g != 0).sum()) - int((o != 0).sum())) <= 5e-3 * g.size
+    assert 0.9 < float(x2[0][x2[0] != 0].std()) < 1.1
+
+
 def test_training_lowers_the_loss_and_weights_round_trip(gpu_lib, tmp_path):
     G = gpu_lib
     ctx = G.Context(0, 512, 0)
