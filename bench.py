@@ -612,8 +612,11 @@ def main():
                 "search_ms": round(nonet["stage"].get("search1d", 0.0) + nonet["stage"].get("search2d", 0.0), 3),
                 "table_candidates": nonet["fast_counts"].get("table_cand"),
                 "tensor_macs": nonet["fast_counts"].get("tensor_macs"),
-                "note": "the same batch through the contraction search without the learned window; the "
-                        "headline's own search_ms is search1d + search2d of stage_ms_per_step"},
+                "learned_search_ms": round(fast["stage"].get("search1d", 0.0) + fast["stage"].get("search2d", 0.0), 3),
+                "learned_network_ms": round(ft.get("network", 0.0), 3),
+                "note": "the same batch through the contraction search without the learned window; "
+                        "learned_search_ms is the headline's search1d + search2d, learned_network_ms its "
+                        "network (inputs and layers), which runs before the search stages"},
             "defocus_error": defocus_error(fast["results"], plain["results"], specs),
             "stage_ms_per_step": {k: round(v, 3) for k, v in fast["stage"].items()},
             "contraction": {"stage_ms": {k: round(v, 3) for k, v in ft.items()}, "counts": fc,

@@ -521,9 +521,9 @@ class Context:
 
     def fast_times(self):
         """Device ms of the contraction stages of the last batched call."""
-        t = (C.c_float * 4)()
+        t = (C.c_float * 5)()
         _check(self.L.gcf_get_fast_times(self._h, t), self._h)
-        return dict(zip(["bin", "product", "table", "finish"], list(t)))
+        return dict(zip(["bin", "product", "table", "finish", "network"], list(t)))
 
     def stage_times(self):
         t = (C.c_float * 7)()

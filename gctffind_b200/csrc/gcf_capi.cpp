@@ -289,8 +289,8 @@ struct gcf_ctx {
     // [2] candidates re-scored in FP32, [3] learned searches that fell back
     long long fast_counts[4] = {0, 0, 0, 0};
     // events around the contraction stages: bin | product | table | FP32 finish
-    cudaEvent_t fev[5] = {};
-    float fast_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t fev[7] = {};          // contraction stages [0..4], network [5..6]
+    float fast_ms[5] = {0, 0, 0, 0, 0};
 
     // learned initialiser
     NnNet* nn = nullptr;
@@ -345,6 +345,7 @@ cudaError_t h2d(gcf_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStre
     }
     void* h = ctx->arena.put(src, bytes);
     if (!h) return cudaErrorMemoryAllocation;
+    ctx->launches += 1;
     return launch_copy_from_host(dst, h, bytes, st);
 }
 
@@ -1444,6 +1445,9 @@ gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
     CK(ctx->cPrior.ensure(n));
     CK(ctx->nx1.ensure((size_t)kNnChunk * kNnProfile));
     CK(ctx->nx2.ensure((size_t)kNnChunk * kNnMap * kNnMap));
+    for (auto& e : ctx->fev)
+        if (!e) CK(cudaEventCreate(&e));
+    CK(record_timing(ctx->fev[5], ctx->st));
     CK(h2d(ctx, ctx->npx.p, px_n.data(), n * sizeof(float), ctx->st));
     const size_t cmp_n = (size_t)(ctx->tile / 2 + 1) * ctx->tile;
     for (int c0 = 0; c0 < n; c0 += kNnChunk) {
@@ -1452,8 +1456,9 @@ gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
         CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, cn, ctx->st));
         launch_prior(nn_pred(ctx->nn), kNnPredPitch, cn, ctx->cPrior.p + c0, ctx->st);
         CKL();
-        ctx->launches += 13;
+        ctx->launches += 14;   // inputs, 4 im2col, 7 products, concat, prior
     }
+    CK(record_timing(ctx->fev[6], ctx->st));
     return GCF_OK;
 }
 
@@ -1501,6 +1506,11 @@ gcf_status search_collect(gcf_ctx* ctx, const std::vector<float>& px_n, const fl
     if (mode == GCF_SEARCH_PLAIN) return run_search_collect(ctx, pend, out);
     CKS(run_fast_collect(ctx, pend, out, nullptr));
     if (mode != GCF_SEARCH_LEARNED) return GCF_OK;
+    {
+        float t = 0.0f;   // the network's inputs and layers (learned_priors)
+        if (cudaEventElapsedTime(&t, ctx->fev[5], ctx->fev[6]) == cudaSuccess) ctx->fast_ms[4] += t;
+        cudaGetLastError();
+    }
     const int n = (int)px_n.size();
     std::vector<SearchJob> jh(n);
     CK(cudaMemcpy(jh.data(), ctx->jobs.p, n * sizeof(SearchJob), cudaMemcpyDeviceToHost));
@@ -3331,10 +3341,10 @@ gcf_status gcf_get_fast_counts(gcf_ctx* ctx, long long counts[4])
     return GCF_OK;
 }
 
-gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[4])
+gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[5])
 {
     if (!ctx || !times_ms) return GCF_ERR_INVALID_ARG;
-    for (int i = 0; i < 4; ++i) times_ms[i] = ctx->fast_ms[i];
+    for (int i = 0; i < 5; ++i) times_ms[i] = ctx->fast_ms[i];
     return GCF_OK;
 }
 

@@ -462,8 +462,9 @@ gcf_status gcf_get_fast_counts(gcf_ctx* ctx, long long counts[4]);
 /* Device time (ms, CUDA events) of the contraction stages of the last
  * gcf_run_batch_mode call: [0] polar binning of the spectra, [1] the
  * tensor-core products (table and normaliser), [2] the table search,
- * [3] FP32 re-score and local passes. */
-gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[4]);
+ * [3] FP32 re-score and local passes, [4] the learned initialiser's
+ * network (its inputs and layers; 0 for the other methods). */
+gcf_status gcf_get_fast_times(gcf_ctx* ctx, float times_ms[5]);
 /* Number of kernels this library launched in the last batched call. */
 gcf_status gcf_get_launch_count(gcf_ctx* ctx, long long* count);
 /* Search work counted on the device since the last gcf_run_series /

@@ -127,8 +127,10 @@ def test_trained_network_gain_on_held_out_spectra(gpu_lib):
     plain, prm = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_PLAIN)
     bf16, _ = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_BF16)
     cb = ctx.fast_counts()
+    assert ctx.fast_times()["network"] == 0.0
     learned, _ = ctx.nn_eval_synthetic(op, TI.EVAL_SEED, 0, n, G.GCF_SEARCH_LEARNED)
     cl = ctx.fast_counts()
+    assert ctx.fast_times()["network"] > 0.0   # its inputs and layers, timed on the device
     ctx.close()
     med_b, frac_b, _ = TI.compare(bf16, plain)
     med_l, frac_l, _ = TI.compare(learned, plain)
