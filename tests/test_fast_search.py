@@ -102,3 +102,76 @@ def test_bf16_mode_rejects_bad_mode(gpu_lib):
     with pytest.raises(G.GcfError):
         ctx.run_batch([img], [1.35], G.make_optics(), mode=7)
     ctx.close()
+
+
+@pytest.mark.parametrize("tile", [256, 1024])
+def test_bf16_search_other_tile_sizes(gpu_lib, tile):
+    """The contraction bins whatever half spectrum the tile size gives (the
+    batched-cuFFT spectrum at tiles 256 and 1024): the BF16 search still lands within one search
+    step of the plain search of the same batch for at least 7 of 8
+    micrographs, with a median |d defocus| <= 30 A."""
+    G = gpu_lib
+    specs = _batch(8, 21)
+    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
+    pxs = [s.pixel_size for s in specs]
+    ctx = G.Context(0, tile, 0)
+    op = G.make_optics()
+    plain = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_PLAIN)
+    fast = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_BF16)
+    ctx.close()
+    within, ddf = 0, []
+    for p, f in zip(plain, fast):
+        mp = 0.5 * (p.df_min + p.df_max)
+        step = max(20.0, 0.105 * mp / 31.0)
+        within += abs(f.df_min - p.df_min) <= step and abs(f.df_max - p.df_max) <= step
+        ddf.append(abs(0.5 * (f.df_min + f.df_max) - mp))
+    assert within >= 7, (tile, within, plain, fast)
+    assert float(np.median(ddf)) <= 30.0, ddf
+
+
+def test_phase_plate_data_take_the_plain_search(gpu_lib):
+    """The table has no extra-phase dimension: with ext_phase_range > 0 the
+    BF16 and learned methods return the plain search's results bit for bit."""
+    G = gpu_lib
+    specs = _batch(3, 33)
+    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
+    pxs = [s.pixel_size for s in specs]
+    ctx = G.Context(0, 512, 0)
+    G.load_learned(ctx)
+    op = G.make_optics(ext_phase_deg=40.0, ext_phase_range=60.0)
+    plain = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_PLAIN)
+    for mode in (G.GCF_SEARCH_BF16, G.GCF_SEARCH_LEARNED):
+        fast = ctx.run_batch(imgs, pxs, op, mode=mode)
+        assert [r.as_dict() for r in fast] == [r.as_dict() for r in plain]
+    ctx.close()
+
+
+def test_learned_batch_over_one_network_chunk(gpu_lib):
+    """520 micrographs in one learned call: the network runs in chunks of
+    512 spectra, and every micrograph -- those of the second chunk included
+    -- lands within one search step of the plain search for >= 97 % of the
+    batch, median |d defocus| <= 20 A."""
+    import torch
+    G = gpu_lib
+    n = 520
+    specs = _batch(n, 44, sizes=((1536, 1536),))
+    for s in specs:
+        s.dose = max(s.dose, 1.5)
+    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
+    pxs = [s.pixel_size for s in specs]
+    ctx = G.Context(0, 512, 0)
+    G.load_learned(ctx)
+    op = G.make_optics()
+    plain = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_PLAIN)
+    fast = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_LEARNED)
+    ctx.close()
+    within, ddf = [], []
+    for p, f in zip(plain, fast):
+        mp = 0.5 * (p.df_min + p.df_max)
+        step = max(20.0, 0.105 * mp / 31.0)
+        within.append(abs(f.df_min - p.df_min) <= step and abs(f.df_max - p.df_max) <= step)
+        ddf.append(abs(0.5 * (f.df_min + f.df_max) - mp))
+    assert np.mean(within) >= 0.97 and np.mean(within[512:]) >= 0.75, (np.mean(within), within[512:])
+    assert float(np.median(ddf)) <= 20.0
+    del imgs
+    torch.cuda.empty_cache()
