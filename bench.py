@@ -296,7 +296,7 @@ def cpu_baseline(host, specs, budget_s=20.0):
                       f"search), FP64 oracle, {cores} OpenMP threads, {dt:.1f} s"}
 
 
-def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, series_tilts=61):
+def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, series_tilts=61, lines_ctx=None):
     """The mixed stream: 2000 micrographs of the uneven mix in batches of 250,
     interleaved with 8 tilt series of 61 tilts (-60..+60 deg in 2 deg
     steps, 4096^2 at 1.35 A/px).  Each batch and series is made on the
@@ -306,13 +306,16 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
     search is the plain one in both columns).  Each batch's first call also
     makes a cuFFT plan for every new rescaled size (the pixel size varies
     continuously); that call is reported on its own, and the timed calls of
-    both methods run with the plans made.  Defocus error: the headline
-    search against the plain one on the 2000 micrographs."""
+    both methods run with the plans made.  With lines_ctx (a context whose
+    rescale is the library's line transforms, which make no plans), each
+    batch's first and second calls through it are reported as well.
+    Defocus error: the headline search against the plain one on the 2000
+    micrographs."""
     import numpy as np
     import torch
     from gctffind_b200 import synth
     op = G.make_optics()
-    fast_ms = plain_ms = first_ms = 0.0
+    fast_ms = plain_ms = first_ms = lines_first_ms = lines_ms = 0.0
     n_mics = 0
     fast_res, plain_res, specs_all = [], [], []
     for b in range(n_batches):
@@ -320,6 +323,11 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
         imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
         pxs = [s.pixel_size for s in specs]
         torch.cuda.synchronize()
+        if lines_ctx is not None:
+            lines_ctx.run_batch(imgs, pxs, op, mode=fast_mode)
+            lines_first_ms += lines_ctx.stage_times()["total"]
+            lines_ctx.run_batch(imgs, pxs, op, mode=fast_mode)
+            lines_ms += lines_ctx.stage_times()["total"]
         ctx.run_batch(imgs, pxs, op, mode=fast_mode)
         first_ms += ctx.stage_times()["total"]
         fast_res += ctx.run_batch(imgs, pxs, op, mode=fast_mode)
@@ -341,11 +349,19 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
         fast_ms += t
         plain_ms += t
         first_ms += t
+        lines_first_ms += t
+        lines_ms += t
         n_mics += series_tilts
         del simgs
         torch.cuda.empty_cache()
     fast_ms = max_over_ranks(fast_ms, world)
     plain_ms = max_over_ranks(plain_ms, world)
+    lines = None
+    if lines_ctx is not None:
+        lines = {"first_call_value": round(world * n_mics / (max_over_ranks(lines_first_ms, world) / 1000.0), 2),
+                 "value": round(world * n_mics / (max_over_ranks(lines_ms, world) / 1000.0), 2),
+                 "note": "the batches' rescale through the library's line transforms (gcf_resize.cu), which "
+                         "make no plans: each batch's first call and its second call; series as above"}
     return {"workload": f"stream of {n_batches * per_batch} micrographs (uneven mix, batches of {per_batch}) "
                         f"interleaved with {n_batches} tilt series of {series_tilts} x 4096^2 (2 deg steps), "
                         "in HBM; each batch / series timed once on the device",
@@ -354,7 +370,8 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
             "first_call_value": round(world * n_mics / (max_over_ranks(first_ms, world) / 1000.0), 2),
             "first_call_note": "each batch's first call, cuFFT plans of its new rescaled sizes included",
             "speedup_vs_plain": round(plain_ms / fast_ms, 3), "micrographs": n_mics,
-            "defocus_error": defocus_error(fast_res, plain_res, specs_all)}
+            "defocus_error": defocus_error(fast_res, plain_res, specs_all),
+            "rescale_lines": lines}
 
 
 def series_figures(ctx, G, steps, warmup, world, rank):
@@ -645,7 +662,12 @@ def main():
     if not args.no_secondary:
         line["series_41x4096"] = series_figures(ctx, G, max(2, min(args.steps, 3)), 2, world, rank)
         line["single_4096_1p0"] = single_1p0(ctx, G, max(2, min(args.steps, 5)))
-        line["stream_2000_plus_8x61"] = stream_figures(ctx, G, fast_mode, world, rank)
+        lines_ctx = G.Context(local, 512, 0)
+        lines_ctx.set_rescale_impl(G.GCF_RESCALE_LINES)
+        if fast_mode == G.GCF_SEARCH_LEARNED:
+            G.load_learned(lines_ctx)
+        line["stream_2000_plus_8x61"] = stream_figures(ctx, G, fast_mode, world, rank, lines_ctx=lines_ctx)
+        lines_ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline([h.numpy() for h in host], specs)
     if rank == 0:

@@ -24,6 +24,9 @@ CLI_PATH = os.path.join(HERE, "bin", "GCtfFind")
 GCF_SPECT_FUSED = 0
 GCF_SPECT_CUFFT = 1
 
+GCF_RESCALE_CUFFT = 0
+GCF_RESCALE_LINES = 1
+
 GCF_SEARCH_PLAIN = 0
 GCF_SEARCH_BF16 = 1
 GCF_SEARCH_LEARNED = 2
@@ -40,7 +43,7 @@ EXPORTS = [
     "gcf_get_stage_times", "gcf_get_launch_count", "gcf_get_search_counts", "gcf_avg_spectrum_noalloc",
     "gcf_gemm_bf16", "gcf_run_batch_mode", "gcf_get_fast_counts", "gcf_get_fast_times",
     "gcf_nn_param_count", "gcf_nn_init", "gcf_nn_set_params", "gcf_nn_get_params", "gcf_nn_save",
-    "gcf_nn_load", "gcf_set_learned_threshold", "gcf_nn_train", "gcf_nn_synth_inputs", "gcf_nn_inputs",
+    "gcf_nn_load", "gcf_set_learned_threshold", "gcf_set_rescale_impl", "gcf_nn_train", "gcf_nn_synth_inputs", "gcf_nn_inputs",
     "gcf_nn_forward_backward", "gcf_nn_eval_synthetic",
     "gcf_write_ctf_file", "gcf_write_ctf_file_ex", "gcf_set_package_callback", "gcf_set_graphs",
     "gcf_get_graph_info", "gcf_autotune", "gcf_mrc_load", "gcf_gemm_bf16_ex",
@@ -171,6 +174,7 @@ def load_library(path: str = LIB_PATH):
     L.gcf_nn_train.argtypes = [vp, C.POINTER(Optics), i, i, ull, ull, f, vp]
     L.gcf_nn_synth_inputs.argtypes = [vp, C.POINTER(Optics), ull, ull, i, vp, vp, vp, vp]
     L.gcf_nn_inputs.argtypes = [vp, vp, vp, i, vp, vp]
+    L.gcf_set_rescale_impl.argtypes = [vp, i]
     L.gcf_nn_forward_backward.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
     L.gcf_nn_eval_synthetic.argtypes = [vp, C.POINTER(Optics), ull, ull, i, i, C.POINTER(Result), vp]
     L.gcf_write_ctf_file.argtypes = [C.c_char_p, C.POINTER(Result), vp, vp, i, i]
@@ -269,6 +273,11 @@ class Context:
 
     def set_spectrum_impl(self, impl: int):
         _check(self.L.gcf_set_spectrum_impl(self._h, impl), self._h)
+
+    def set_rescale_impl(self, impl: int):
+        """GCF_RESCALE_CUFFT (the reference's cuFFT calls, default) or
+        GCF_RESCALE_LINES (the library's line transforms: no plans to make)."""
+        _check(self.L.gcf_set_rescale_impl(self._h, impl), self._h)
 
     def set_fused_shape(self, shape: int):
         """0 (auto), 8, 816, 16, 162 or 168: cluster shape of the fused tile kernel."""

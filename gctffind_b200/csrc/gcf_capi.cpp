@@ -258,6 +258,7 @@ struct gcf_ctx {
     int fused_clusters = 0;
     int fused_shape = 0;
     int fused_shape_req = 0;   // 0: pick by SM coverage
+    int rescale_impl = GCF_RESCALE_CUFFT;
 
     // CFindCtf2D call-shape state
     gcf_optics optics{};
@@ -1566,8 +1567,17 @@ gcf_status set_device(gcf_ctx* ctx)
     return GCF_OK;
 }
 
+// The line-transform rescale takes even raw widths and lines of at most
+// kResizeMaxLine (raw rows w/2, columns h and nh, new rows nw/2).
+bool rescale_lines_supported(int w, int h, int nw, int nh)
+{
+    return w % 2 == 0 && nw >= 2 && nh >= 2 && resize_line_ok(w / 2) && resize_line_ok(h) && resize_line_ok(nh) &&
+           resize_line_ok(nw / 2);
+}
+
 // CRescaleImage::DoIt on the device: returns a dense new_w x new_h image
-// (FindCTF/CRescaleImage.cpp:68-99).
+// (FindCTF/CRescaleImage.cpp:68-99), through the line transforms of
+// gcf_resize.cu or through cuFFT like the reference.
 gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px, float* out,
                           int* nw_out, int* nh_out, float* px_out, bool* copied)
 {
@@ -1585,6 +1595,21 @@ gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px
     }
     *copied = true;
     int cxi = w / 2 + 1, cxo = nw / 2 + 1;
+    if (ctx->rescale_impl == GCF_RESCALE_LINES && rescale_lines_supported(w, h, nw, nh)) {
+        ResizeLine La, Lf, Li, Lc;
+        const float2 *tA = nullptr, *tC = nullptr;
+        CK(resize_line(w / 2, &La));
+        CK(resize_line(h, &Lf));
+        CK(resize_line(nh, &Li));
+        CK(resize_line(nw / 2, &Lc));
+        CK(resize_twiddles(w, -1, w / 2 + 1, &tA));
+        CK(resize_twiddles(nw, 1, nw / 2, &tC));
+        CK(ctx->rs_cmp.ensure((size_t)cxo * h));
+        CK(ctx->rs_crop.ensure((size_t)cxo * nh));
+        CK(launch_resize(img, w, h, nw, nh, La, tA, Lf, Li, Lc, tC, ctx->rs_cmp.p, ctx->rs_crop.p, out, ctx->st));
+        ctx->launches += 3;
+        return GCF_OK;
+    }
     CK(ctx->rs_cmp.ensure((size_t)cxi * h));
     CK(ctx->rs_crop.ensure((size_t)cxo * nh));
     cufftHandle p1, p2;
@@ -1947,6 +1972,13 @@ void gcf_destroy(gcf_ctx* ctx)
     if (ctx->st_tile) cudaStreamDestroy(ctx->st_tile);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
+}
+
+gcf_status gcf_set_rescale_impl(gcf_ctx* ctx, int impl)
+{
+    if (!ctx || (impl != GCF_RESCALE_LINES && impl != GCF_RESCALE_CUFFT)) return GCF_ERR_INVALID_ARG;
+    ctx->rescale_impl = impl;
+    return GCF_OK;
 }
 
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl)
@@ -2636,6 +2668,7 @@ unsigned long long batch_key(const gcf_ctx* ctx, const gcf_item* items, int n, i
     k.v(op);
     k.v(ctx->tile);
     k.v(ctx->impl);
+    k.v(ctx->rescale_impl);
     k.v(ctx->log_spect);
     k.v(ctx->fused_shape);
     k.v(ctx->fused_clusters);

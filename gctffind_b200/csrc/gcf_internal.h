@@ -29,6 +29,29 @@ unsigned long long device_alloc_epoch();
 // node of the graph (recorded again on every replay).
 cudaError_t record_timing(cudaEvent_t ev, cudaStream_t st);
 
+// gcf_resize.cu: the Fourier-crop rescale as line transforms.  A line of
+// length n (<= kResizeMaxLine): FFT length M (n when a power of two, else
+// the power of two >= 2n - 1 of Bluestein's convolution), and for Bluestein
+// lines the chirp exp(-i pi j^2 / n) and the spectrum of its conjugate over
+// M, divided by M.
+constexpr int kResizeMaxLine = 4096;
+struct ResizeLine {
+    int n, M;
+    const float2* chirp;
+    const float2* bf;
+};
+bool resize_line_ok(int n);
+cudaError_t resize_line(int n, ResizeLine* out);
+// exp(sign 2 pi i k / len), k < count
+cudaError_t resize_twiddles(int len, int sign, int count, const float2** out);
+size_t resize_cols_smem(int h, int m_max);
+// img (w x h, w even) -> out (nw x nh); T1: (nw/2 + 1) x h, T2: (nw/2 + 1) x nh
+// complex scratch; tA = exp(-2 pi i k / w), k <= w/2; tC = exp(2 pi i k / nw),
+// k < nw/2.
+cudaError_t launch_resize(const float* img, int w, int h, int nw, int nh, const ResizeLine& rowA,
+                          const float2* tA, const ResizeLine& colF, const ResizeLine& colI, const ResizeLine& rowC,
+                          const float2* tC, float2* T1, float2* T2, float* out, cudaStream_t st);
+
 // gcf_mrc.cpp: section layout of an MRC file (false if unreadable) and the
 // bytes per pixel of a mode (0 if unsupported).
 bool mrc_layout(const char* path, int dims[3], int* mode, bool* swap, long long* data_off);

@@ -66,6 +66,16 @@ typedef enum {
     GCF_SPECT_CUFFT = 1    /* batched cuFFT comparison variant            */
 } gcf_spectrum_impl;
 
+/* Rescale implementation (CRescaleImage::DoIt, FindCTF/CRescaleImage.cpp:76-99). */
+typedef enum {
+    GCF_RESCALE_CUFFT = 0, /* cuFFT R2C + crop + C2R, the reference's calls
+                              (default: the faster once a size's plans exist) */
+    GCF_RESCALE_LINES = 1  /* hand-written line transforms (gcf_resize.cu): no
+                              plans to make, so new sizes cost nothing extra;
+                              raw width even and every line of the raw and new
+                              sizes <= 4096 long, else cuFFT */
+} gcf_rescale_impl;
+
 /* ---------------------------------------------------------------------- */
 /* Context                                                                  */
 /* ---------------------------------------------------------------------- */
@@ -79,6 +89,9 @@ const char* gcf_strerror(gcf_status s);
 /* Last error detail of this context (CUDA/cuFFT message), never NULL. */
 const char* gcf_last_error(gcf_ctx* ctx);
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
+/* GCF_RESCALE_CUFFT (default) or GCF_RESCALE_LINES for the images below
+ * 1.2 A/px. */
+gcf_status gcf_set_rescale_impl(gcf_ctx* ctx, int impl);
 /* Cluster shape of the fused tile kernel: 0 = the shape that keeps the most
  * SMs busy (default), 8 = 8 CTAs x 8 warps, 816 = 8 CTAs x 16 warps,
  * 16 = 16 CTAs x 16 warps, 162 = 16 CTAs x 8 warps with two CTAs per SM,
