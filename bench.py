@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--batch", type=int, default=N_BATCH)
     ap.add_argument("--mode", default="auto", choices=["auto", "bf16", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rescale-compare", action="store_true",
+                    help="only rescale one frame of each raw size of the batch (3838x3710 @ 0.9, 5760x4092 @ 0.8, "
+                         "4096x4096 @ 1.0 A/px) through both rescale implementations, 2 + 5 calls each "
+                         "(for a profiler's launch list), and print their wall-clock times")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel from the host")
     ap.add_argument("--no-autotune", action="store_true", help="default shapes instead of the autotuner's")
     ap.add_argument("--no-secondary", action="store_true",
@@ -545,6 +549,34 @@ def run_reference(args, rank, world):
     return 0
 
 
+def rescale_compare(G, dev):
+    """One frame of each raw size below 1.2 A/px of the uneven batch through
+    gcf_rescale with the line transforms and with cuFFT; wall clock per call
+    (the rescaled frame is copied to the host by the call)."""
+    import numpy as np
+    import torch
+    ctx = G.Context(dev, 512, 0)
+    rng = np.random.default_rng(0)
+    out = []
+    for (w, h, px) in [(3838, 3710, 0.9), (5760, 4092, 0.8), (4096, 4096, 1.0)]:
+        img = torch.from_numpy(rng.poisson(2.0, size=(h, w)).astype(np.float32)).to(f"cuda:{dev}")
+        for name, impl in (("lines", G.GCF_RESCALE_LINES), ("cufft", G.GCF_RESCALE_CUFFT)):
+            ctx.set_rescale_impl(impl)
+            for _ in range(2):
+                ctx.rescale(img, px)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(5):
+                ctx.rescale(img, px)
+            torch.cuda.synchronize()
+            out.append({"raw": [w, h], "px": px, "impl": name,
+                        "wall_ms_per_call": round((time.perf_counter() - t0) / 5 * 1e3, 3)})
+    ctx.close()
+    print(json.dumps({"rescale_compare": out, "note": "wall clock includes the copy of the rescaled frame to "
+                      "the host; kernel times come from a profiler's launch list of this command"}))
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup()
@@ -554,6 +586,8 @@ def main():
     import torch
     import gctffind_b200 as G
     torch.cuda.set_device(local)
+    if args.rescale_compare:
+        return rescale_compare(G, local)
     ctx = G.Context(local, 512, 0)
     op = G.make_optics()
     # the project's autotuner picks the tile-kernel shape and the contraction
