@@ -338,7 +338,14 @@ k_fused_spectrum(const FusedTab* __restrict__ imgs, const int4* __restrict__ ite
             const double* bs = im.bsum + (size_t)ty * im.nbx + tx;
             const float mean = (float)((bs[0] + bs[1] + bs[im.nbx] + bs[im.nbx + 1]) / ((double)FT * FT));
             float2* colbuf = colbuf0 + (S::DB ? (size_t)par * (S::BUF / sizeof(float2)) : 0);
-            if (!S::DB) cluster.sync();   // peers are done reading this CTA's column buffer
+            // peers are done reading this CTA's column buffer: an execution
+            // barrier only (the values those reads returned were consumed by
+            // the column transforms before the arrive), so the arrive is
+            // relaxed and carries no memory fence
+            if (!S::DB) {
+                asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+                asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+            }
 
             // ---- row transforms: two rows per FFT, rows read straight from global ----
             // S::PF: the next row pair is loaded into registers while this one
