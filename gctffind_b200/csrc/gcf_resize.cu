@@ -124,12 +124,30 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int M, int Ns, const 
         if (j < groups) {
             const int k = j & (Ns - 1);
             if constexpr (TW) {
-                const int step = (M / (Ns * R)) << sh;   // in units of 2 pi / 8192
+                // w_r = exp(-2 pi i r q / 8192), q = k * step: w_1, w_2, w_4 and
+                // w_8 from the tables, every other w_r the product of at most
+                // four of them (a few float roundings, like the table pair)
+                static_assert(R == 16, "twiddled passes are radix 16");
+                const int q = k * ((M / (Ns * R)) << sh);   // in units of 2 pi / 8192
+                float2 wr[16];
 #pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const int q = r * k * step;
-                    v[g][r] = cmulf(v[g][r], cmulf(stw[kTwLo + (q >> 7)], stw[q & (kTwLo - 1)]));
+                for (int b = 1; b < 16; b <<= 1) {
+                    const int qb = b * q;
+                    wr[b] = cmulf(stw[kTwLo + (qb >> 7)], stw[qb & (kTwLo - 1)]);
                 }
+                wr[3] = cmulf(wr[2], wr[1]);
+                wr[5] = cmulf(wr[4], wr[1]);
+                wr[6] = cmulf(wr[4], wr[2]);
+                wr[7] = cmulf(wr[6], wr[1]);
+                wr[9] = cmulf(wr[8], wr[1]);
+                wr[10] = cmulf(wr[8], wr[2]);
+                wr[11] = cmulf(wr[10], wr[1]);
+                wr[12] = cmulf(wr[8], wr[4]);
+                wr[13] = cmulf(wr[12], wr[1]);
+                wr[14] = cmulf(wr[12], wr[2]);
+                wr[15] = cmulf(wr[14], wr[1]);
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[g][r] = cmulf(v[g][r], wr[r]);
             }
             dft_reg<R>(v[g]);
             const int base = (j - k) * R + k;

@@ -46,9 +46,12 @@ def test_line_rescale_matches_cufft(gpu_lib, w, h, px):
     assert _rel(a, b) <= 1e-5, _rel(a, b)
 
 
-def test_odd_raw_width_takes_the_cufft_path(gpu_lib):
+@pytest.mark.parametrize("w,h", [(1537, 1024), (1024, 5000)])
+def test_sizes_beyond_the_line_transforms_take_the_cufft_path(gpu_lib, w, h):
+    """An odd raw width, and a raw height above 4096 (a column line too
+    long): the cuFFT path runs, bit for bit."""
     G = gpu_lib
-    img = np.random.default_rng(5).poisson(2.0, size=(1024, 1537)).astype(np.float32)
+    img = np.random.default_rng(5).poisson(2.0, size=(h, w)).astype(np.float32)
     lines = G.Context(0, 512, 0)
     lines.set_rescale_impl(G.GCF_RESCALE_LINES)
     cufft = G.Context(0, 512, 0)
