@@ -32,7 +32,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <complex>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -369,23 +368,38 @@ cudaError_t launch_line(K kernel, int lines, size_t smem, int sms, cudaStream_t 
 // its filter spectrum stay allocated for the life of the process (a graph
 // captured with them keeps their addresses): about 100 KB per line length,
 // at most kResizeMaxLine lengths.
-void fft_host(std::vector<std::complex<double>>& a)   // forward, in place, size a power of two
+// Forward FFT in place of n = 2^k complex values held as interleaved
+// (re, im) doubles (explicit arithmetic: std::complex products check for
+// NaN and run several times slower).
+void fft_host(std::vector<double>& a)
 {
-    const size_t n = a.size();
+    const size_t n = a.size() / 2;
     for (size_t i = 1, j = 0; i < n; ++i) {
         size_t bit = n >> 1;
         for (; j & bit; bit >>= 1) j ^= bit;
         j ^= bit;
-        if (i < j) std::swap(a[i], a[j]);
+        if (i < j) {
+            std::swap(a[2 * i], a[2 * j]);
+            std::swap(a[2 * i + 1], a[2 * j + 1]);
+        }
+    }
+    std::vector<double> wr(n / 2), wi(n / 2);   // exp(-2 pi i k / n)
+    for (size_t k = 0; k < n / 2; ++k) {
+        wr[k] = std::cos(-2.0 * M_PI * (double)k / (double)n);
+        wi[k] = std::sin(-2.0 * M_PI * (double)k / (double)n);
     }
     for (size_t len = 2; len <= n; len <<= 1) {
-        const double ang = -2.0 * M_PI / (double)len;
+        const size_t half = len / 2, stride = n / len;
         for (size_t i = 0; i < n; i += len)
-            for (size_t k = 0; k < len / 2; ++k) {
-                const std::complex<double> w(std::cos(ang * k), std::sin(ang * k));
-                const std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
-                a[i + k] = u + v;
-                a[i + k + len / 2] = u - v;
+            for (size_t k = 0; k < half; ++k) {
+                double* u = &a[2 * (i + k)];
+                double* x = &a[2 * (i + k + half)];
+                const double tr = wr[k * stride], ti = wi[k * stride];
+                const double vr = x[0] * tr - x[1] * ti, vi = x[0] * ti + x[1] * tr;
+                x[0] = u[0] - vr;
+                x[1] = u[1] - vi;
+                u[0] += vr;
+                u[1] += vi;
             }
     }
 }
@@ -456,18 +470,23 @@ cudaError_t resize_line(int n, ResizeLine* out)
     if (!pow2) {
         // chirp c_j = exp(-i pi j^2 / n) (j^2 reduced mod 2n exactly), and
         // the spectrum of b (b_j = conj c_j for |j| < n, circular) over M
-        std::vector<std::complex<double>> cj(n), b(L.M, 0.0);
+        std::vector<double> cr(n), ci(n), b(2 * (size_t)L.M, 0.0);
         for (int j = 0; j < n; ++j) {
             const long long q = ((long long)j * j) % (2LL * n);
             const double a = -M_PI * (double)q / (double)n;
-            cj[j] = std::complex<double>(std::cos(a), std::sin(a));
+            cr[j] = std::cos(a);
+            ci[j] = std::sin(a);
         }
-        b[0] = std::conj(cj[0]);
-        for (int j = 1; j < n; ++j) b[j] = b[L.M - j] = std::conj(cj[j]);
+        b[0] = cr[0];
+        b[1] = -ci[0];
+        for (int j = 1; j < n; ++j) {
+            b[2 * j] = b[2 * (L.M - j)] = cr[j];
+            b[2 * j + 1] = b[2 * (L.M - j) + 1] = -ci[j];
+        }
         fft_host(b);
         std::vector<float2> hc(n), hb(L.M);
-        for (int j = 0; j < n; ++j) hc[j] = make_float2((float)cj[j].real(), (float)cj[j].imag());
-        for (int k = 0; k < L.M; ++k) hb[k] = make_float2((float)(b[k].real() / L.M), (float)(b[k].imag() / L.M));
+        for (int j = 0; j < n; ++j) hc[j] = make_float2((float)cr[j], (float)ci[j]);
+        for (int k = 0; k < L.M; ++k) hb[k] = make_float2((float)(b[2 * k] / L.M), (float)(b[2 * k + 1] / L.M));
         float2 *dc = nullptr, *db = nullptr;
         if ((e = upload(hc, &dc)) != cudaSuccess) return e;
         if ((e = upload(hb, &db)) != cudaSuccess) {
