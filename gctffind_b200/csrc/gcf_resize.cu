@@ -157,15 +157,9 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int M, int Ns, const 
     __syncthreads();
 }
 
-// Forward FFT of the padded line buf (length M, a power of two, 1..8192)
-// in place; stw: the twiddle tables in shared memory, sh = log2(8192 / M).
-// Entered and left synchronised.
-// Radix plan: the radix left over by the 16s (2, 4 or 8) first, where
-// Ns = 1 and no twiddles apply, then radix-16 passes of at most T groups.
-// Not inlined: each kernel calls it up to four times, and inlined copies
-// spill.
 // Groups per thread of a first pass of radix r: its largest length is the
-// largest r 16^k <= mmax (2 x 16^3 = 8192 gives 4096 groups, 16 per thread).
+// largest r 16^k <= mmax (2 x 16^3 = 8192 gives 4096 groups, 8 per thread
+// of 512).
 __host__ __device__ constexpr int first_pass_groups(int r, int mmax, int t)
 {
     int m = r;
@@ -173,6 +167,12 @@ __host__ __device__ constexpr int first_pass_groups(int r, int mmax, int t)
     return (m / r + t - 1) / t;
 }
 
+// Forward FFT of the padded line buf (length M, a power of two, 1..MMAX)
+// in place; stw: the twiddle tables in shared memory, sh = log2(8192 / M).
+// Entered and left synchronised.  Radix plan: the radix left over by the
+// 16s (2, 4 or 8) first, where Ns = 1 and no twiddles apply, then radix-16
+// passes of at most T groups.  Not inlined: each kernel calls it up to
+// four times, and inlined copies spill.
 template <int MMAX>
 __device__ __noinline__ void line_fft(float2* buf, int M, const float2* stw)
 {
