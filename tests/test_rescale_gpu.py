@@ -90,3 +90,11 @@ def test_batch_through_line_rescale(gpu_lib):
         assert abs(x.df_min - y.df_min) <= step and abs(x.df_max - y.df_max) <= step, (x, y)
         assert abs(x.score - y.score) <= 1e-3
     assert [r.as_dict() for r in b[2]] == [r.as_dict() for r in b[0]]
+
+
+def test_rescale_impl_rejects_unknown_values(gpu_lib):
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    with pytest.raises(G.GcfError):
+        ctx.set_rescale_impl(7)
+    ctx.close()
