@@ -175,3 +175,24 @@ def test_learned_batch_over_one_network_chunk(gpu_lib):
     assert float(np.median(ddf)) <= 20.0
     del imgs
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("mode_name", ["GCF_SEARCH_BF16", "GCF_SEARCH_LEARNED"])
+def test_fast_methods_on_a_single_micrograph(gpu_lib, mode_name):
+    """A batch of one: the table has one micrograph's angle bins, the tile
+    plan one column block; the result within one search step of the plain
+    search."""
+    G = gpu_lib
+    spec = synth.MicrographSpec(width=2048, height=2048, pixel_size=1.3, df_min=21800.0, df_max=22400.0,
+                                azimuth_deg=-35.0, dose=2.0, seed=808)
+    img = synth.make_micrograph(spec, device="cuda")
+    ctx = G.Context(0, 512, 0)
+    if mode_name == "GCF_SEARCH_LEARNED":
+        G.load_learned(ctx)
+    op = G.make_optics()
+    p = ctx.run_batch([img], [1.3], op, mode=G.GCF_SEARCH_PLAIN)[0]
+    f = ctx.run_batch([img], [1.3], op, mode=getattr(G, mode_name))[0]
+    ctx.close()
+    step = max(20.0, 0.105 * 0.5 * (p.df_min + p.df_max) / 31.0)
+    assert abs(f.df_min - p.df_min) <= step and abs(f.df_max - p.df_max) <= step, (p, f)
+    assert f.score >= p.score - 2e-3
