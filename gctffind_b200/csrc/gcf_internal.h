@@ -30,21 +30,26 @@ unsigned long long device_alloc_epoch();
 cudaError_t record_timing(cudaEvent_t ev, cudaStream_t st);
 
 // gcf_resize.cu: the Fourier-crop rescale as line transforms.  A line of
-// length n (<= kResizeMaxLine): FFT length M (n when a power of two, else
-// the power of two >= 2n - 1 of Bluestein's convolution), and for Bluestein
-// lines the chirp exp(-i pi j^2 / n) and the spectrum of its conjugate over
-// M, divided by M.
+// length n (<= kResizeMaxLine) is transformed whole, or (split = 1) as the
+// DFTs of its even and odd samples combined by one radix-2 step with the
+// twiddles ts[k] = exp(-2 pi i k / n), k < n/2.  The transform of length
+// n (or n/2 when split): FFT length M (that length when a power of two,
+// else the power of two >= 2 length - 1 of Bluestein's convolution), and for
+// Bluestein the chirp exp(-i pi j^2 / length) and the spectrum of its
+// conjugate over M, divided by M.
 constexpr int kResizeMaxLine = 4096;
 struct ResizeLine {
     int n, M;
     const float2* chirp;
     const float2* bf;
+    int split;
+    const float2* ts;
 };
 bool resize_line_ok(int n);
 cudaError_t resize_line(int n, ResizeLine* out);
 // exp(sign 2 pi i k / len), k < count
 cudaError_t resize_twiddles(int len, int sign, int count, const float2** out);
-size_t resize_cols_smem(int h, int m_max);
+size_t resize_cols_smem(int h, int m_max, int e_max);
 // img (w x h, w even) -> out (nw x nh); T1: (nw/2 + 1) x h, T2: (nw/2 + 1) x nh
 // complex scratch; tA = exp(-2 pi i k / w), k <= w/2; tC = exp(2 pi i k / nw),
 // k < nw/2.

@@ -224,6 +224,36 @@ __device__ __forceinline__ float2 line_out(const float2* buf, const ResizeLine& 
     return L.chirp ? cmulf(conjf2(buf[lpad(k)]), __ldg(L.chirp + k)) : buf[lpad(k)];
 }
 
+// A line that may be split (L.split): the DFT of its even samples into ebuf
+// (n/2 values), then that of its odd samples into buf; line_out_s combines.
+template <int MMAX, class Load>
+__device__ __forceinline__ void line_dft_s(float2* buf, float2* ebuf, const ResizeLine& L, const float2* stw,
+                                           Load load)
+{
+    if (!L.split) {
+        line_dft<MMAX>(buf, L, stw, load);
+        return;
+    }
+    ResizeLine H = L;
+    H.n = L.n / 2;
+    line_dft<MMAX>(buf, H, stw, [&](int i) { return load(2 * i); });
+    for (int k = threadIdx.x; k < H.n; k += LineThreads<MMAX>::T) ebuf[k] = line_out(buf, H, k);
+    __syncthreads();
+    line_dft<MMAX>(buf, H, stw, [&](int i) { return load(2 * i + 1); });
+}
+
+// Output k (< L.n) of the last line_dft_s: X_k = E_k + t_k O_k and
+// X_{k + n/2} = E_k - t_k O_k, t_k = exp(-2 pi i k / n).
+__device__ __forceinline__ float2 line_out_s(const float2* buf, const float2* ebuf, const ResizeLine& L, int k)
+{
+    if (!L.split) return line_out(buf, L, k);
+    ResizeLine H = L;
+    H.n = L.n / 2;
+    const int kk = k < H.n ? k : k - H.n;
+    const float2 e = ebuf[kk], o = cmulf(line_out(buf, H, kk), __ldg(L.ts + kk));
+    return k < H.n ? addf2(e, o) : subf2(e, o);
+}
+
 // Pass A: raw rows (w even) -> T1[y][k], k < K = nw/2 + 1.
 template <int MMAX>
 __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>::T) k_resize_rows_fwd(const float* __restrict__ img, int w, int h, int vec,
@@ -233,19 +263,21 @@ __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>:
     extern __shared__ float2 rbuf[];
     __shared__ float2 stw[kTwN];
     load_twiddles<LineThreads<MMAX>::T>(stw, tw2);
+    float2* ebuf = rbuf + La.M + La.M / 16;   // even-sample DFT of a split line
     const int N = w / 2;
     for (int y = blockIdx.x; y < h; y += gridDim.x) {
         const float* row = img + (size_t)y * w;
         if (vec) {
             const float2* r2 = reinterpret_cast<const float2*>(row);
-            line_dft<MMAX>(rbuf, La, stw, [&](int i) { return __ldg(r2 + i); });
+            line_dft_s<MMAX>(rbuf, ebuf, La, stw, [&](int i) { return __ldg(r2 + i); });
         } else {
-            line_dft<MMAX>(rbuf, La, stw, [&](int i) { return make_float2(__ldg(row + 2 * i), __ldg(row + 2 * i + 1)); });
+            line_dft_s<MMAX>(rbuf, ebuf, La, stw,
+                             [&](int i) { return make_float2(__ldg(row + 2 * i), __ldg(row + 2 * i + 1)); });
         }
         // X_k = ((Z_k + conj Z_{N-k}) - i t_k (Z_k - conj Z_{N-k})) / 2, t_k = exp(-2 pi i k / w)
         for (int k = threadIdx.x; k < K; k += LineThreads<MMAX>::T) {
-            const float2 zk = line_out(rbuf, La, k < N ? k : k - N);
-            const float2 zn = conjf2(line_out(rbuf, La, k == 0 ? 0 : N - k));
+            const float2 zk = line_out_s(rbuf, ebuf, La, k < N ? k : k - N);
+            const float2 zn = conjf2(line_out_s(rbuf, ebuf, La, k == 0 ? 0 : N - k));
             const float2 s = addf2(zk, zn), t = cmulf(__ldg(tA + k), subf2(zk, zn));
             T1[(size_t)y * K + k] = make_float2(0.5f * (s.x + t.y), 0.5f * (s.y - t.x));
         }
@@ -264,6 +296,8 @@ __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>:
     load_twiddles<LineThreads<MMAX>::T>(stw, tw2);
     float2* stash = cbuf;                          // [kColGroup][hs]
     float2* buf = cbuf + (size_t)kColGroup * hs;   // the line
+    const int mb = max(Lf.M, Li.M);
+    float2* ebuf = buf + mb + mb / 16;             // even-sample DFT of a split line
     for (int k0 = blockIdx.x * kColGroup; k0 < K; k0 += gridDim.x * kColGroup) {
         const int cb = min(kColGroup, K - k0);
 #pragma unroll 8
@@ -274,13 +308,14 @@ __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>:
         __syncthreads();
         for (int c = 0; c < cb; ++c) {
             float2* col = stash + c * hs;
-            line_dft<MMAX>(buf, Lf, stw, [&](int i) { return col[i]; });
+            line_dft_s<MMAX>(buf, ebuf, Lf, stw, [&](int i) { return col[i]; });
             // the kept frequencies, conjugated for the inverse transform
             for (int m = threadIdx.x; m < nh; m += LineThreads<MMAX>::T)
-                col[m] = conjf2(line_out(buf, Lf, m <= nh / 2 ? m : m - nh + h));
+                col[m] = conjf2(line_out_s(buf, ebuf, Lf, m <= nh / 2 ? m : m - nh + h));
             __syncthreads();
-            line_dft<MMAX>(buf, Li, stw, [&](int i) { return col[i]; });
-            for (int m = threadIdx.x; m < nh; m += LineThreads<MMAX>::T) col[m] = conjf2(line_out(buf, Li, m));
+            line_dft_s<MMAX>(buf, ebuf, Li, stw, [&](int i) { return col[i]; });
+            for (int m = threadIdx.x; m < nh; m += LineThreads<MMAX>::T)
+                col[m] = conjf2(line_out_s(buf, ebuf, Li, m));
             __syncthreads();
         }
         for (int i = threadIdx.x; i < nh * kColGroup; i += LineThreads<MMAX>::T) {
@@ -306,9 +341,10 @@ __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>:
     __shared__ float2 stw[kTwN];
     load_twiddles<LineThreads<MMAX>::T>(stw, tw2);
     const int Nn = nw / 2;
+    float2* ebuf = rbuf + Lc.M + Lc.M / 16;   // even-sample DFT of a split line
     for (int y = blockIdx.x; y < nh; y += gridDim.x) {
         const float2* Y = T2 + (size_t)y * K;
-        line_dft<MMAX>(rbuf, Lc, stw, [&](int k) {
+        line_dft_s<MMAX>(rbuf, ebuf, Lc, stw, [&](int k) {
             float2 a = Y[k], b = Y[Nn - k];
             if (k == 0) {   // Y_0 and Y_Nn: real parts only
                 a.y = 0.0f;
@@ -319,7 +355,7 @@ __global__ void __launch_bounds__(LineThreads<MMAX>::T, 512 / LineThreads<MMAX>:
             return make_float2(s.x - t.y, -(s.y + t.x));   // conjugated: the inverse through the forward DFT
         });
         float2* o2 = reinterpret_cast<float2*>(out + (size_t)y * nw);
-        for (int m = threadIdx.x; m < Nn; m += LineThreads<MMAX>::T) o2[m] = conjf2(line_out(rbuf, Lc, m));
+        for (int m = threadIdx.x; m < Nn; m += LineThreads<MMAX>::T) o2[m] = conjf2(line_out_s(rbuf, ebuf, Lc, m));
         __syncthreads();
     }
 }
@@ -448,19 +484,16 @@ cudaError_t twiddles_locked(TabCache& c, int dev, int len, int sign, int count, 
 
 bool resize_line_ok(int n) { return n >= 1 && n <= kResizeMaxLine; }
 
-cudaError_t resize_line(int n, ResizeLine* out)
+namespace {
+// The tables of a line of length n transformed whole (held in the lock).
+cudaError_t whole_line_locked(TabCache& c, int dev, int n, ResizeLine* out)
 {
-    if (!resize_line_ok(n)) return cudaErrorInvalidValue;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    TabCache& c = tabs();
-    std::lock_guard<std::mutex> lock(c.mu);
     auto it = c.lines.find({dev, n});
     if (it != c.lines.end()) {
         *out = it->second;
         return cudaSuccess;
     }
+    cudaError_t e = cudaSuccess;
     ResizeLine L{};
     L.n = n;
     const bool pow2 = (n & (n - 1)) == 0;
@@ -499,6 +532,34 @@ cudaError_t resize_line(int n, ResizeLine* out)
     c.lines[{dev, n}] = L;
     *out = L;
     return cudaSuccess;
+}
+}  // namespace
+
+// An even length above 2048 that is not a power of two (whose Bluestein
+// FFT would be 8192 long) is split: the DFTs of its even and odd samples
+// (length n/2, FFTs of at most 4096) and one radix-2 step with the twiddles
+// exp(-2 pi i k / n), k < n/2.
+cudaError_t resize_line(int n, ResizeLine* out)
+{
+    if (!resize_line_ok(n)) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    TabCache& c = tabs();
+    std::lock_guard<std::mutex> lock(c.mu);
+    const bool pow2 = (n & (n - 1)) == 0;
+    if (n % 2 == 0 && n > 2048 && !pow2) {
+        ResizeLine H{};
+        if ((e = whole_line_locked(c, dev, n / 2, &H)) != cudaSuccess) return e;
+        float2* ts = nullptr;
+        if ((e = twiddles_locked(c, dev, n, -1, n / 2, &ts)) != cudaSuccess) return e;
+        H.n = n;
+        H.split = 1;
+        H.ts = ts;
+        *out = H;
+        return cudaSuccess;
+    }
+    return whole_line_locked(c, dev, n, out);
 }
 
 // lo[t] = exp(-2 pi i t / 8192), t < 128, then hi[u] = exp(-2 pi i u / 64), u < 64
@@ -547,10 +608,10 @@ cudaError_t resize_twiddles(int len, int sign, int count, const float2** out)
     return e;
 }
 
-size_t resize_cols_smem(int h, int m_max)
+size_t resize_cols_smem(int h, int m_max, int e_max)
 {
     const int hs = h + ((h & 1) ? 0 : 1);
-    return (size_t)kColGroup * hs * sizeof(float2) + line_smem(m_max);
+    return (size_t)kColGroup * hs * sizeof(float2) + line_smem(m_max) + (size_t)e_max * sizeof(float2);
 }
 
 cudaError_t launch_resize(const float* img, int w, int h, int nw, int nh, const ResizeLine& rowA,
@@ -564,8 +625,10 @@ cudaError_t launch_resize(const float* img, int w, int h, int nw, int nh, const 
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int K = nw / 2 + 1;
     const int vec = ((reinterpret_cast<uintptr_t>(img) & 7) == 0) ? 1 : 0;
-    const size_t sa = line_smem(rowA.M), sc = line_smem(rowC.M);
-    const size_t sb = resize_cols_smem(h, std::max(colF.M, colI.M));
+    auto ehalf = [](const ResizeLine& L) { return L.split ? L.n / 2 : 0; };
+    const size_t sa = line_smem(rowA.M) + ehalf(rowA) * sizeof(float2);
+    const size_t sc = line_smem(rowC.M) + ehalf(rowC) * sizeof(float2);
+    const size_t sb = resize_cols_smem(h, std::max(colF.M, colI.M), std::max(ehalf(colF), ehalf(colI)));
     const int hs = h + ((h & 1) ? 0 : 1);
     const float2* tw2 = nullptr;
     if ((e = resize_fft_twiddles(&tw2)) != cudaSuccess) return e;
