@@ -455,7 +455,12 @@ cudaError_t upload(const std::vector<float2>& h, float2** d)
 {
     cudaError_t e = cudaMalloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(float2));
     if (e != cudaSuccess) return e;
-    return cudaMemcpy(*d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(*d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(*d);
+        *d = nullptr;
+    }
+    return e;
 }
 
 // exp(sign 2 pi i k / len), k < count (held in the cache's lock)
