@@ -18,7 +18,9 @@ built from its sources (oracle/_ref/libgcfref.so) and the FP64 oracle.
   envelope -- mean defocus below the 1D search floor 3000 * px^2 A
   (FindCTF/CFindCtf1D.cpp:78-79) or an astigmatism ratio above the full
   search's 0.06 (FindCTF/CFindDefocus2D.cpp:117-118) -- are counted and left
-  out of the comparison.
+  out of the comparison.  The same draw through the BF16 contraction and the
+  learned search, and the plain search with the line-transform rescale, each
+  against the reference.
 
 Accuracy bar (the path's): defocus within one search step of the reference's
 last mean-defocus line search, max(20 A, 0.105 * mean / 31); azimuth 1 degree
@@ -113,16 +115,38 @@ def test_uneven_batch_draw_matches_reference(gpu_lib, ref):
     specs = synth.uneven_batch_specs(32, 7)
     imgs = [synth.make_micrograph(s, device="cuda").cpu().numpy() for s in specs]
     torch.cuda.empty_cache()
+    pxs = [s.pixel_size for s in specs]
+    op = G.make_optics()
     ctx = G.Context(0, 512, 0)
-    mine = ctx.run_batch(imgs, [s.pixel_size for s in specs], G.make_optics())
+    mine = ctx.run_batch(imgs, pxs, op)
+    bf16 = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_BF16)
+    G.load_learned(ctx)
+    learned = ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_LEARNED)
     ctx.close()
+    lines = G.Context(0, 512, 0)
+    lines.set_rescale_impl(G.GCF_RESCALE_LINES)
+    mine_lines = lines.run_batch(imgs, pxs, op)
+    lines.close()
     checked = excluded = 0
-    for img, s, r in zip(imgs, specs, mine):
+    within = {"bf16": [], "learned": [], "lines": []}
+    for k, (img, s, r) in enumerate(zip(imgs, specs, mine)):
         if not synth.inside_reference_envelope(s):
             excluded += 1
             continue
         R, _, _ = ref.run_series([img], s.pixel_size, [0], is_tomo=False, tile=512)
-        _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], [float(x) for x in R[0]])
+        ref_row = [float(x) for x in R[0]]
+        _close([r.df_min, r.df_max, r.azimuth, r.ext_phase, r.score], ref_row)
+        step = max(20.0, 0.105 * 0.5 * (ref_row[0] + ref_row[1]) / 31.0)
+        for name, res in (("bf16", bf16), ("learned", learned), ("lines", mine_lines)):
+            f = res[k]
+            within[name].append(abs(f.df_min - ref_row[0]) <= step and abs(f.df_max - ref_row[1]) <= step)
         checked += 1
-    print(f"uneven batch draw: {checked} compared, {excluded} outside the reference envelope")
+    print(f"uneven batch draw: {checked} compared, {excluded} outside the reference envelope; "
+          f"within one step of the reference: " + ", ".join(f"{k} {np.mean(v):.3f}" for k, v in within.items()))
     assert checked >= 24
+    # the faster methods against the reference itself: the headline path's
+    # accuracy bar (>= 99 % within one step on the 256-micrograph batch) at
+    # this sample size allows one miss; the line-transform rescale changes
+    # only rounding, so the plain search through it lands with the reference
+    assert sum(not x for x in within["bf16"]) <= 1 and sum(not x for x in within["learned"]) <= 1, within
+    assert all(within["lines"]), within["lines"]
