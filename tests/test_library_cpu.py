@@ -39,6 +39,22 @@ def test_strerror_codes():
     assert L.gcf_strerror(5) == b"image smaller than one tile"
 
 
+def test_entry_points_reject_a_missing_context():
+    """Entry points that take a context return GCF_ERR_INVALID_ARG (1) for a
+    NULL one, before touching any device."""
+    import ctypes as C
+    L = G.load_library()
+    f = (C.c_float * 8)()
+    ll = (C.c_longlong * 8)()
+    assert L.gcf_set_rescale_impl(None, 0) == 1
+    assert L.gcf_set_fused_shape(None, 8) == 1
+    assert L.gcf_set_graphs(None, 1) == 1
+    assert L.gcf_get_fast_times(None, f) == 1
+    assert L.gcf_get_fast_counts(None, ll) == 1
+    assert L.gcf_get_stage_times(None, f) == 1
+    assert L.gcf_nn_inputs(None, f, f, 1, f, f) == 1
+
+
 def test_rescale_dims_like_crescaleimage():
     # CRescaleImage::Setup (FindCTF/CRescaleImage.cpp:47-66), float32 arithmetic
     assert G.rescale_dims(4096, 4096, 1.0)[:2] == (3412, 3412)
