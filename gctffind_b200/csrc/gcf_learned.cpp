@@ -214,8 +214,24 @@ static cudaError_t layer_fwd(NnNet* n, int li, const __nv_bfloat16* in, int rows
     g.bias = n->w.p + l.off + (size_t)l.out * l.in;
     g.relu = relu ? 1 : 0;
     g.err = n->err.p;
-    const int bn = l.out <= 32 ? 32 : (l.out <= 64 ? 64 : (l.out <= 128 ? 128 : 256));
-    return launch_umma_gemm(in, l.in, n->wb.p + n->wb_off[li], l.in, g, bn, bn == 256 ? 3 : 4, 0, st);
+    // Tile width: the layer's width, narrowed while the product would have
+    // fewer than 64 tiles (the MLP's few batch rows would otherwise run on a
+    // couple of CTAs); every output element sums the same products in the
+    // same order whatever the tile.  Layers of many tiles (the convolutions'
+    // im2col rows) take the persistent kernel, one CTA per SM, whose
+    // epilogue of one tile overlaps the products of the next.
+    const int mt = (rows + 127) / 128;
+    int bn = l.out <= 32 ? 32 : (l.out <= 64 ? 64 : (l.out <= 128 ? 128 : 256));
+    while (bn > 32 && mt * ((l.out + bn - 1) / bn) < 64) bn /= 2;
+    const int stages = bn == 256 ? 3 : 4;
+    const __nv_bfloat16* w = n->wb.p + n->wb_off[li];
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (mt * ((l.out + bn - 1) / bn) > 2 * sms)
+        return launch_umma_gemm_persistent(in, l.in, w, l.in, g, bn, stages, 0, st);
+    return launch_umma_gemm(in, l.in, w, l.in, g, bn, stages, 0, st);
 }
 
 cudaError_t nn_forward(NnNet* n, const __nv_bfloat16* x1, const __nv_bfloat16* x2, int B, cudaStream_t st)

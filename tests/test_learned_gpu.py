@@ -51,6 +51,27 @@ def test_gradients_match_oracle(gpu_lib):
                 assert rel <= rel_bar and cos >= cos_bar, (emulate, k, rel, cos)
 
 
+def test_forward_through_the_persistent_product(gpu_lib):
+    """40 samples: the first two convolutions have 1280 and 320 tiles of 128
+    im2col rows, enough for the persistent tensor-core product (one CTA per
+    SM); loss and predictions against the BF16-emulating oracle as in the
+    gradient check."""
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    ctx.nn_init(13)
+    op = G.make_optics()
+    x1, x2, t, p = ctx.nn_synth_inputs(op, seed=9, first=0, n=40)
+    params = ctx.nn_params()
+    loss, grads, pred = ctx.nn_forward_backward(x1, x2, t)
+    ctx.close()
+    oloss, ograds, opred = N.forward_backward(params, N.bf16(x1), N.bf16(x2), t, emulate_bf16=True)
+    assert abs(loss - oloss) <= 2e-2 * abs(oloss), (loss, oloss)
+    assert np.abs(pred - opred).max() <= 2e-2 * (np.abs(opred).max() + 1e-3)
+    for (gw, gb), (ow, ob) in zip(N.split(grads), N.split(ograds)):
+        a, b = gw.ravel().astype(np.float64), ow.ravel()
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b)
+
+
 @pytest.mark.parametrize("px", [1.2, 1.35, 1.5])
 def test_network_inputs_match_oracle(gpu_lib, px):
     """The polar binning of a background-removed half spectrum (k_nn_input)
