@@ -1457,7 +1457,7 @@ gcf_status learned_priors(gcf_ctx* ctx, const std::vector<float>& px_n)
         CK(nn_forward(ctx->nn, ctx->nx1.p, ctx->nx2.p, cn, ctx->st));
         launch_prior(nn_pred(ctx->nn), kNnPredPitch, cn, ctx->cPrior.p + c0, ctx->st);
         CKL();
-        ctx->launches += 14;   // inputs, 4 im2col, 7 products, concat, prior
+        ctx->launches += 13;   // inputs, first layer, 3 im2col, 6 products, concat, prior
     }
     CK(record_timing(ctx->fev[6], ctx->st));
     return GCF_OK;

@@ -364,6 +364,10 @@ void launch_synth_params(unsigned long long seed, unsigned long long first, int 
 void launch_synth_raw(unsigned long long seed, unsigned long long first, const float* params, int n, int tile,
                       const PixOptics& base, float* raw, cudaStream_t st);
 void launch_im2col_p4(const __nv_bfloat16* x, int B, __nv_bfloat16* cols, cudaStream_t st);
+// the first layer (4 x 4 stride-4 patches of x, 16 outputs, bias + ReLU)
+// without im2col rows; w: [16][16] BF16
+void launch_conv1_direct(const __nv_bfloat16* x, int B, const __nv_bfloat16* w, const float* bias,
+                         __nv_bfloat16* y, cudaStream_t st);
 void launch_im2col_3s2(const __nv_bfloat16* x, int B, int H, int W, int C, __nv_bfloat16* cols, cudaStream_t st);
 void launch_col2im_3s2_relu(const float* dcols, const __nv_bfloat16* y, int B, int H, int W, int C,
                             __nv_bfloat16* dz, cudaStream_t st);

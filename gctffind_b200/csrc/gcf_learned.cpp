@@ -240,8 +240,10 @@ cudaError_t nn_forward(NnNet* n, const __nv_bfloat16* x1, const __nv_bfloat16* x
     if (e != cudaSuccess) return e;
     n->x1 = x1;
     n->x2 = x2;
-    launch_im2col_p4(x2, B, n->cols1.p, st);
-    if ((e = layer_fwd(n, 0, n->cols1.p, B * 4096, n->y1.p, nullptr, 16, true, st)) != cudaSuccess) return e;
+    // the first layer (K = N = 16) on CUDA cores: as a tensor-core product of
+    // im2col rows its tiles are too small to keep the pipeline busy
+    launch_conv1_direct(x2, B, n->wb.p + n->wb_off[0], n->w.p + n->L[0].off + (size_t)n->L[0].out * n->L[0].in,
+                        n->y1.p, st);
     launch_im2col_3s2(n->y1.p, B, 64, 64, 16, n->cols2.p, st);
     if ((e = layer_fwd(n, 1, n->cols2.p, B * 1024, n->y2.p, nullptr, 32, true, st)) != cudaSuccess) return e;
     launch_im2col_3s2(n->y2.p, B, 32, 32, 32, n->cols3.p, st);
@@ -309,7 +311,9 @@ cudaError_t nn_backward(NnNet* n, const float* target, int B, float* loss, cudaS
     layer_dw(n, 1, n->dz_a.p, 32, n->cols2.p, B * 1024, st);
     if ((e = layer_dx(n, 1, n->dz_a.p, 32, B * 1024, n->fbuf.p, st)) != cudaSuccess) return e;
     launch_col2im_3s2_relu(n->fbuf.p, n->y1.p, B, 64, 64, 16, n->dz_b.p, st);
-    // conv1 (its input needs no gradient)
+    // conv1 (its input needs no gradient): its im2col rows for the weight
+    // gradient (the forward reads the input directly)
+    launch_im2col_p4(n->x2, B, n->cols1.p, st);
     layer_dw(n, 0, n->dz_b.p, 16, n->cols1.p, B * 4096, st);
     return cudaGetLastError();
 }

@@ -303,6 +303,52 @@ __global__ void k_im2col_p4(const __nv_bfloat16* __restrict__ x, int B, __nv_bfl
     }
 }
 
+// The first layer directly (no im2col rows): output row (b, oy, ox) is
+// ReLU(bias + W x) for the 16 pixels x of patch (oy, ox) in (ky, kx) order,
+// as the tensor-core product of those rows computes it (FP32 sums of the
+// BF16 products, rounded to BF16); W is [16 out][16 in] BF16.  One thread
+// per output row: four 8-byte patch-row loads, 256 FMAs, two 16-byte
+// stores.
+__global__ void __launch_bounds__(256) k_conv1_direct(const __nv_bfloat16* __restrict__ x, int B,
+                                                      const __nv_bfloat16* __restrict__ w,
+                                                      const float* __restrict__ bias,
+                                                      __nv_bfloat16* __restrict__ y)
+{
+    __shared__ float sw[16][17];
+    __shared__ float sb[16];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sw[i >> 4][i & 15] = __bfloat162float(w[i]);
+    if (threadIdx.x < 16) sb[threadIdx.x] = bias[threadIdx.x];
+    __syncthreads();
+    const long long n = (long long)B * 4096;
+    const uint2* __restrict__ xv = reinterpret_cast<const uint2*>(x);
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+        const int ox = (int)(r & 63), oy = (int)((r >> 6) & 63);
+        const long long b = r >> 12;
+        float in[16];
+#pragma unroll
+        for (int ky = 0; ky < 4; ++ky) {
+            const uint2 q = xv[(size_t)b * 16384 + (oy * 4 + ky) * 64 + ox];
+            const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&q.x);
+            const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&q.y);
+            in[4 * ky + 0] = __low2float(lo);
+            in[4 * ky + 1] = __high2float(lo);
+            in[4 * ky + 2] = __low2float(hi);
+            in[4 * ky + 3] = __high2float(hi);
+        }
+        __align__(16) __nv_bfloat16 o[16];
+#pragma unroll 2
+        for (int c = 0; c < 16; ++c) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) acc = fmaf(sw[c][k], in[k], acc);
+            o[c] = __float2bfloat16_rn(fmaxf(acc + sb[c], 0.0f));
+        }
+        uint4* yv = reinterpret_cast<uint4*>(y + (size_t)r * 16);
+        yv[0] = *reinterpret_cast<const uint4*>(&o[0]);
+        yv[1] = *reinterpret_cast<const uint4*>(&o[8]);
+    }
+}
+
 // im2col of a 3 x 3 stride-2 pad-1 layer on channel-last [B][H][W][C]:
 // row (b, oy, ox), column (ky * 3 + kx) * C + c.  One thread per (row, tap,
 // 8 channels): 16 bytes in and out (C a multiple of 8).
@@ -522,6 +568,12 @@ void launch_synth_raw(unsigned long long seed, unsigned long long first, const f
 void launch_im2col_p4(const __nv_bfloat16* x, int B, __nv_bfloat16* cols, cudaStream_t st)
 {
     k_im2col_p4<<<grid_for((long long)B * 4096 * 4, 256), 256, 0, st>>>(x, B, cols);
+}
+
+void launch_conv1_direct(const __nv_bfloat16* x, int B, const __nv_bfloat16* w, const float* bias,
+                         __nv_bfloat16* y, cudaStream_t st)
+{
+    k_conv1_direct<<<grid_for((long long)B * 4096, 256), 256, 0, st>>>(x, B, w, bias, y);
 }
 
 void launch_im2col_3s2(const __nv_bfloat16* x, int B, int H, int W, int C, __nv_bfloat16* cols, cudaStream_t st)
