@@ -112,15 +112,26 @@ k_nn_input(const float* __restrict__ ctf, int tile, const float* __restrict__ px
                 if (s2 < s2lo || s2 >= s2hi) continue;
                 const int k = min(max((int)((s2 - s2lo) / ds2), 0), 255);
                 const int t = min(max((int)((atan2f(fy, fx) + 0.5f * kPiF) * (256.0f / kPiF)), 0), 255);
-                const float v = S[(size_t)y * cx + x];
-                atomicAdd(&s_prof[k], v);
-                atomicAdd(&s_pcnt[k], 1);
                 if ((t >> 7) != half) continue;
+                const float v = S[(size_t)y * cx + x];
                 const int c = (t & 127) * 256 + k;
                 atomicAdd(&sum[c], v);
                 // counts stay below 65536: at most a few hundred pixels per cell
                 atomicAdd(reinterpret_cast<unsigned int*>(&cnt[c & ~1]), (c & 1) ? 65536u : 1u);
             }
+        }
+        __syncthreads();
+        // the profile's sums from this half's cells (every band pixel is in
+        // exactly one cell of one half)
+        for (int k = threadIdx.x; k < 256; k += blockDim.x) {
+            float ps = 0.0f;
+            int pc = 0;
+            for (int t = 0; t < 128; ++t) {
+                ps += sum[t * 256 + k];
+                pc += cnt[t * 256 + k];
+            }
+            s_prof[k] += ps;
+            s_pcnt[k] += pc;
         }
         __syncthreads();
         for (int i = threadIdx.x; i < 128 * 256; i += blockDim.x) {
