@@ -48,7 +48,8 @@ __global__ void k_polar_model(PolarGrid g, __nv_bfloat16* __restrict__ A, __nv_b
 
 // One CTA per job: the job's background-removed half spectrum (tile/2+1
 // columns x tile rows, DC at (0, tile/2)) summed into (s^2, angle) cells in
-// shared memory [t][k], then written as envelope-weighted BF16 rows.
+// shared memory [t][k], then written as envelope-weighted BF16 rows.  One
+// warp per row over the row's in-band columns.
 __global__ void __launch_bounds__(1024)
 k_polar_bin(const float* __restrict__ ctf, int tile, const SearchJob* __restrict__ jobs, PolarGrid g,
             __nv_bfloat16* __restrict__ B, __nv_bfloat16* __restrict__ E, double* __restrict__ ss)
@@ -67,23 +68,36 @@ k_polar_bin(const float* __restrict__ ctf, int tile, const SearchJob* __restrict
     const float inv_px2 = 1.0f / (px * px);
     const float s2_hi = g.s2_lo + g.ns * g.ds2;
     const float th_scale = (float)g.nth / (float)kPiD;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     double acc = 0.0;
-    for (int p = threadIdx.x; p < cx * cy; p += blockDim.x) {
-        const int y = p / cx, x = p - y * cx;
-        const float fx = (float)x / (float)tile, fy = (float)(y - cy / 2) / (float)tile;
-        const float s2 = (fx * fx + fy * fy) * inv_px2;
-        if (s2 < g.s2_lo || s2 >= s2_hi) continue;
-        int k = (int)((s2 - g.s2_lo) / g.ds2);
-        k = min(max(k, 0), g.ns - 1);
-        // angle from +x towards +y (row index), the convention of
-        // GCalcCTF2D (FindCTF/GCalcCTF2D.cu:20-27): [-90, 90] degrees
-        const float th = atan2f(fy, fx);
-        int t = (int)((th + 0.5f * (float)kPiD) * th_scale);
-        t = min(max(t, 0), g.nth - 1);
-        const float v = S[p];
-        atomicAdd(&cell[t * g.ns + k], v);
-        atomicAdd(&cnt[k], 1);
-        acc += (double)v * v;
+    // one warp per row, over the row's columns whose s^2 can be in the band
+    // (one column of slack each side; the exact test below decides)
+    for (int y = warp; y < cy; y += nwarps) {
+        const float fy = (float)(y - cy / 2) / (float)tile;
+        const float alo = g.s2_lo * px * px - fy * fy, ahi = s2_hi * px * px - fy * fy;
+        const int xlo = alo > 0.0f ? max((int)(sqrtf(alo) * (float)tile) - 1, 0) : 0;
+        const int xhi = min(ahi > 0.0f ? (int)(sqrtf(ahi) * (float)tile) + 2 : 2, cx);
+        for (int x0 = xlo; x0 < xhi; x0 += 32) {
+            const int x = x0 + lane;
+            const float fx = (float)x / (float)tile;
+            const float s2 = (fx * fx + fy * fy) * inv_px2;
+            const bool in = x < xhi && s2 >= g.s2_lo && s2 < s2_hi;
+            int k = -1;
+            if (in) {
+                k = min(max((int)((s2 - g.s2_lo) / g.ds2), 0), g.ns - 1);
+                // angle from +x towards +y (row index), the convention of
+                // GCalcCTF2D (FindCTF/GCalcCTF2D.cu:20-27): [-90, 90] degrees
+                const float th = atan2f(fy, fx);
+                int t = (int)((th + 0.5f * (float)kPiD) * th_scale);
+                t = min(max(t, 0), g.nth - 1);
+                const float v = S[(size_t)y * cx + x];
+                atomicAdd(&cell[t * g.ns + k], v);
+                acc += (double)v * v;
+            }
+            // the s^2 counts: one atomic per run of equal bins in the warp
+            const unsigned grp = __match_any_sync(0xffffffffu, k);
+            if (in && lane == __ffs(grp) - 1) atomicAdd(&cnt[k], __popc(grp));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
