@@ -88,14 +88,15 @@ __global__ void k_finalize_raw(const double* __restrict__ acc, int n, double inv
 }
 
 // GFtResize2D::mGTruncate without summation (Util/GFtResize2D.cu:7-32).
+// One output row per blockIdx.y (its source row computed once), columns
+// over the threads of blockIdx.x.
 __global__ void k_fourier_crop(const float2* __restrict__ in, int cx_in, int cy_in,
                                float2* __restrict__ out, int cx_out, int cy_out)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= cx_out * cy_out) return;
-    int y = i / cx_out, x = i - y * cx_out;
-    int ys = (y > cy_out / 2) ? y - cy_out + cy_in : y;
-    out[i] = in[(size_t)ys * cx_in + x];
+    const int y = blockIdx.y, x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= cx_out) return;
+    const int ys = (y > cy_out / 2) ? y - cy_out + cy_in : y;
+    out[(size_t)y * cx_out + x] = __ldg(in + (size_t)ys * cx_in + x);
 }
 
 }  // namespace
@@ -125,8 +126,8 @@ void launch_finalize_raw(const double* acc, int n, double inv, float* raw, cudaS
 void launch_fourier_crop(const float2* in, int cx_in, int cy_in, float2* out, int cx_out,
                          int cy_out, cudaStream_t st)
 {
-    int n = cx_out * cy_out;
-    k_fourier_crop<<<(n + 255) / 256, 256, 0, st>>>(in, cx_in, cy_in, out, cx_out, cy_out);
+    const dim3 grid((cx_out + 255) / 256, cy_out);
+    k_fourier_crop<<<grid, 256, 0, st>>>(in, cx_in, cy_in, out, cx_out, cy_out);
 }
 
 }  // namespace gcf
