@@ -216,6 +216,7 @@ struct gcf_ctx {
     // buffers
     DBuf<float> images, rescaled, tiles;
     DBuf<float2> cmp, rs_cmp, rs_crop;
+    DBuf<float> rs_src;   // an aligned copy of a device image cuFFT cannot read in place
     DBuf<double> acc, hsum, moments, moments2;
     DBuf<float> lpfull;
     DBuf<float2> lpcmp;
@@ -1612,6 +1613,13 @@ gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px
     }
     CK(ctx->rs_cmp.ensure((size_t)cxi * h));
     CK(ctx->rs_crop.ensure((size_t)cxo * nh));
+    if (reinterpret_cast<uintptr_t>(img) & 255) {
+        // a caller's device view at an offset: cuFFT's R2C wants an aligned
+        // input (staged host images are placed 256-byte aligned)
+        CK(ctx->rs_src.ensure((size_t)w * h));
+        CK(cudaMemcpyAsync(ctx->rs_src.p, img, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToDevice, ctx->st));
+        img = ctx->rs_src.p;
+    }
     cufftHandle p1, p2;
     CKS(get_plan(ctx, 1, h, w, &p1));
     CKS(get_plan(ctx, 2, nh, nw, &p2));
@@ -1892,6 +1900,7 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->cmp.release();
     ctx->rs_cmp.release();
     ctx->rs_crop.release();
+    ctx->rs_src.release();
     ctx->acc.release();
     ctx->hsum.release();
     ctx->lpfull.release();
