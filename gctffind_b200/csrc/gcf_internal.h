@@ -365,7 +365,8 @@ void launch_synth_raw(unsigned long long seed, unsigned long long first, const f
                       const PixOptics& base, float* raw, cudaStream_t st);
 void launch_im2col_p4(const __nv_bfloat16* x, int B, __nv_bfloat16* cols, cudaStream_t st);
 // the first layer (4 x 4 stride-4 patches of x, 16 outputs, bias + ReLU)
-// without im2col rows; w: [16][16] BF16
+// without im2col rows; w: [16][16] BF16; x 8-byte and y 16-byte aligned (the
+// network's own buffers)
 void launch_conv1_direct(const __nv_bfloat16* x, int B, const __nv_bfloat16* w, const float* bias,
                          __nv_bfloat16* y, cudaStream_t st);
 void launch_im2col_3s2(const __nv_bfloat16* x, int B, int H, int W, int C, __nv_bfloat16* cols, cudaStream_t st);
