@@ -164,3 +164,38 @@ def test_trained_network_gain_on_held_out_spectra(gpu_lib):
     assert cl["table_cand"] < 0.5 * cb["table_cand"], (cl, cb)
     # both stay as close to the generator's truth as the plain search
     assert TI.truth_error(learned, prm) <= TI.truth_error(plain, prm) + 20.0
+
+
+def test_learned_threshold_sends_searches_to_the_full_search(gpu_lib):
+    """gcf_set_learned_threshold: with the CC threshold at 1 every learned
+    search falls back to the full contraction search, so the learned method
+    returns the BF16 method's results; values outside [-1, 1] are rejected."""
+    from gctffind_b200 import synth
+    G = gpu_lib
+    specs = [synth.MicrographSpec(width=1536, height=1536, pixel_size=1.3, df_min=12000.0 + 3000 * k,
+                                  df_max=12400.0 + 3000 * k, azimuth_deg=20.0 * k, dose=2.0, seed=600 + k)
+             for k in range(4)]
+    imgs = [synth.make_micrograph(s, device="cuda") for s in specs]
+    op = G.make_optics()
+    ctx = G.Context(0, 512, 0)
+    G.load_learned(ctx)
+    bf16 = ctx.run_batch(imgs, [1.3] * 4, op, mode=G.GCF_SEARCH_BF16)
+    ctx.set_learned_threshold(1.0)
+    learned = ctx.run_batch(imgs, [1.3] * 4, op, mode=G.GCF_SEARCH_LEARNED)
+    assert ctx.fast_counts()["fallbacks"] == 4
+    assert [r.as_dict() for r in learned] == [r.as_dict() for r in bf16]
+    with pytest.raises(G.GcfError):
+        ctx.set_learned_threshold(1.5)
+    ctx.close()
+
+
+def test_set_params_round_trip_and_size_check(gpu_lib):
+    G = gpu_lib
+    ctx = G.Context(0, 512, 0)
+    ctx.nn_init(5)
+    p = ctx.nn_params() * 0.5
+    ctx.nn_set_params(p)
+    assert np.array_equal(ctx.nn_params(), p.astype(np.float32))
+    with pytest.raises(G.GcfError):
+        ctx.nn_set_params(p[:-1])
+    ctx.close()
