@@ -9,10 +9,12 @@ defocus 5000-40000 A, astigmatism 0-1000 A at a random angle, dose
 
   value  : micrographs/s of the learned + batched + BF16 contraction path
            (GCF_SEARCH_LEARNED when trained weights are present, else
-           GCF_SEARCH_BF16), micrographs resident in HBM, device time from
-           CUDA events on the library stream
+           GCF_SEARCH_BF16) with the rescale as two BF16 tensor-core
+           products (GCF_RESCALE_GEMM; `fast_with_cufft_rescale` is the same
+           path with the reference's cuFFT rescale), micrographs resident in
+           HBM, device time from CUDA events on the library stream
   plain  : the same batch through this project's plain FP32 exhaustive
-           search, batched (one GCF_SEARCH_PLAIN call) and in the
+           search and the cuFFT rescale, batched (one GCF_SEARCH_PLAIN call) and in the
            reference's single-file mode (one call per micrograph)
   e2e    : the headline path with pinned HOST buffers, host clock around the
            call: host->device copies of the 256 images and the result rows
@@ -73,6 +75,8 @@ def parse():
                     help="only rescale one frame of each raw size of the batch (3838x3710 @ 0.9, 5760x4092 @ 0.8, "
                          "4096x4096 @ 1.0 A/px) through both rescale implementations, 2 + 5 calls each "
                          "(for a profiler's launch list), and print their wall-clock times")
+    ap.add_argument("--rescale", default="gemm", choices=["gemm", "cufft", "lines"],
+                    help="rescale of the headline path (the plain path always takes cuFFT, the reference's calls)")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel from the host")
     ap.add_argument("--no-autotune", action="store_true", help="default shapes instead of the autotuner's")
     ap.add_argument("--no-secondary", action="store_true",
@@ -300,7 +304,8 @@ def cpu_baseline(host, specs, budget_s=20.0):
                       f"search), FP64 oracle, {cores} OpenMP threads, {dt:.1f} s"}
 
 
-def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, series_tilts=61, lines_ctx=None):
+def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, series_tilts=61, lines_ctx=None,
+                   fast_rescale=0):
     """The mixed stream: 2000 micrographs of the uneven mix in batches of 250,
     interleaved with 8 tilt series of 61 tilts (-60..+60 deg in 2 deg
     steps, 4096^2 at 1.35 A/px).  Each batch and series is made on the
@@ -309,8 +314,9 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
     search, the series through the reference's series policy (the series
     search is the plain one in both columns).  Each batch's first call also
     makes a cuFFT plan for every new rescaled size (the pixel size varies
-    continuously); that call is reported on its own, and the timed calls of
-    both methods run with the plans made.  With lines_ctx (a context whose
+    continuously); that call (headline search, cuFFT rescale) is reported on
+    its own, and the timed calls run with the plans made: the headline
+    search with its rescale (fast_rescale), the plain search with cuFFT's.  With lines_ctx (a context whose
     rescale is the library's line transforms, which make no plans), each
     batch's first and second calls through it are reported as well.
     Defocus error: the headline search against the plain one on the 2000
@@ -332,10 +338,13 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
             lines_first_ms += lines_ctx.stage_times()["total"]
             lines_ctx.run_batch(imgs, pxs, op, mode=fast_mode)
             lines_ms += lines_ctx.stage_times()["total"]
+        ctx.set_rescale_impl(G.GCF_RESCALE_CUFFT)
         ctx.run_batch(imgs, pxs, op, mode=fast_mode)
         first_ms += ctx.stage_times()["total"]
+        ctx.set_rescale_impl(fast_rescale)
         fast_res += ctx.run_batch(imgs, pxs, op, mode=fast_mode)
         fast_ms += ctx.stage_times()["total"]
+        ctx.set_rescale_impl(G.GCF_RESCALE_CUFFT)
         plain_res += ctx.run_batch(imgs, pxs, op, mode=G.GCF_SEARCH_PLAIN)
         plain_ms += ctx.stage_times()["total"]
         specs_all += specs
@@ -372,7 +381,8 @@ def stream_figures(ctx, G, fast_mode, world, rank, n_batches=8, per_batch=250, s
             "value": round(world * n_mics / (fast_ms / 1000.0), 2), "unit": "micrographs/s",
             "plain_value": round(world * n_mics / (plain_ms / 1000.0), 2),
             "first_call_value": round(world * n_mics / (max_over_ranks(first_ms, world) / 1000.0), 2),
-            "first_call_note": "each batch's first call, cuFFT plans of its new rescaled sizes included",
+            "first_call_note": "each batch's first call (cuFFT rescale), cuFFT plans of its new rescaled sizes "
+                               "included",
             "speedup_vs_plain": round(plain_ms / fast_ms, 3), "micrographs": n_mics,
             "defocus_error": defocus_error(fast_res, plain_res, specs_all),
             "rescale_lines": lines}
@@ -551,8 +561,9 @@ def run_reference(args, rank, world):
 
 def rescale_compare(G, dev):
     """One frame of each raw size below 1.2 A/px of the uneven batch through
-    gcf_rescale with the line transforms and with cuFFT; wall clock per call
-    (the rescaled frame is copied to the host by the call)."""
+    gcf_rescale with the line transforms, the tensor-core products and cuFFT;
+    wall clock per call (the rescaled frame is copied to the host by the
+    call)."""
     import numpy as np
     import torch
     ctx = G.Context(dev, 512, 0)
@@ -560,7 +571,8 @@ def rescale_compare(G, dev):
     out = []
     for (w, h, px) in [(3838, 3710, 0.9), (5760, 4092, 0.8), (4096, 4096, 1.0)]:
         img = torch.from_numpy(rng.poisson(2.0, size=(h, w)).astype(np.float32)).to(f"cuda:{dev}")
-        for name, impl in (("lines", G.GCF_RESCALE_LINES), ("cufft", G.GCF_RESCALE_CUFFT)):
+        for name, impl in (("lines", G.GCF_RESCALE_LINES), ("gemm", G.GCF_RESCALE_GEMM),
+                           ("cufft", G.GCF_RESCALE_CUFFT)):
             ctx.set_rescale_impl(impl)
             for _ in range(2):
                 ctx.rescale(img, px)
@@ -600,19 +612,27 @@ def main():
     fast_mode = G.GCF_SEARCH_LEARNED if learned else G.GCF_SEARCH_BF16
     if learned:
         G.load_learned(ctx)
+    fast_rescale = {"gemm": G.GCF_RESCALE_GEMM, "cufft": G.GCF_RESCALE_CUFFT,
+                    "lines": G.GCF_RESCALE_LINES}[args.rescale]
 
     clk = ClockSampler(local)
     clk.start()
     # ---- the headline path, device-resident ----
+    ctx.set_rescale_impl(fast_rescale)
     torch.cuda.nvtx.range_push("fast_steps")
     fast = timed_batch(ctx, imgs, pxs, op, fast_mode, args.steps, args.warmup, world)
     torch.cuda.nvtx.range_pop()
-    # ---- plain FP32 search: batched, and single-file mode ----
-    plain = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_PLAIN, args.steps, min(args.warmup, 2), world)
     # ---- the contraction search without the network (what the network saves) ----
     nonet = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_BF16, args.steps, min(args.warmup, 2), world) \
         if learned else None
+    # ---- plain FP32 search with the reference's cuFFT rescale: batched, and single-file mode ----
+    ctx.set_rescale_impl(G.GCF_RESCALE_CUFFT)
+    plain = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_PLAIN, args.steps, min(args.warmup, 2), world)
     single_ms, single_wall = timed_single_file(ctx, imgs, pxs, op, max(1, min(args.steps, 2)), world)
+    # ---- the headline search with the cuFFT rescale (what the tensor-core rescale saves) ----
+    fast_cufft = timed_batch(ctx, imgs, pxs, op, fast_mode, args.steps, min(args.warmup, 2), world) \
+        if fast_rescale != G.GCF_RESCALE_CUFFT else None
+    ctx.set_rescale_impl(fast_rescale)
     # ---- end to end: pinned host inputs, host clock around the call ----
     host = [im.cpu().pin_memory() for im in imgs]
     dims = [(G.rescale_dims(s.width, s.height, s.pixel_size)[0], G.rescale_dims(s.width, s.height, s.pixel_size)[1])
@@ -646,6 +666,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
             "data": "synthetic",
             "config": {"workload": workload_name(n), "search": ["bf16", "learned"][int(learned)],
+                       "rescale": args.rescale,
                        "tile": 512, "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({sum(4 * s.width * s.height for s in specs) / 1e9:.1f} GB "
                              "per step)"},
@@ -668,6 +689,12 @@ def main():
                 "note": "the same batch through the contraction search without the learned window; "
                         "learned_search_ms is the headline's search1d + search2d, learned_network_ms its "
                         "network (inputs and layers), which runs before the search stages"},
+            "fast_with_cufft_rescale": None if fast_cufft is None else {
+                "value": round(world * n / (fast_cufft["ms"] / 1000.0), 2),
+                "ms_per_step": round(fast_cufft["ms"], 3),
+                "stage_ms": {k: round(v, 3) for k, v in fast_cufft["stage"].items()},
+                "defocus_error": defocus_error(fast_cufft["results"], plain["results"], specs),
+                "note": "the headline search with the reference's cuFFT rescale instead of the tensor-core one"},
             "defocus_error": defocus_error(fast["results"], plain["results"], specs),
             "stage_ms_per_step": {k: round(v, 3) for k, v in fast["stage"].items()},
             "contraction": {"stage_ms": {k: round(v, 3) for k, v in ft.items()}, "counts": fc,
@@ -688,19 +715,22 @@ def main():
                             "graph_nodes": fast["graph"]["nodes"],
                             "library_kernels_in_graph": fast["graph"]["kernels"],
                             "note": "each timed step is one graph launch holding gpu_launches kernels of this "
-                                    "library (plus cuFFT's rescale and lowpass kernels) when graph_launches_per_step "
+                                    "library (plus cuFFT's lowpass kernels, and its rescale kernels when the "
+                                    "rescale takes cuFFT) when graph_launches_per_step "
                                     "is 1"},
             "autotune": tuning,
             "roofline": tile_kernel_roofline(fast["stage"], dims, pk),
             "clocks": clocks}
     if not args.no_secondary:
         line["series_41x4096"] = series_figures(ctx, G, max(2, min(args.steps, 3)), 2, world, rank)
+        ctx.set_rescale_impl(G.GCF_RESCALE_CUFFT)
         line["single_4096_1p0"] = single_1p0(ctx, G, max(2, min(args.steps, 5)))
         lines_ctx = G.Context(local, 512, 0)
         lines_ctx.set_rescale_impl(G.GCF_RESCALE_LINES)
         if fast_mode == G.GCF_SEARCH_LEARNED:
             G.load_learned(lines_ctx)
-        line["stream_2000_plus_8x61"] = stream_figures(ctx, G, fast_mode, world, rank, lines_ctx=lines_ctx)
+        line["stream_2000_plus_8x61"] = stream_figures(ctx, G, fast_mode, world, rank, lines_ctx=lines_ctx,
+                                                       fast_rescale=fast_rescale)
         lines_ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline([h.numpy() for h in host], specs)

@@ -9,6 +9,6 @@ from .api import (  # noqa: F401
     CCTFTheory, CFindCtf2D, Context, CtfParam, GcfError, Item, Optics, Result, GCF_SPECT_CUFFT,
     GCF_SPECT_FUSED, EXPORTS, LIB_PATH, CLI_PATH, load_library, make_optics, mrc_info, mrc_read,
     mrc_read_tilts, mrc_write, rescale_dims, series_order, write_ctf_file,
-    GCF_SEARCH_PLAIN, GCF_SEARCH_BF16, GCF_SEARCH_LEARNED, GCF_RESCALE_LINES, GCF_RESCALE_CUFFT,
+    GCF_SEARCH_PLAIN, GCF_SEARCH_BF16, GCF_SEARCH_LEARNED, GCF_RESCALE_LINES, GCF_RESCALE_CUFFT, GCF_RESCALE_GEMM,
 )
 from .learned import WEIGHTS_PATH, learned_available, load_learned  # noqa: F401

@@ -26,6 +26,7 @@ GCF_SPECT_CUFFT = 1
 
 GCF_RESCALE_CUFFT = 0
 GCF_RESCALE_LINES = 1
+GCF_RESCALE_GEMM = 2
 
 GCF_SEARCH_PLAIN = 0
 GCF_SEARCH_BF16 = 1
@@ -275,8 +276,9 @@ class Context:
         _check(self.L.gcf_set_spectrum_impl(self._h, impl), self._h)
 
     def set_rescale_impl(self, impl: int):
-        """GCF_RESCALE_CUFFT (the reference's cuFFT calls, default) or
-        GCF_RESCALE_LINES (the library's line transforms: no plans to make)."""
+        """GCF_RESCALE_CUFFT (the reference's cuFFT calls, default),
+        GCF_RESCALE_LINES (the library's line transforms: no plans to make) or
+        GCF_RESCALE_GEMM (the crop as two BF16 tensor-core products)."""
         _check(self.L.gcf_set_rescale_impl(self._h, impl), self._h)
 
     def set_fused_shape(self, shape: int):

@@ -217,6 +217,9 @@ struct gcf_ctx {
     DBuf<float> images, rescaled, tiles;
     DBuf<float2> cmp, rs_cmp, rs_crop;
     DBuf<float> rs_src;   // an aligned copy of a device image cuFFT cannot read in place
+    DBuf<__nv_bfloat16> rsg_bf;   // scratch of the tensor-core rescale (gcf_rsgemm.cu)
+    DBuf<float> rsg_f;
+    DBuf<int> rsg_err;            // its products' bounded-wait flag, checked when results are read
     DBuf<double> acc, hsum, moments, moments2;
     DBuf<float> lpfull;
     DBuf<float2> lpcmp;
@@ -1146,6 +1149,16 @@ gcf_status run_search_enqueue(gcf_ctx* ctx, const std::vector<JobSpec>& specs, S
 }
 
 // Reads back the results of an enqueued search (waits for it on the host).
+// The tensor-core rescale's flag, read back with a call's results: a
+// bounded wait of its products gave up (the flag is cleared for the next
+// call).
+gcf_status check_rescale_gemm(gcf_ctx* ctx, int flag)
+{
+    if (!flag) return GCF_OK;
+    CK(cudaMemset(ctx->rsg_err.p, 0, sizeof(int)));
+    return fail(ctx, GCF_ERR_TIMEOUT, "tensor-core rescale product: a bounded wait gave up");
+}
+
 gcf_status run_search_collect(gcf_ctx* ctx, const SearchPending& pend, std::vector<gcf_result>& out)
 {
     const int nj = pend.nj;
@@ -1154,7 +1167,11 @@ gcf_status run_search_collect(gcf_ctx* ctx, const SearchPending& pend, std::vect
     CK(cudaMemcpyAsync(out.data(), ctx->d_res.p, nj * sizeof(gcf_result), cudaMemcpyDeviceToHost, pend.st));
     std::vector<int> cnt(3 * (size_t)nj);
     CK(cudaMemcpyAsync(cnt.data(), ctx->d_counts.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, pend.st));
+    int rs_err = 0;
+    if (ctx->rsg_err.p)
+        CK(cudaMemcpyAsync(&rs_err, ctx->rsg_err.p, sizeof(int), cudaMemcpyDeviceToHost, pend.st));
     CK(cudaStreamSynchronize(pend.st));
+    CKS(check_rescale_gemm(ctx, rs_err));
     for (int j = 0; j < nj; ++j) {
         const long long n2 = cnt[3 * j], n1 = cnt[3 * j + 1], p1 = cnt[3 * j + 2];
         ctx->search_counts[0] += n2;
@@ -1611,6 +1628,18 @@ gcf_status rescale_device(gcf_ctx* ctx, const float* img, int w, int h, float px
         ctx->launches += 3;
         return GCF_OK;
     }
+    if (ctx->rescale_impl == GCF_RESCALE_GEMM && rescale_gemm_supported(w, h, nw, nh)) {
+        const RescaleGemmLayout L = rescale_gemm_layout(w, h, nw, nh);
+        CK(ctx->rsg_bf.ensure((size_t)L.bf16_elems));
+        CK(ctx->rsg_f.ensure((size_t)L.f32_elems));
+        if (!ctx->rsg_err.p) {
+            CK(ctx->rsg_err.ensure(1));
+            CK(cudaMemset(ctx->rsg_err.p, 0, sizeof(int)));
+        }
+        CK(launch_rescale_gemm(img, w, w, h, nw, nh, ctx->rsg_bf.p, ctx->rsg_f.p, ctx->rsg_err.p, out, ctx->st));
+        ctx->launches += 5;
+        return GCF_OK;
+    }
     CK(ctx->rs_cmp.ensure((size_t)cxi * h));
     CK(ctx->rs_crop.ensure((size_t)cxo * nh));
     if (reinterpret_cast<uintptr_t>(img) & 255) {
@@ -1901,6 +1930,9 @@ void gcf_destroy(gcf_ctx* ctx)
     ctx->rs_cmp.release();
     ctx->rs_crop.release();
     ctx->rs_src.release();
+    ctx->rsg_bf.release();
+    ctx->rsg_f.release();
+    ctx->rsg_err.release();
     ctx->acc.release();
     ctx->hsum.release();
     ctx->lpfull.release();
@@ -1985,7 +2017,8 @@ void gcf_destroy(gcf_ctx* ctx)
 
 gcf_status gcf_set_rescale_impl(gcf_ctx* ctx, int impl)
 {
-    if (!ctx || (impl != GCF_RESCALE_LINES && impl != GCF_RESCALE_CUFFT)) return GCF_ERR_INVALID_ARG;
+    if (!ctx || (impl != GCF_RESCALE_LINES && impl != GCF_RESCALE_CUFFT && impl != GCF_RESCALE_GEMM))
+        return GCF_ERR_INVALID_ARG;
     ctx->rescale_impl = impl;
     return GCF_OK;
 }
@@ -2043,8 +2076,11 @@ gcf_status gcf_rescale(gcf_ctx* ctx, const float* img, int w, int h, float px, i
         CK(cudaMemcpy2DAsync(host_out, nw * sizeof(float), d, w * sizeof(float),
                              nw * sizeof(float), nh, cudaMemcpyDeviceToHost, ctx->st));
     }
+    int rs_err = 0;
+    if (ctx->rsg_err.p)
+        CK(cudaMemcpyAsync(&rs_err, ctx->rsg_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    return GCF_OK;
+    return check_rescale_gemm(ctx, rs_err);
 }
 
 gcf_status gcf_set_fused_shape(gcf_ctx* ctx, int shape)

@@ -296,6 +296,24 @@ cudaError_t launch_umma_gemm(const __nv_bfloat16* A, long long lda, const __nv_b
 cudaError_t launch_umma_gemm_persistent(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B,
                                         long long ldb, GemmArgs g, int bn, int stages, int ntiles, cudaStream_t st);
 
+// gcf_rsgemm.cu: the Fourier-crop rescale as two BF16 tensor-core products
+// (raw sides up to kRescaleGemmMax).  Scratch: bf16_elems BF16 and
+// f32_elems FP32 elements, laid out as below (offsets in elements).
+constexpr int kRescaleGemmMax = 16384;
+struct RescaleGemmLayout {
+    long long ldw, ldk;                   // row pitches: K = w, K = h + 1
+    long long off_x, off_w, off_k, off_t; // BF16 image, row map, column map, T^T
+    long long bf16_elems;
+    long long off_uc, off_bias;           // FP32: partial column sums at 0, (u, cos, sin, cos) per
+    long long f32_elems;                  // column, the per-column bias
+};
+bool rescale_gemm_supported(int w, int h, int nw, int nh);
+RescaleGemmLayout rescale_gemm_layout(int w, int h, int nw, int nh);
+// img (w x h, row pitch `pitch` floats) -> out (nw x nh, dense); err: the
+// products' device flag (0 on entry; set if a bounded wait gave up).
+cudaError_t launch_rescale_gemm(const float* img, long long pitch, int w, int h, int nw, int nh,
+                                __nv_bfloat16* bf, float* f32, int* err, float* out, cudaStream_t st);
+
 // gcf_contract.cu: the BF16 candidate contraction.
 // Common polar grid of a batch: ns bins uniform in s^2 (1/A^2) over the
 // band [s2_lo, s2_lo + ns * ds2), nth angle bins over [-90, 90) degrees, and

@@ -70,10 +70,15 @@ typedef enum {
 typedef enum {
     GCF_RESCALE_CUFFT = 0, /* cuFFT R2C + crop + C2R, the reference's calls
                               (default: the faster once a size's plans exist) */
-    GCF_RESCALE_LINES = 1  /* hand-written line transforms (gcf_resize.cu): no
+    GCF_RESCALE_LINES = 1, /* hand-written line transforms (gcf_resize.cu): no
                               plans to make, so new sizes cost nothing extra;
                               raw width even and every line of the raw and new
                               sizes <= 4096 long, else cuFFT */
+    GCF_RESCALE_GEMM = 2   /* the crop as two BF16 tensor-core products
+                              (gcf_rsgemm.cu): img -> Rh img Rw^T with closed-form
+                              maps; BF16 operands, so within ~0.5 % of rms of
+                              cuFFT, not bit-identical; raw sides <= 16384,
+                              else cuFFT */
 } gcf_rescale_impl;
 
 /* ---------------------------------------------------------------------- */
@@ -89,8 +94,8 @@ const char* gcf_strerror(gcf_status s);
 /* Last error detail of this context (CUDA/cuFFT message), never NULL. */
 const char* gcf_last_error(gcf_ctx* ctx);
 gcf_status gcf_set_spectrum_impl(gcf_ctx* ctx, int impl);
-/* GCF_RESCALE_CUFFT (default) or GCF_RESCALE_LINES for the images below
- * 1.2 A/px. */
+/* GCF_RESCALE_CUFFT (default), GCF_RESCALE_LINES or GCF_RESCALE_GEMM for
+ * the images below 1.2 A/px. */
 gcf_status gcf_set_rescale_impl(gcf_ctx* ctx, int impl);
 /* Cluster shape of the fused tile kernel: 0 = the shape that keeps the most
  * SMs busy (default), 8 = 8 CTAs x 8 warps, 816 = 8 CTAs x 16 warps,
