@@ -229,7 +229,7 @@ def defocus_error(fast, plain, specs):
             "one_step": "max(20 A, 0.105 * mean / 31): the plain search's last mean-defocus step"}
 
 
-def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
+def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world, tag=""):
     import torch
     for _ in range(warmup):
         ctx.run_batch(imgs, pxs, op, mode=mode)
@@ -238,7 +238,7 @@ def timed_batch(ctx, imgs, pxs, op, mode, steps, warmup, world):
     dev_ms, launches, stage, ftimes, fcounts = 0.0, 0, {}, {}, {}
     graph_launches = 0
     res = None
-    torch.cuda.nvtx.range_push(f"timed_mode{mode}")
+    torch.cuda.nvtx.range_push(f"timed_mode{mode}{tag}")
     for _ in range(steps):
         res = ctx.run_batch(imgs, pxs, op, mode=mode)
         st = ctx.stage_times()
@@ -630,8 +630,8 @@ def main():
     plain = timed_batch(ctx, imgs, pxs, op, G.GCF_SEARCH_PLAIN, args.steps, min(args.warmup, 2), world)
     single_ms, single_wall = timed_single_file(ctx, imgs, pxs, op, max(1, min(args.steps, 2)), world)
     # ---- the headline search with the cuFFT rescale (what the tensor-core rescale saves) ----
-    fast_cufft = timed_batch(ctx, imgs, pxs, op, fast_mode, args.steps, min(args.warmup, 2), world) \
-        if fast_rescale != G.GCF_RESCALE_CUFFT else None
+    fast_cufft = timed_batch(ctx, imgs, pxs, op, fast_mode, args.steps, min(args.warmup, 2), world,
+                             tag="_cufft_rescale") if fast_rescale != G.GCF_RESCALE_CUFFT else None
     ctx.set_rescale_impl(fast_rescale)
     # ---- end to end: pinned host inputs, host clock around the call ----
     host = [im.cpu().pin_memory() for im in imgs]
