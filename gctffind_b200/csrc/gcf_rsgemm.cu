@@ -19,13 +19,13 @@
 // and Iw[x][j] = (1 - (-1)^x cos(pi j nw / w)) cot(pi t)  (0 at t = 0).
 //
 // A constant image c maps to c w h, so the BF16 copy holds img - c (c: the
-// mean of 256 pixels of the middle row), and the second product adds c w h back in FP32
-// as a per-column bias: the BF16 rounding then scales with the image's
-// fluctuations, not with its mean.
+// mean of 256 pixels of the middle row), and the second product adds c w h
+// back in FP32 as a per-column bias: the BF16 rounding then scales with the
+// image's fluctuations, not with its mean.
 //
 // So: img -> BF16 (with the column sums u), the two maps in BF16, then
-//   T^T = (img Rw^T)^T   (nw x h, BF16; the product's transposed output),
-//   out = Rh' T'          (FP32), Rh' = [Rh | -a], T' = [T^T | v]:
+//   T^T = (img Rw^T)^T    (nw x h, BF16; the product's transposed output),
+//   out = Rh' T'^T + c w h (FP32), Rh' = [Rh | -a], T' = [T^T | v]:
 // the rank-one term rides in one extra K column of the second product.
 // The maps cost O(n_out n_in) to write, far less than the products.
 #include <cuda_bf16.h>
