@@ -33,6 +33,17 @@ def test_library_exports_every_declared_symbol():
         assert re.search(r"\bT %s\b" % s, out), s
 
 
+def test_python_constants_match_the_header_enums():
+    """Every GCF_SPECT_*, GCF_RESCALE_* and GCF_SEARCH_* value the binding
+    exports equals the header's."""
+    src = open(os.path.join(ROOT, "include", "gctf_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    vals = {k: int(v) for k, v in re.findall(r"\b(GCF_(?:SPECT|RESCALE|SEARCH)_[A-Z0-9]+)\s*=\s*(\d+)", src)}
+    assert {"GCF_RESCALE_CUFFT", "GCF_RESCALE_LINES", "GCF_RESCALE_GEMM"} <= set(vals)
+    for k, v in vals.items():
+        assert getattr(G, k) == v, k
+
+
 def test_strerror_codes():
     L = G.load_library()
     assert L.gcf_strerror(0) == b"ok"
